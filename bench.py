@@ -1,0 +1,364 @@
+"""Throughput of the MPS particle step on B200: particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload explicit|semi]
+                    [--impl ours|reference] [--arith exact|fast]
+
+One step = one MPS time step of the whole scene (all particles: fluid, wall
+and dummy).  `value` = particles x steps / device time of the timed steps
+(CUDA events on the library's stream, L2 flushed before every timed step,
+max over ranks), `e2e` = the same metric through the C ABI with host
+buffers: every step uploads the state from pinned host memory
+(mps_set_state), steps (mps_step_async) and reads positions, velocities and
+pressures back (mps_get_state), timed by the host clock.
+
+Multi-GPU: the scenes are independent, so N GPUs run N replicas (one scene
+per rank, seeded by rank) with no data-path collective; NCCL is used only for
+the barrier and the max of the timings.
+
+--impl reference times the reference's own CPU step on the host cores
+(oracle/_ref: MPS_CAL_expl_v1.0 for the explicit workload), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+# algorithmic bytes per particle per stage (fixed accounting model: float3 =
+# 12 B, scalar/type = 4 B, neighbour reads counted once per stage)
+STAGE_BYTES = {
+    "visc": 52, "collision": 52, "pnd": 24, "dash": 56, "pressure": 8,
+    "cell_keys": 20, "radix_sort": 32, "gather": 64, "update_dt": 12,
+}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def make_scene(workload: str, seed: int):
+    from mps_solvers_b200 import scene
+    if workload == "explicit":
+        return scene.dam_break_explicit(seed=seed)
+    return scene.dam_break_semi(seed=seed)
+
+
+def workload_name(workload: str) -> str:
+    if workload == "explicit":
+        return ("explicit EOS dam break: 70,912 particles (8,000 fluid), l0=0.02 m, "
+                "r0=2.1 l0, rlap=4.0 l0, c0=20 m/s, dt=1e-4 s")
+    return ("semi-implicit dam break: 310,912 particles (80,000 fluid), l0=0.01 m, "
+            "PPE diagonally scaled CG to 1e-8 relative residual, dt=5e-4 s")
+
+
+def cpu_baseline(workload: str, case_dir: str, n_particles: int, sample_steps: int):
+    """Reference CPU step on the host cores (oracle/_ref); bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    if workload == "explicit" and oracle.have_reference_build():
+        out = os.path.join(case_dir, "ref_bench.bin")
+        info = oracle.run_reference("expl", case_dir, sample_steps, 0, out, threads=threads,
+                                    timeout=1800)
+        os.unlink(out)
+        v = n_particles * sample_steps / info["steps_s"]
+        return {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                "sample": f"{sample_steps} steps of the same scene, MPS_CAL_expl_v1.0 CPU path "
+                          f"(GPU_CUDA off) built from the reference sources, {threads} OpenMP "
+                          f"threads, step() only",
+                "cpu": _cpu_model()}
+    # semi-implicit: the oracle's sparse restatement of the reference rules
+    orc = oracle.Oracle(case_dir, oracle.SEMI_JACOBI, 64)
+    orc.set_cg(True, 1e-8, 100000)
+    t0 = time.perf_counter()
+    orc.step(sample_steps)
+    dt = time.perf_counter() - t0
+    return {"value": n_particles * sample_steps / dt, "unit": "particle-steps/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{sample_steps} steps, sparse FP64 restatement of MPS_CAL_v4.0 "
+                      f"MPS_CPU_EXPL (the dense reference cannot hold this size), {threads} threads",
+            "cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return None
+    from mps_solvers_b200 import scene
+    with tempfile.TemporaryDirectory() as d:
+        pos, nb2, nb1 = scene.write_case(d, make_scene(args.workload, 0))
+        n = len(pos)
+        # each "step" of this arm is the bounded CPU sample
+        sample = args.ref_sample if args.ref_sample else (100 if args.workload == "explicit" else 1)
+        vals = []
+        cb = None
+        for _ in range(max(1, args.steps)):
+            cb = cpu_baseline(args.workload, d, n, sample)
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    cb["value"] = v
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.workload == "explicit" else "f64",
+        "data": "synthetic", "config": {"workload": workload_name(args.workload), "particles": n},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    from mps_solvers_b200 import capi, scene
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    method = capi.METHOD_EXPLICIT if args.workload == "explicit" else capi.METHOD_SEMI_IMPLICIT
+    arith = capi.ARITH_EXACT if args.arith == "exact" else capi.ARITH_FAST
+    tmpd = tempfile.mkdtemp(prefix=f"mpsb_{rank}_")
+    pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank))
+    n = len(pos0)
+    sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    # warm-up (also captures the step graphs)
+    for _ in range(args.warmup):
+        sim.step_async(1)
+    sim.step(0)
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))  # write > L2 between timed steps
+                ev[k][0].record(stream)
+                sim.step_async(1)
+                ev[k][1].record(stream)
+        stream.synchronize()
+    stats = sim.step(0)
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    clocks = clk.summary()
+
+    # e2e: host buffers through the C ABI
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    npart = sim.counts()["np"]
+    hpos, hvel, hp = pin((npart, 3)), pin((npart, 3)), pin((npart,))
+    sim.get_state_into(hpos, hvel, hp)
+    e2e_steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.set_state(pos=hpos, vel=hvel, press=hp)
+        sim.step_async(1)
+        sim.get_state_into(hpos, hvel, hp)
+    e2e_s = time.perf_counter() - t0
+    h2d = npart * (12 + 12 + 4)
+    d2h = npart * (12 + 12 + 4)
+
+    # per-stage device times (stage by stage, no graph) for the roofline
+    prof = sim.profile(max(3, min(args.steps, 10)))
+    prof_steps = max(3, min(args.steps, 10))
+    launches = int(sim.scalars()["launches_per_step"])
+    sim.close()
+
+    # max over ranks
+    tot = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    ms, e2e_s = float(tot[0]), float(tot[1])
+    if rank != 0:
+        return None
+
+    value = world * n * args.steps / (ms / 1e3)
+    e2e_v = world * n * e2e_steps / e2e_s
+    peak, peak_kind = measured_peaks()
+    # dominant kernel: the stage with the largest device time
+    kern = {k: v for k, v in prof.items() if k in STAGE_BYTES}
+    dom = max(kern, key=kern.get)
+    per_step_launches = 3 if dom in ("cell_keys", "radix_sort", "gather") else 1
+    dom_ms = kern[dom] / (prof_steps * per_step_launches)
+    alg_bytes = STAGE_BYTES[dom] * n
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    traffic = _traffic_from_profiles(dom, args.workload)
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if method == capi.METHOD_EXPLICIT else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": workload_name(args.workload), "particles": n,
+                   "fluid": int(n - nb2 - nb1), "arith": args.arith,
+                   "l2": "flushed (256 MB write) before every timed step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "ms_per_launch": dom_ms},
+        "stage_ms_per_step": {k: v / prof_steps for k, v in prof.items()},
+        "e2e": {"value": e2e_v, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+        "final": {"np": stats.np, "step": stats.step, "time": stats.time, "dt": stats.dt,
+                  "cg_iters": stats.cg_iters},
+    }
+    return line
+
+
+def _traffic_from_profiles(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any
+    (a line `traffic_bytes_per_launch: <kernel> <workload> <bytes>`)."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, f)):
+            if line.startswith("traffic_bytes_per_launch:"):
+                parts = line.split()
+                if len(parts) >= 4 and parts[1] == kernel and parts[2] == workload:
+                    return float(parts[3])
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="explicit", choices=["explicit", "semi"])
+    ap.add_argument("--arith", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--ref-sample", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        line = run_reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    line = run_ours(args, rank, world, local_rank)
+    if line is not None and world == 1 and not args.no_cpu_baseline:
+        from mps_solvers_b200 import scene
+        with tempfile.TemporaryDirectory() as d:
+            pos, _, _ = scene.write_case(d, make_scene(args.workload, 0))
+            sample = 300 if args.workload == "explicit" else 2
+            line["cpu_baseline"] = cpu_baseline(args.workload, d, len(pos), sample)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

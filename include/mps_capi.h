@@ -1,0 +1,221 @@
+/* mps_capi.h -- C ABI of libmps_b200.so, the B200 (sm_100a) MPS particle step.
+ *
+ * This is the boundary a caller of the reference binds instead of the
+ * reference's step classes.  The reference's interface is the C++ class chain
+ * OBJECT -> MPS -> MPS_GPU -> MPS_GPU_EXPL (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.h:16-37,
+ * MPS_CAL_/MPS_GPU.h:18-166) and its CPU twin MPS_CPU_EXPL
+ * (MPS_CAL_v4.0/MPS_CPU_EXPL.h:13-33); each entry point below names the member
+ * it replaces.  include/mps_gpu_expl.hpp rebuilds that class interface on top
+ * of these functions.
+ *
+ * Conventions: plain pointers and sizes only; every function returns an
+ * mps_status (the reference calls exit(code) instead, see mps_status);
+ * arrays passed in or out are HOST memory unless the name ends in _dev;
+ * the library owns all device memory of a handle; one handle must be used
+ * from one host thread at a time; every handle owns one CUDA stream.
+ * Particle arrays are in the reference's cell-sorted order unless an
+ * MPS_ORDER_BY_ID order is requested.
+ */
+#ifndef MPS_CAPI_H
+#define MPS_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPS_CAPI_VERSION 1
+
+/* Status codes.  The reference's exit codes map as: exit(3) no GEO.dat
+ * (MPS_CAL_expl_v1.0/MPS.cpp:340-345) -> MPS_ERR_IO; exit(5) cells too thin
+ * (:610-619) -> MPS_ERR_CELLS_TOO_THIN; exit(1) dt below dt_min
+ * (MPS_GPU.cpp:770-776) -> MPS_ERR_DT_TOO_SMALL; exit(4) particle outside the
+ * grid (MPS_CAL_v4.0/MPS_CPU.cpp:172-176) -> MPS_ERR_PARTICLE_OUT (the
+ * explicit method instead drops such particles as the reference's type 3 and
+ * counts them, MPS_CAL_expl_v1.0/MPS_GPU.cpp:268-280). */
+typedef enum {
+    MPS_OK = 0,
+    MPS_ERR_IO = 1,
+    MPS_ERR_CELLS_TOO_THIN = 2,
+    MPS_ERR_DT_TOO_SMALL = 3,
+    MPS_ERR_PARTICLE_OUT = 4,
+    MPS_ERR_CG_NOT_CONVERGED = 5,
+    MPS_ERR_DEVICE_TIMEOUT = 6,
+    MPS_ERR_CUDA = 7,
+    MPS_ERR_NAN = 8,
+    MPS_ERR_INVALID = 9,
+    MPS_ERR_CAPACITY = 10
+} mps_status;
+
+/* Step methods. */
+enum {
+    /* MPS_GPU_EXPL::step: viscosity, collision, PND, equation-of-state
+     * pressure, pressure gradient (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:277-339). */
+    MPS_METHOD_EXPLICIT = 0,
+    /* MPS_CPU_EXPL::step: viscosity, collision, PND, pressure Poisson
+     * equation solved by CG, clamp, gradient (MPS_CAL_v4.0/MPS_CPU_EXPL.cpp:79-135),
+     * every particle update applied two-phase (old state read, then written). */
+    MPS_METHOD_SEMI_IMPLICIT = 1
+};
+
+/* Arithmetic modes of the particle sums. */
+enum {
+    /* float operations in the reference's order with IEEE division and square
+     * root and no fused multiply-add: the explicit step reproduces the
+     * reference's float results bit for bit. */
+    MPS_ARITH_EXACT = 0,
+    /* fused multiply-add and a reciprocal-square-root weight; results agree
+     * with MPS_ARITH_EXACT within float rounding. */
+    MPS_ARITH_FAST = 1
+};
+
+/* PPE preconditioners (semi-implicit method). */
+enum { MPS_PRECOND_DIAGONAL = 0, MPS_PRECOND_LEARNED = 1 };
+
+/* Particle orders for getters. */
+enum { MPS_ORDER_SORTED = 0, MPS_ORDER_BY_ID = 1 };
+
+typedef struct {
+    int method;          /* MPS_METHOD_*                                      */
+    int arith;           /* MPS_ARITH_*                                       */
+    int device;          /* CUDA device ordinal                               */
+    int use_graph;       /* capture each step in a CUDA graph (1) or launch   */
+    double cg_tol;       /* PPE: stop when |r| <= cg_tol * |b| (FP64 norms)   */
+    int cg_max_iter;     /* PPE: iteration limit (0: 10000)                   */
+    int cg_check_every;  /* PPE: iterations between FP64 true-residual checks */
+    int precond;         /* MPS_PRECOND_*                                     */
+    uint32_t capacity;   /* particle capacity (0: the scene's np)             */
+    uint32_t reserved[8];
+} mps_options;
+
+/* The 16 values of input.dat as the reference holds them after
+ * MPS::loadCase: r0, rlap and col_dis already multiplied by dp, dt_min
+ * already multiplied by dt_max (MPS_CAL_expl_v1.0/MPS.cpp:173-331). */
+typedef struct {
+    int dim;
+    float rho, niu, dp, rzero, rlap, beta, cs, cfl, col_dis, col_rate, dt_max, dt_min, tt, tout,
+        max_dis;
+} mps_params;
+
+typedef struct {
+    uint32_t np;         /* active particles (the reference's i_np)            */
+    uint32_t nexcl;      /* particles dropped for leaving the grid (i_nexcl)    */
+    int step;            /* steps taken (i_step)                                */
+    float time;          /* simulated time (d_time, float as in the reference)  */
+    float dt;            /* dt of the last step (d_dt)                          */
+    int cg_iters;        /* PPE iterations of the last step                     */
+    double cg_relres;    /* final FP64 |b - Ax| / |b| of the last step          */
+    int status;          /* sticky device error word mapped to mps_status      */
+    float ms;            /* device time of the call (CUDA events on the stream) */
+    uint32_t reserved[4];
+} mps_step_stats;
+
+typedef struct mps_handle mps_handle;
+
+/* Grid of the reference's cell list (MPS::allocateCellList,
+ * MPS_CAL_expl_v1.0/MPS.cpp:567-642). */
+typedef struct {
+    float left, back, bottom, cell_size;
+    uint32_t cdx, cdy, cdz, ncells;
+    int dim;
+} mps_grid;
+
+const char* mps_status_string(mps_status s);
+void mps_default_options(mps_options* opt);
+
+/* MPS::loadCase + MPS::createGeo + MPS_GPU::Initial (MPS_CAL_expl_v1.0/MPS.cpp:173-407,
+ * MPS_GPU.cpp:63-115): read input.dat and GEO.dat, build the cell grid, sort,
+ * compute n0, lambda and the dummy-to-wall map on the device. */
+mps_status mps_create(const char* input_dat, const char* geo_dat, const mps_options* opt,
+                      mps_handle** out);
+/* Same from memory: positions/velocities (3*np floats, x y z per particle),
+ * pressures (np floats) in GEO.dat order (nb2 dummy, nb1 wall, then fluid). */
+mps_status mps_create_from_arrays(const mps_params* p, uint32_t np, uint32_t nb2, uint32_t nb1,
+                                  const float* pos3, const float* vel3, const float* press,
+                                  const mps_options* opt, mps_handle** out);
+void mps_destroy(mps_handle* h);
+
+/* MPS_GPU_EXPL::step / MPS_CPU_EXPL::step, nsteps times, plus the mps_cal
+ * loop's i_step++ and d_time += d_dt.  Asynchronous on the handle's stream
+ * except that it waits for the steps to end to report stats (may be NULL). */
+mps_status mps_step(mps_handle* h, int nsteps, mps_step_stats* stats);
+
+/* Same steps, only enqueued on the handle's stream: returns without waiting
+ * and reports no device error (the next mps_step, getter or
+ * mps_step(h, 0, &stats) reports it). */
+mps_status mps_step_async(mps_handle* h, int nsteps);
+
+/* MPS_GPU_EXPL::mps_cal (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:216-272): steps
+ * while time < tt, writing out_dir/NNNN.out in the reference's text format
+ * every tout (writeCase, MPS_GPU.cpp:138-152).  out_dir NULL: no output. */
+mps_status mps_run(mps_handle* h, const char* out_dir);
+
+/* getNp / getNb2 / getNb1 (MPS_CAL_/MPS_GPU.h:157-160). */
+mps_status mps_get_counts(mps_handle* h, uint32_t* np, uint32_t* nb2, uint32_t* nb1,
+                          uint32_t* nexcl);
+/* getId / getType / getPos / getVel / getPres (MPS_CAL_/MPS_GPU.h:162-166) plus
+ * the particle number density, copied into caller buffers of np (3*np)
+ * entries; any pointer may be NULL.  order: MPS_ORDER_*; with BY_ID, entry k
+ * is the particle whose GEO.dat index is k (np0 entries, dropped particles
+ * get type 3 and zeros). */
+mps_status mps_get_state(mps_handle* h, uint32_t* id, uint32_t* type, float* pos3, float* vel3,
+                         float* press, float* n, int order);
+/* Overwrite pos/vel/press/n of the active particles (sorted order); used to
+ * drive single stages from a known state.  NULL pointers leave a field. */
+mps_status mps_set_state(mps_handle* h, const float* pos3, const float* vel3, const float* press,
+                         const float* n);
+/* i_cell_list, i_cell_start, i_cell_end after the last divideCell
+ * (MPS_CAL_expl_v1.0/MPS.h:41-45): np, ncells, ncells entries. */
+mps_status mps_get_cell_tables(mps_handle* h, uint32_t* cell_of, uint32_t* start, uint32_t* end);
+mps_status mps_get_grid(mps_handle* h, mps_grid* g);
+/* n0, lambda, dt, time, c_lap = 2d/(n0 lambda), rho c^2, alpha, cg iterations,
+ * cg relative residual, step, status, number of cells, kernels launched by
+ * one step, and 3 spare slots. */
+mps_status mps_get_scalars(mps_handle* h, double out16[16]);
+/* i_normal as GEO.dat indices: for each particle (by GEO index) the GEO index
+ * of its wall particle (itself when it has none), np0 entries. */
+mps_status mps_get_normal_ids(mps_handle* h, uint32_t* normal_id);
+
+/* One stage of the step (for per-stage parity tests):
+ * 0 update_dt, 1 viscosity, 2 divideCell, 3 collision, 4 cal_n,
+ * 5 EOS pressure + dummy copy, 6 pressure gradient + update, 7 PPE + clamp.
+ * Stages 1, 3 and 6 leave their update pending; the next stage 2 applies it
+ * while re-sorting, as the reference's divideCell follows each of them. */
+mps_status mps_phase(mps_handle* h, int phase);
+
+/* Per-stage device times: nsteps steps launched stage by stage (no graph)
+ * with CUDA events between stages; stage_ms[k] (k < max_stages) receives the
+ * summed milliseconds of stage k, *nstages the number of stages, and
+ * mps_stage_name(k) its name (update_dt, visc, collision, pnd, pressure,
+ * dash, step_end, cell_keys, radix_sort, cell_table, gather).  The steps
+ * advance the simulation like mps_step. */
+mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int max_stages, int* nstages);
+const char* mps_stage_name(int k);
+
+/* The handle's cudaStream_t, for callers that time or order work around it. */
+mps_status mps_get_stream(mps_handle* h, void** stream);
+/* Write the reference's text output for the current state:
+ * format 0 = MPS_GPU::writeCase "id type x y z u v w p " (MPS_CAL_expl_v1.0/MPS_GPU.cpp:138-152),
+ * format 1 = MPS_CPU::writeCase "x y z u v w p id " (MPS_CAL_v4.0/MPS_CPU.cpp:127-140). */
+mps_status mps_write_case(mps_handle* h, const char* path, int format);
+/* Text of the last error on this handle. */
+const char* mps_last_error(mps_handle* h);
+
+/* ---- device-pointer primitive: the neighbour-search rebuild ----------------
+ * MPS_GPU::divideCell's ranking (MPS_CAL_expl_v1.0/MPS_GPU.cpp:248-315) on
+ * device arrays: cell id of each of n particles (x y z w float4, w unused),
+ * stable sort by cell, cell start/end tables.  perm_dev[new] = old index;
+ * cell_of_dev[new] = cell id (ncells for a particle outside the grid, sorted
+ * last); start_dev/end_dev get ncells entries; *n_in_grid_dev (device) the
+ * count of particles inside the grid.  Scratch memory is allocated and freed
+ * by the call; stream may be NULL (legacy default stream). */
+mps_status mps_cell_sort_dev(const float* pos4_dev, uint32_t n, const mps_grid* g,
+                             uint32_t* perm_dev, uint32_t* cell_of_dev, uint32_t* start_dev,
+                             uint32_t* end_dev, uint32_t* n_in_grid_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

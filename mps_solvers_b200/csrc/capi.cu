@@ -1,0 +1,770 @@
+// capi.cu -- libmps_b200.so: the C ABI of include/mps_capi.h.
+//
+// A handle owns one scene on one device: two particle buffer sets (the
+// rebuild gathers from one into the other), the sort scratch, the cell
+// table, the per-step device scalars, and one stream.  Every step is the
+// reference's stage order; with use_graph the launches of a step are
+// captured once per buffer parity and replayed.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mps_capi.h"
+#include "cellsort.cuh"
+#include "host_io.h"
+#include "physics.cuh"
+#include "ppe.cuh"
+
+using namespace mpsb;
+
+struct mps_handle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    mps_options opt{};
+    mps_params prm{};
+    HostGrid hg{};
+    HostConst hc{};
+    Grid g{};
+    Phys P{};
+    uint32_t np0 = 0, nb2 = 0, nb1 = 0, cap = 0;
+    int passes = 1;
+    int normal_reach = 1;
+    // device memory
+    State S[2]{};
+    int cur = 0;
+    float4* tmp = nullptr;
+    uint32_t* index_of_id = nullptr;
+    uint32_t* normal_id_of = nullptr;
+    uint32_t* cell_start = nullptr;
+    SortScratch sort{};
+    Scalars* sc = nullptr;
+    unsigned long long* best = nullptr;
+    float* lambda_dev = nullptr;
+    PpeWork ppe{};
+    Staging stage{};
+    // graphs, one per buffer parity
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int pending_apply = APPLY_NONE;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-stage profiling: events recorded between stages when enabled
+    bool prof_on = false;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<int> prof_tag;
+    size_t prof_used = 0;
+    int launches = 0;  // kernels enqueued by the last enqueue_step
+    std::string err;
+    std::vector<void*> allocs;
+};
+
+// ---------------------------------------------------------------- helpers
+static const char* kStatusNames[] = {"ok",
+                                     "io error",
+                                     "cells too thin",
+                                     "dt too small",
+                                     "particle outside the grid",
+                                     "CG did not converge",
+                                     "device wait timed out",
+                                     "CUDA error",
+                                     "NaN detected",
+                                     "invalid argument",
+                                     "capacity exceeded"};
+
+extern "C" const char* mps_status_string(mps_status s) {
+    int k = (int)s;
+    if (k < 0 || k > 10) return "unknown";
+    return kStatusNames[k];
+}
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(_e);         \
+            return MPS_ERR_CUDA;                                                 \
+        }                                                                        \
+    } while (0)
+
+template <class T>
+static cudaError_t dalloc(mps_handle* h, T** p, size_t count) {
+    void* v = nullptr;
+    cudaError_t e = cudaMalloc(&v, count * sizeof(T) + 16);
+    if (e == cudaSuccess) {
+        h->allocs.push_back(v);
+        cudaMemsetAsync(v, 0, count * sizeof(T) + 16, h->stream);
+    }
+    *p = (T*)v;
+    return e;
+}
+
+static StageArgs stage_args(mps_handle* h) {
+    StageArgs a;
+    a.cur = h->S[h->cur];
+    a.cell_start = h->cell_start;
+    a.tmp = h->tmp;
+    a.sc = h->sc;
+    a.g = h->g;
+    a.P = h->P;
+    a.exact = h->opt.arith == MPS_ARITH_EXACT;
+    a.semi = h->opt.method == MPS_METHOD_SEMI_IMPLICIT;
+    return a;
+}
+
+// Stage tags of mps_profile_steps (names in kStageNames).
+enum { ST_UPDATE_DT = 0, ST_VISC, ST_COLLISION, ST_PND, ST_PRESSURE, ST_DASH, ST_STEP_END, ST_KEYS, ST_SORT,
+       ST_CELLS, ST_GATHER, ST_COUNT };
+static const char* kStageNames[ST_COUNT] = {"update_dt", "visc", "collision", "pnd", "pressure", "dash",
+                                            "step_end", "cell_keys", "radix_sort", "cell_table", "gather"};
+
+static void mark(mps_handle* h, int tag) {
+    if (!h->prof_on) return;
+    if (h->prof_used == h->prof_ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->prof_ev.push_back(e);
+        h->prof_tag.push_back(0);
+    }
+    h->prof_tag[h->prof_used] = tag;
+    cudaEventRecord(h->prof_ev[h->prof_used], h->stream);
+    h->prof_used++;
+}
+
+// The reference's divideCell: keys (after the pending update), stable sort,
+// cell table, gather into the other buffer set.
+static void rebuild(mps_handle* h, int apply) {
+    cudaStream_t st = h->stream;
+    State& src = h->S[h->cur];
+    State& dst = h->S[h->cur ^ 1];
+    mark(h, ST_KEYS);
+    launch_cell_keys(src.pos, src.vel, h->tmp, apply, h->g, h->sc, h->sort.keys[0], h->sort.vals[0], h->cap, st);
+    mark(h, ST_SORT);
+    const int r = launch_radix_sort(h->sort, &h->sc->np, h->passes, h->cap, st);
+    mark(h, ST_CELLS);
+    launch_cell_start(h->sort.keys[r], h->g, h->sc, h->cell_start, h->cap, st);
+    mark(h, ST_GATHER);
+    launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st);
+    h->launches += 3 + 3 * h->passes;
+    h->cur ^= 1;
+}
+
+// One step in the reference's order.
+//  explicit: MPS_GPU_EXPL::step (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:277-339)
+//  semi:     MPS_CPU_EXPL::step (MPS_CAL_v4.0/MPS_CPU_EXPL.cpp:79-135)
+static void enqueue_step(mps_handle* h) {
+    cudaStream_t st = h->stream;
+    const uint32_t cap = h->cap;
+    h->launches = 0;
+    mark(h, ST_UPDATE_DT);
+    launch_update_dt(stage_args(h), cap, st);
+    mark(h, ST_VISC);
+    launch_visc(stage_args(h), cap, st);
+    rebuild(h, APPLY_SET_VEL);
+    mark(h, ST_COLLISION);
+    launch_collision(stage_args(h), cap, st);
+    rebuild(h, APPLY_ADD_VEL);
+    mark(h, ST_PND);
+    if (h->opt.method == MPS_METHOD_EXPLICIT) {
+        launch_pnd(stage_args(h), 1, 0, cap, st);
+        mark(h, ST_PRESSURE);
+        launch_dummy_press(stage_args(h), h->normal_id_of, h->index_of_id, cap, st);
+        h->launches += 2;
+    } else {
+        launch_pnd(stage_args(h), 0, 0, cap, st);
+        mark(h, ST_PRESSURE);
+        h->launches += 1 + ppe_enqueue(h->ppe, stage_args(h), h->opt, cap, st);
+    }
+    mark(h, ST_DASH);
+    launch_dash(stage_args(h), cap, st);
+    rebuild(h, APPLY_ADD_VEL);
+    mark(h, ST_STEP_END);
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        launch_update_dt(stage_args(h), cap, st);
+        h->launches += 1;
+    }
+    launch_step_end(h->sc, st);
+    h->launches += 5;
+}
+
+static mps_status read_status(mps_handle* h, Scalars* out) {
+    Scalars s;
+    CK(cudaMemcpyAsync(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (out) *out = s;
+    if (s.err & ERR_NAN) { h->err = "NaN in particle state"; return MPS_ERR_NAN; }
+    if (s.err & ERR_DT_TOO_SMALL) { h->err = "dt below dt_min"; return MPS_ERR_DT_TOO_SMALL; }
+    if (s.err & ERR_DEVICE_TIMEOUT) { h->err = "device wait timed out"; return MPS_ERR_DEVICE_TIMEOUT; }
+    if (s.err & ERR_CG_NOT_CONVERGED) { h->err = "PPE CG did not reach its tolerance"; return MPS_ERR_CG_NOT_CONVERGED; }
+    if (s.err & ERR_PARTICLE_OUT) { h->err = "particle left the grid"; return MPS_ERR_PARTICLE_OUT; }
+    return MPS_OK;
+}
+
+// ---------------------------------------------------------------- create
+extern "C" void mps_default_options(mps_options* o) {
+    memset(o, 0, sizeof *o);
+    o->method = MPS_METHOD_EXPLICIT;
+    o->arith = MPS_ARITH_EXACT;
+    o->device = 0;
+    o->use_graph = 1;
+    o->cg_tol = 1e-8;
+    o->cg_max_iter = 10000;
+    o->cg_check_every = 50;
+    o->precond = MPS_PRECOND_DIAGONAL;
+    o->capacity = 0;
+}
+
+static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint32_t nb2, uint32_t nb1,
+                        const float* pos3, const float* vel3, const float* press) {
+    h->prm = prm;
+    h->np0 = np;
+    h->nb2 = nb2;
+    h->nb1 = nb1;
+    h->cap = h->opt.capacity > np ? h->opt.capacity : np;
+    CK(cudaSetDevice(h->opt.device));
+    h->dev = h->opt.device;
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    int st = make_grid(prm, pos3, np, &h->hg, &h->err);
+    if (st != MPS_OK) return (mps_status)st;
+    Grid& g = h->g;
+    g.left = h->hg.left;
+    g.back = h->hg.back;
+    g.bottom = h->hg.bottom;
+    g.cell_size = h->hg.cell_size;
+    g.cdx = h->hg.cdx;
+    g.cdy = h->hg.cdy;
+    g.cdz = h->hg.cdz;
+    g.sheet = h->hg.sheet;
+    g.ncells = h->hg.ncells;
+    g.dim = h->hg.dim;
+    h->passes = sort_passes(g.ncells);
+    // reach (in cells) that covers sqrt(2) r0 for the dummy-to-wall search
+    {
+        double need = std::sqrt(2.0) * (double)prm.rzero;
+        int r = (int)std::ceil(need / (double)g.cell_size - 1e-12);
+        h->normal_reach = r < 1 ? 1 : r;
+    }
+
+    const uint32_t cap = h->cap;
+    for (int b = 0; b < 2; b++) {
+        State& s = h->S[b];
+        CK(dalloc(h, &s.pos, cap));
+        CK(dalloc(h, &s.vel, cap));
+        CK(dalloc(h, &s.press, cap));
+        CK(dalloc(h, &s.n, cap));
+        CK(dalloc(h, &s.id, cap));
+        CK(dalloc(h, &s.cell, cap));
+    }
+    CK(dalloc(h, &h->tmp, cap));
+    CK(dalloc(h, &h->index_of_id, cap));
+    CK(dalloc(h, &h->normal_id_of, cap));
+    CK(dalloc(h, &h->cell_start, (size_t)g.ncells + 1));
+    h->sort.tiles = sort_tiles(cap);
+    for (int b = 0; b < 2; b++) {
+        CK(dalloc(h, &h->sort.keys[b], cap));
+        CK(dalloc(h, &h->sort.vals[b], cap));
+    }
+    CK(dalloc(h, &h->sort.hist, (size_t)SORT_RADIX * h->sort.tiles));
+    CK(dalloc(h, &h->stage.pos3, 3 * (size_t)cap));
+    CK(dalloc(h, &h->stage.vel3, 3 * (size_t)cap));
+    CK(dalloc(h, &h->stage.press, cap));
+    CK(dalloc(h, &h->stage.n, cap));
+    CK(dalloc(h, &h->stage.id, cap));
+    CK(dalloc(h, &h->stage.type, cap));
+    CK(dalloc(h, &h->sc, 1));
+    CK(dalloc(h, &h->best, 1));
+    CK(dalloc(h, &h->lambda_dev, 1));
+
+    // upload in GEO.dat order: type from the b2 / b1 / fluid ranges
+    {
+        std::vector<float4> p4(np), v4(np);
+        std::vector<uint32_t> ids(np);
+        for (uint32_t i = 0; i < np; i++) {
+            const uint32_t t = i < nb2 ? T_DUMMY : (i < nb2 + nb1 ? T_WALL : T_FLUID);
+            float w;
+            memcpy(&w, &t, 4);
+            p4[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], w);
+            v4[i] = make_float4(vel3 ? vel3[3 * i] : 0.f, vel3 ? vel3[3 * i + 1] : 0.f, vel3 ? vel3[3 * i + 2] : 0.f, 0.f);
+            ids[i] = i;
+        }
+        State& s = h->S[0];
+        CK(cudaMemcpyAsync(s.pos, p4.data(), np * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(s.vel, v4.data(), np * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        if (press) CK(cudaMemcpyAsync(s.press, press, np * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(s.id, ids.data(), np * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        Scalars sc0;
+        memset(&sc0, 0, sizeof sc0);
+        sc0.np = np;
+        sc0.np_new = np;
+        sc0.dt = prm.dt_max;
+        CK(cudaMemcpyAsync(h->sc, &sc0, sizeof sc0, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+
+    // constants that do not depend on n0
+    Phys& P = h->P;
+    memset(&P, 0, sizeof P);
+    P.rzero = prm.rzero;
+    P.rlap = prm.rlap;
+    P.col_dis = prm.col_dis;
+    P.col_rate = prm.col_rate;
+    P.niu = prm.niu;
+    P.rho = prm.rho;
+    P.dt_max = prm.dt_max;
+    P.dt_min = prm.dt_min;
+    P.cfl_dp = prm.cfl * prm.dp;
+    P.beta = prm.beta;
+    P.g[0] = 0.0f;
+    P.g[1] = 0.0f;
+    P.g[2] = -9.81f;
+    P.dim_f = (float)prm.dim;
+    P.rzero_thr = rr_threshold(prm.rzero);
+    P.rlap_thr = rr_threshold(prm.rlap);
+    P.col_thr = rr_threshold(prm.col_dis);
+    P.rzero2 = prm.rzero * prm.rzero;
+
+    // MPS_GPU::Initial (MPS_CAL_expl_v1.0/MPS_GPU.cpp:63-115): divideCell, then calOnce.
+    rebuild(h, APPLY_NONE);
+    {
+        StageArgs a = stage_args(h);
+        launch_pnd(a, 0, 1, h->cap, h->stream);  // n of every particle
+        launch_nzero(h->S[h->cur].n, h->sc, h->best, h->cap, h->stream);
+        launch_lambda(a, h->best, h->lambda_dev, h->stream);
+        launch_normals(a, h->normal_reach, h->normal_id_of, h->cap, h->stream);
+        unsigned long long best = 0;
+        float lam = 0.f;
+        CK(cudaMemcpyAsync(&best, h->best, 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&lam, h->lambda_dev, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaGetLastError());
+        uint32_t nbits = (uint32_t)(best >> 32);
+        float n0;
+        memcpy(&n0, &nbits, 4);
+        if (!(n0 > 0.f)) {
+            h->err = "n0 is not positive: no particle has a neighbour within r0";
+            return MPS_ERR_INVALID;
+        }
+        derive_constants(prm, n0, lam, &h->hc);
+    }
+    P.nzero = h->hc.nzero;
+    P.one_over_nzero = h->hc.one_over_nzero;
+    P.one_over_alpha = h->hc.one_over_alpha;
+    P.one_over_rho = h->hc.one_over_rho;
+    P.c_lap = h->hc.c_lap;
+    P.lambda = h->hc.lambda;
+    P.alpha = h->hc.alpha;
+    P.one_over_dt_fixed = h->hc.one_over_dt;
+
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
+        if (e != MPS_OK) return (mps_status)e;
+    }
+    Scalars s;
+    return read_status(h, &s);
+}
+
+static mps_status create_common(mps_handle** out, const mps_options* opt) {
+    mps_handle* h = new mps_handle();
+    if (opt) h->opt = *opt;
+    else mps_default_options(&h->opt);
+    if (h->opt.cg_max_iter <= 0) h->opt.cg_max_iter = 10000;
+    if (h->opt.cg_check_every <= 0) h->opt.cg_check_every = 50;
+    if (h->opt.cg_tol <= 0) h->opt.cg_tol = 1e-8;
+    *out = h;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_create(const char* input_dat, const char* geo_dat, const mps_options* opt,
+                                 mps_handle** out) {
+    if (!out || !input_dat || !geo_dat) return MPS_ERR_INVALID;
+    *out = nullptr;
+    mps_handle* h;
+    create_common(&h, opt);
+    mps_params p;
+    int st = read_input_dat(input_dat, &p, &h->err);
+    Geo geo;
+    if (st == MPS_OK) st = read_geo_dat(geo_dat, &geo, &h->err);
+    if (st == MPS_OK)
+        st = setup(h, p, geo.np, geo.nb2, geo.nb1, geo.pos.data(), geo.vel.data(), geo.press.data());
+    *out = h;  // returned even on error so that mps_last_error can explain
+    return (mps_status)st;
+}
+
+extern "C" mps_status mps_create_from_arrays(const mps_params* p, uint32_t np, uint32_t nb2, uint32_t nb1,
+                                             const float* pos3, const float* vel3, const float* press,
+                                             const mps_options* opt, mps_handle** out) {
+    if (!out || !p || !pos3 || np == 0 || nb2 + nb1 > np) return MPS_ERR_INVALID;
+    mps_handle* h;
+    create_common(&h, opt);
+    int st = setup(h, *p, np, nb2, nb1, pos3, vel3, press);
+    *out = h;
+    return (mps_status)st;
+}
+
+extern "C" void mps_destroy(mps_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int b = 0; b < 2; b++)
+        if (h->graph[b]) cudaGraphExecDestroy(h->graph[b]);
+    for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
+    ppe_free(h->ppe);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+extern "C" const char* mps_last_error(mps_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+// ---------------------------------------------------------------- stepping
+static mps_status capture_graph(mps_handle* h, int parity) {
+    cudaGraph_t g;
+    const int saved = h->cur;
+    h->cur = parity;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    const int after = h->cur;
+    h->cur = saved;
+    if (e != cudaSuccess) {
+        h->err = std::string("graph capture: ") + cudaGetErrorString(e);
+        return MPS_ERR_CUDA;
+    }
+    if (after != (parity ^ 1)) {
+        cudaGraphDestroy(g);
+        h->err = "unexpected buffer parity after a step";
+        return MPS_ERR_INVALID;
+    }
+    e = cudaGraphInstantiate(&h->graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+        return MPS_ERR_CUDA;
+    }
+    return MPS_OK;
+}
+
+static mps_status step_async(mps_handle* h, int nsteps) {
+    CK(cudaSetDevice(h->dev));
+    for (int k = 0; k < nsteps; k++) {
+        if (h->opt.use_graph && h->opt.method == MPS_METHOD_EXPLICIT) {
+            const int p = h->cur;
+            if (!h->graph[p]) {
+                mps_status s = capture_graph(h, p);
+                if (s != MPS_OK) return s;
+            }
+            CK(cudaGraphLaunch(h->graph[p], h->stream));
+            h->cur ^= 1;
+        } else {
+            enqueue_step(h);
+        }
+    }
+    CK(cudaGetLastError());
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_step(mps_handle* h, int nsteps, mps_step_stats* stats) {
+    if (!h || nsteps < 0) return MPS_ERR_INVALID;
+    if (h->pending_apply != APPLY_NONE) {
+        h->err = "a stage update is pending; run stage 2 (divideCell) first";
+        return MPS_ERR_INVALID;
+    }
+    CK(cudaEventRecord(h->ev0, h->stream));
+    mps_status s = step_async(h, nsteps);
+    if (s != MPS_OK) return s;
+    CK(cudaEventRecord(h->ev1, h->stream));
+    Scalars sc;
+    s = read_status(h, &sc);
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->np = sc.np;
+        stats->nexcl = sc.nexcl;
+        stats->step = sc.step;
+        stats->time = sc.time;
+        stats->dt = sc.dt;
+        stats->cg_iters = sc.cg_iters;
+        stats->cg_relres = sc.cg_relres;
+        stats->status = (int)s;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        stats->ms = ms;
+    }
+    return s;
+}
+
+extern "C" mps_status mps_step_async(mps_handle* h, int nsteps) {
+    if (!h || nsteps < 0) return MPS_ERR_INVALID;
+    if (h->pending_apply != APPLY_NONE) {
+        h->err = "a stage update is pending; run stage 2 (divideCell) first";
+        return MPS_ERR_INVALID;
+    }
+    return step_async(h, nsteps);
+}
+
+extern "C" mps_status mps_phase(mps_handle* h, int phase) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    cudaStream_t st = h->stream;
+    const uint32_t cap = h->cap;
+    switch (phase) {
+        case 0: launch_update_dt(stage_args(h), cap, st); break;
+        case 1: launch_visc(stage_args(h), cap, st); h->pending_apply = APPLY_SET_VEL; break;
+        case 2: rebuild(h, h->pending_apply); h->pending_apply = APPLY_NONE; break;
+        case 3: launch_collision(stage_args(h), cap, st); h->pending_apply = APPLY_ADD_VEL; break;
+        case 4: launch_pnd(stage_args(h), 0, 0, cap, st); break;
+        case 5:
+            launch_pnd(stage_args(h), 1, 0, cap, st);
+            launch_dummy_press(stage_args(h), h->normal_id_of, h->index_of_id, cap, st);
+            break;
+        case 6: launch_dash(stage_args(h), cap, st); h->pending_apply = APPLY_ADD_VEL; break;
+        case 7:
+            if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) return MPS_ERR_INVALID;
+            ppe_enqueue(h->ppe, stage_args(h), h->opt, cap, st);
+            break;
+        default: return MPS_ERR_INVALID;
+    }
+    CK(cudaGetLastError());
+    return read_status(h, nullptr);
+}
+
+// ---------------------------------------------------------------- getters
+static mps_status counts(mps_handle* h, Scalars* s) { return read_status(h, s) == MPS_ERR_CUDA ? MPS_ERR_CUDA : MPS_OK; }
+
+extern "C" mps_status mps_get_counts(mps_handle* h, uint32_t* np, uint32_t* nb2, uint32_t* nb1, uint32_t* nexcl) {
+    if (!h) return MPS_ERR_INVALID;
+    Scalars s;
+    if (counts(h, &s) != MPS_OK) return MPS_ERR_CUDA;
+    if (np) *np = s.np;
+    if (nb2) *nb2 = h->nb2;
+    if (nb1) *nb1 = h->nb1;
+    if (nexcl) *nexcl = s.nexcl;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_get_state(mps_handle* h, uint32_t* id, uint32_t* type, float* pos3, float* vel3,
+                                    float* press, float* n, int order) {
+    if (!h || (order != MPS_ORDER_SORTED && order != MPS_ORDER_BY_ID)) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    Scalars s;
+    if (counts(h, &s) != MPS_OK) return MPS_ERR_CUDA;
+    const int by_id = order == MPS_ORDER_BY_ID;
+    const size_t cnt = by_id ? h->np0 : s.np;
+    if (cnt == 0) return MPS_OK;
+    cudaStream_t st = h->stream;
+    launch_unpack(h->S[h->cur], h->stage, by_id, h->np0, h->sc, h->cap, st);
+    if (id) CK(cudaMemcpyAsync(id, h->stage.id, cnt * 4, cudaMemcpyDeviceToHost, st));
+    if (type) CK(cudaMemcpyAsync(type, h->stage.type, cnt * 4, cudaMemcpyDeviceToHost, st));
+    if (pos3) CK(cudaMemcpyAsync(pos3, h->stage.pos3, cnt * 12, cudaMemcpyDeviceToHost, st));
+    if (vel3) CK(cudaMemcpyAsync(vel3, h->stage.vel3, cnt * 12, cudaMemcpyDeviceToHost, st));
+    if (press) CK(cudaMemcpyAsync(press, h->stage.press, cnt * 4, cudaMemcpyDeviceToHost, st));
+    if (n) CK(cudaMemcpyAsync(n, h->stage.n, cnt * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_set_state(mps_handle* h, const float* pos3, const float* vel3, const float* press,
+                                    const float* n) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    Scalars s;
+    if (counts(h, &s) != MPS_OK) return MPS_ERR_CUDA;
+    const size_t np = s.np;
+    if (np == 0) return MPS_OK;
+    cudaStream_t st = h->stream;
+    int mask = 0;
+    if (pos3) { CK(cudaMemcpyAsync(h->stage.pos3, pos3, np * 12, cudaMemcpyHostToDevice, st)); mask |= 1; }
+    if (vel3) { CK(cudaMemcpyAsync(h->stage.vel3, vel3, np * 12, cudaMemcpyHostToDevice, st)); mask |= 2; }
+    if (press) { CK(cudaMemcpyAsync(h->stage.press, press, np * 4, cudaMemcpyHostToDevice, st)); mask |= 4; }
+    if (n) { CK(cudaMemcpyAsync(h->stage.n, n, np * 4, cudaMemcpyHostToDevice, st)); mask |= 8; }
+    if (mask) launch_pack(h->S[h->cur], h->stage, mask, h->sc, h->cap, st);
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_get_cell_tables(mps_handle* h, uint32_t* cell_of, uint32_t* start, uint32_t* end) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    Scalars s;
+    if (counts(h, &s) != MPS_OK) return MPS_ERR_CUDA;
+    const uint32_t nc = h->g.ncells;
+    std::vector<uint32_t> cs(nc + 1);
+    CK(cudaMemcpyAsync(cs.data(), h->cell_start, (nc + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (cell_of && s.np)
+        CK(cudaMemcpyAsync(cell_of, h->S[h->cur].cell, s.np * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t c = 0; c < nc; c++) {
+        if (start) start[c] = cs[c];
+        if (end) end[c] = cs[c + 1];
+    }
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_get_grid(mps_handle* h, mps_grid* g) {
+    if (!h || !g) return MPS_ERR_INVALID;
+    g->left = h->g.left;
+    g->back = h->g.back;
+    g->bottom = h->g.bottom;
+    g->cell_size = h->g.cell_size;
+    g->cdx = h->g.cdx;
+    g->cdy = h->g.cdy;
+    g->cdz = h->g.cdz;
+    g->ncells = h->g.ncells;
+    g->dim = h->g.dim;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
+    if (!h || !o) return MPS_ERR_INVALID;
+    Scalars s;
+    mps_status st = read_status(h, &s);
+    if (st == MPS_ERR_CUDA) return st;
+    for (int k = 0; k < 16; k++) o[k] = 0.0;
+    o[0] = h->hc.nzero;
+    o[1] = h->hc.lambda;
+    o[2] = s.dt;
+    o[3] = s.time;
+    o[4] = h->hc.c_lap;
+    o[5] = h->hc.one_over_alpha;
+    o[6] = h->hc.alpha;
+    o[7] = s.cg_iters;
+    o[8] = s.cg_relres;
+    o[9] = s.step;
+    o[10] = (double)st;
+    o[11] = h->g.ncells;
+    o[12] = h->launches;
+    return MPS_OK;
+}
+
+extern "C" const char* mps_stage_name(int k) { return (k >= 0 && k < ST_COUNT) ? kStageNames[k] : ""; }
+
+extern "C" mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int max_stages,
+                                        int* nstages) {
+    if (!h || nsteps < 0 || !stage_ms) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    for (int k = 0; k < max_stages; k++) stage_ms[k] = 0.0;
+    if (nstages) *nstages = ST_COUNT;
+    for (int s = 0; s < nsteps; s++) {
+        h->prof_on = true;
+        h->prof_used = 0;
+        enqueue_step(h);
+        mark(h, -1);
+        h->prof_on = false;
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaGetLastError());
+        for (size_t k = 0; k + 1 < h->prof_used; k++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->prof_ev[k], h->prof_ev[k + 1]);
+            const int t = h->prof_tag[k];
+            if (t >= 0 && t < max_stages) stage_ms[t] += ms;
+        }
+    }
+    return read_status(h, nullptr);
+}
+
+extern "C" mps_status mps_get_normal_ids(mps_handle* h, uint32_t* normal_id) {
+    if (!h || !normal_id) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaMemcpyAsync(normal_id, h->normal_id_of, h->np0 * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_get_stream(mps_handle* h, void** stream) {
+    if (!h || !stream) return MPS_ERR_INVALID;
+    *stream = (void*)h->stream;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_write_case(mps_handle* h, const char* path, int format) {
+    if (!h || !path || (format != 0 && format != 1)) return MPS_ERR_INVALID;
+    uint32_t np = 0;
+    mps_status s = mps_get_counts(h, &np, nullptr, nullptr, nullptr);
+    if (s != MPS_OK) return s;
+    std::vector<uint32_t> id(np), type(np);
+    std::vector<float> pos(3 * (size_t)np), vel(3 * (size_t)np), pr(np);
+    s = mps_get_state(h, id.data(), type.data(), pos.data(), vel.data(), pr.data(), nullptr, MPS_ORDER_SORTED);
+    if (s != MPS_OK) return s;
+    return (mps_status)write_case_text(path, format, np, id.data(), type.data(), pos.data(), vel.data(), pr.data());
+}
+
+// MPS_GPU_EXPL::mps_cal (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:216-272): output
+// whenever time - threshold >= 0, threshold += tout; then a step.
+extern "C" mps_status mps_run(mps_handle* h, const char* out_dir) {
+    if (!h) return MPS_ERR_INVALID;
+    float threshold = 0.0f;
+    int count = 0;
+    for (;;) {
+        Scalars s;
+        mps_status st = read_status(h, &s);
+        if (st != MPS_OK) return st;
+        if (!(s.time < h->prm.tt)) break;
+        if (s.time - threshold >= 0.0f) {
+            if (out_dir) {
+                char path[4096];
+                snprintf(path, sizeof path, "%s/%04d.out", out_dir, count);
+                st = mps_write_case(h, path, h->opt.method == MPS_METHOD_EXPLICIT ? 0 : 1);
+                if (st != MPS_OK) return st;
+            }
+            threshold += h->prm.tout;
+            count++;
+        }
+        st = step_async(h, 1);
+        if (st != MPS_OK) return st;
+    }
+    return MPS_OK;
+}
+
+// ---------------------------------------------------------------- primitive
+extern "C" mps_status mps_cell_sort_dev(const float* pos4_dev, uint32_t n, const mps_grid* gg, uint32_t* perm_dev,
+                                        uint32_t* cell_of_dev, uint32_t* start_dev, uint32_t* end_dev,
+                                        uint32_t* n_in_grid_dev, void* stream) {
+    if (!gg || (n && (!pos4_dev || !perm_dev || !cell_of_dev)) || !start_dev || !end_dev || !n_in_grid_dev)
+        return MPS_ERR_INVALID;
+    if (gg->ncells == 0 || gg->ncells >= 0x7fffffffu) return MPS_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    Grid g;
+    g.left = gg->left;
+    g.back = gg->back;
+    g.bottom = gg->bottom;
+    g.cell_size = gg->cell_size;
+    g.cdx = gg->cdx;
+    g.cdy = gg->cdy;
+    g.cdz = gg->cdz;
+    g.sheet = gg->cdx * gg->cdy;
+    g.ncells = gg->ncells;
+    g.dim = gg->dim;
+    const uint32_t tiles = sort_tiles(n > 0 ? n : 1);
+    SortScratch s;
+    s.tiles = tiles;
+    void* blk = nullptr;
+    const size_t nk = (size_t)(n > 0 ? n : 1);
+    const size_t bytes = 4 * nk * sizeof(uint32_t) + (size_t)SORT_RADIX * tiles * sizeof(uint32_t) +
+                         ((size_t)g.ncells + 1) * sizeof(uint32_t) + sizeof(uint32_t) + 256;
+    if (cudaMalloc(&blk, bytes) != cudaSuccess) return MPS_ERR_CUDA;
+    uint32_t* b = (uint32_t*)blk;
+    s.keys[0] = b;
+    s.vals[0] = b + nk;
+    s.keys[1] = b + 2 * nk;
+    s.vals[1] = b + 3 * nk;
+    s.hist = b + 4 * nk;
+    uint32_t* cs = s.hist + (size_t)SORT_RADIX * tiles;
+    uint32_t* n_dev = cs + g.ncells + 1;
+    cudaMemcpyAsync(n_dev, &n, sizeof n, cudaMemcpyHostToDevice, st);
+    launch_cell_keys_plain((const float4*)pos4_dev, n, g, s.keys[0], s.vals[0], st);
+    const int r = launch_radix_sort(s, n_dev, sort_passes(g.ncells), n, st);
+    launch_cell_start_plain(s.keys[r], n, g, cs, n_in_grid_dev, st);
+    if (n) {
+        cudaMemcpyAsync(perm_dev, s.vals[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(cell_of_dev, s.keys[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    }
+    launch_cell_end_from_start(cs, g.ncells, start_dev, end_dev, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(blk);
+    if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return MPS_ERR_CUDA;
+    return MPS_OK;
+}

@@ -1,0 +1,258 @@
+// cellsort.cu -- cell keys, stable radix sort by cell, cell tables.
+//
+// Replaces MPS_GPU::divideCell (MPS_CAL_expl_v1.0/MPS_GPU.cpp:248-331): the
+// reference bins particles on the host with an atomic count, a serial prefix
+// sum and a serial stable counting-sort rank.  Here the same stable order
+// (particles grouped by cell, ascending previous index inside a cell) comes
+// from an LSD radix sort on the cell id with the previous index as value.
+#include "cellsort.cuh"
+
+namespace mpsb {
+
+// ---------------------------------------------------------------- keys
+__global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                   const float4* __restrict__ tmp, int apply, Grid g,
+                                                   Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
+                                                   uint32_t* __restrict__ vals) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    if (apply != APPLY_NONE && ptype(p) == T_FLUID) {
+        const float dt = sc->dt;
+        float4 t = tmp[i];
+        // x = x + dt * tmp, in float with one rounding per operation
+        p.x = __fadd_rn(p.x, __fmul_rn(dt, t.x));
+        p.y = __fadd_rn(p.y, __fmul_rn(dt, t.y));
+        p.z = __fadd_rn(p.z, __fmul_rn(dt, t.z));
+    }
+    bool nan_flag = false;
+    uint32_t k = cell_of_pos(g, p.x, p.y, p.z, &nan_flag);
+    if (nan_flag) atomicOr(&sc->err, ERR_NAN);
+    keys[i] = k;
+    vals[i] = i;
+}
+
+__global__ void __launch_bounds__(256) k_cell_keys_plain(const float4* __restrict__ pos, uint32_t n, Grid g,
+                                                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    bool nan_flag = false;
+    keys[i] = cell_of_pos(g, p.x, p.y, p.z, &nan_flag);
+    vals[i] = i;
+}
+
+// ---------------------------------------------------------------- radix sort
+// Upsweep: digit histogram of each tile, stored digit-major
+// (hist[d * tiles + tile]) so that one exclusive scan over hist yields the
+// global output offset of (digit, tile) for a stable LSD pass.
+__global__ void __launch_bounds__(SORT_THREADS) k_radix_upsweep(const uint32_t* __restrict__ keys,
+                                                                const uint32_t* __restrict__ n_dev, int shift,
+                                                                uint32_t* __restrict__ hist, uint32_t tiles) {
+    __shared__ uint32_t h[SORT_RADIX];
+    const uint32_t n = *n_dev;
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) h[d] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * SORT_TILE;
+    if (base < n) {
+#pragma unroll
+        for (int k = 0; k < SORT_ITEMS; k++) {
+            uint32_t idx = base + k * SORT_THREADS + threadIdx.x;
+            if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 0xffu], 1u);
+        }
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) hist[d * tiles + blockIdx.x] = h[d];
+}
+
+// Exclusive scan of `total` counters by one block.
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, uint32_t total) {
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = threadIdx.x * per;
+    const uint32_t b1 = min(total, b0 + per);
+    uint32_t s = 0;
+    for (uint32_t k = b0; k < b1; k++) s += a[k];
+    // block exclusive scan of s
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t v = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        warp_sums[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    uint32_t run = v - s + (warp > 0 ? warp_sums[warp - 1] : 0u);
+    for (uint32_t k = b0; k < b1; k++) {
+        uint32_t t = a[k];
+        a[k] = run;
+        run += t;
+    }
+}
+
+// Downsweep: stable rank of every key inside its tile and scatter.
+// Warp w of the block owns keys [tile + 256w, tile + 256w + 256) and walks
+// them 32 at a time in index order; __match_any_sync groups equal digits in a
+// round, and the group's running count in warp_hist[w][digit] gives each key
+// its rank among equal digits before it in the warp.  An exclusive scan over
+// warps per digit then orders the warps, and the upsweep scan orders tiles.
+__global__ void __launch_bounds__(SORT_THREADS) k_radix_downsweep(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ n_dev, int shift,
+    uint32_t tiles) {
+    constexpr int WARPS = SORT_THREADS / 32;
+    __shared__ uint32_t warp_hist[WARPS][SORT_RADIX];
+    __shared__ uint32_t tile_off[SORT_RADIX];
+    const uint32_t n = *n_dev;
+    const uint32_t base = blockIdx.x * SORT_TILE;
+    if (base >= n) return;  // the whole block exits together
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < WARPS * SORT_RADIX; k += SORT_THREADS) (&warp_hist[0][0])[k] = 0;
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) tile_off[d] = hist[d * tiles + blockIdx.x];
+    __syncthreads();
+
+    uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
+    const uint32_t lt_mask = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; r++) {
+        const uint32_t idx = base + warp * (32 * SORT_ITEMS) + r * 32 + lane;
+        const bool valid = idx < n;
+        key[r] = valid ? keys_in[idx] : 0u;
+        val[r] = valid ? vals_in[idx] : 0u;
+        const uint32_t d = valid ? ((key[r] >> shift) & 0xffu) : 0x100u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t prev = 0;
+        if (lane == leader && valid) {
+            prev = warp_hist[warp][d];
+            warp_hist[warp][d] = prev + __popc(peers);
+        }
+        prev = __shfl_sync(0xffffffffu, prev, leader);
+        rank[r] = prev + __popc(peers & lt_mask);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive scan across warps for each digit
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < WARPS; w++) {
+            uint32_t t = warp_hist[w][d];
+            warp_hist[w][d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; r++) {
+        const uint32_t idx = base + warp * (32 * SORT_ITEMS) + r * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[r] >> shift) & 0xffu;
+            const uint32_t dst = tile_off[d] + warp_hist[warp][d] + rank[r];
+            keys_out[dst] = key[r];
+            vals_out[dst] = val[r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- cell tables
+// cell_start[c] = first sorted position whose key is >= c, for c in
+// [0, ncells]; equal to the reference's serial prefix sum of per-cell counts
+// (MPS_CAL_expl_v1.0/MPS_GPU.cpp:293-297), with cell_end[c] = cell_start[c+1]
+// and cell_start[ncells] = number of particles inside the grid.
+__device__ __forceinline__ void cell_start_fill(const uint32_t* keys, uint32_t n, uint32_t ncells, uint32_t p,
+                                                uint32_t* cell_start) {
+    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
+    long long cur = p < n ? (long long)keys[p] : (long long)ncells;
+    if (cur > (long long)ncells) cur = ncells;
+    for (long long c = prev + 1; c <= cur; c++) cell_start[c] = p;
+}
+
+__global__ void __launch_bounds__(256) k_cell_start(const uint32_t* __restrict__ keys, Grid g,
+                                                    Scalars* __restrict__ sc, uint32_t* __restrict__ cell_start) {
+    const uint32_t n = sc->np;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    cell_start_fill(keys, n, g.ncells, p, cell_start);
+    // the thread whose range reaches c = ncells knows the in-grid count
+    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
+    long long cur = p < n ? (long long)keys[p] : (long long)g.ncells;
+    if (prev < (long long)g.ncells && cur >= (long long)g.ncells) sc->np_new = p;
+}
+
+__global__ void __launch_bounds__(256) k_cell_start_plain(const uint32_t* __restrict__ keys, uint32_t n, Grid g,
+                                                          uint32_t* __restrict__ cell_start,
+                                                          uint32_t* __restrict__ n_in_grid) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    cell_start_fill(keys, n, g.ncells, p, cell_start);
+    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
+    long long cur = p < n ? (long long)keys[p] : (long long)g.ncells;
+    if (prev < (long long)g.ncells && cur >= (long long)g.ncells) *n_in_grid = p;
+}
+
+__global__ void k_start_end(const uint32_t* __restrict__ cs, uint32_t ncells, uint32_t* __restrict__ start,
+                            uint32_t* __restrict__ end) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    start[c] = cs[c];
+    end[c] = cs[c + 1];
+}
+
+// ---------------------------------------------------------------- launchers
+static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
+                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st) {
+    k_cell_keys<<<blocks_for(cap, 256), 256, 0, st>>>(pos, vel, tmp, apply, g, sc, keys, vals);
+}
+
+int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st) {
+    (void)cap;
+    int cur = 0;
+    for (int p = 0; p < passes; p++) {
+        const int shift = 8 * p;
+        k_radix_upsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], n_dev, shift, s.hist, s.tiles);
+        k_scan_exclusive<<<1, 1024, 0, st>>>(s.hist, SORT_RADIX * s.tiles);
+        k_radix_downsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], s.vals[cur], s.keys[cur ^ 1],
+                                                             s.vals[cur ^ 1], s.hist, n_dev, shift, s.tiles);
+        cur ^= 1;
+    }
+    return cur;
+}
+
+void launch_cell_start(const uint32_t* keys_sorted, const Grid& g, Scalars* sc, uint32_t* cell_start, uint32_t cap,
+                       cudaStream_t st) {
+    k_cell_start<<<blocks_for(cap + 1, 256), 256, 0, st>>>(keys_sorted, g, sc, cell_start);
+}
+
+void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32_t* keys, uint32_t* vals,
+                            cudaStream_t st) {
+    if (n == 0) return;
+    k_cell_keys_plain<<<blocks_for(n, 256), 256, 0, st>>>(pos, n, g, keys, vals);
+}
+
+void launch_cell_start_plain(const uint32_t* keys_sorted, uint32_t n, const Grid& g, uint32_t* cell_start,
+                             uint32_t* n_in_grid, cudaStream_t st) {
+    k_cell_start_plain<<<blocks_for(n + 1, 256), 256, 0, st>>>(keys_sorted, n, g, cell_start, n_in_grid);
+}
+
+void launch_cell_end_from_start(const uint32_t* cell_start, uint32_t ncells, uint32_t* start_out, uint32_t* end_out,
+                                cudaStream_t st) {
+    if (ncells == 0) return;
+    k_start_end<<<blocks_for(ncells, 256), 256, 0, st>>>(cell_start, ncells, start_out, end_out);
+}
+
+}  // namespace mpsb

@@ -1,0 +1,60 @@
+// cellsort.cuh -- the neighbour-search rebuild (the reference's divideCell).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mps_device.cuh"
+
+namespace mpsb {
+
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_ITEMS = 8;
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;  // 2048 keys per tile
+constexpr int SORT_RADIX = 256;
+
+inline uint32_t sort_tiles(uint32_t cap) { return (cap + SORT_TILE - 1) / SORT_TILE; }
+
+// Number of 8-bit passes to sort keys in [0, ncells] (ncells is the
+// out-of-grid sentinel).
+inline int sort_passes(uint32_t ncells) {
+    int bits = 0;
+    while (bits < 32 && (uint64_t(1) << bits) <= ncells) bits++;
+    return (bits + 7) / 8;
+}
+
+// Scratch of one sort, sized for `cap` keys.
+struct SortScratch {
+    uint32_t* keys[2];
+    uint32_t* vals[2];
+    uint32_t* hist;  // SORT_RADIX * tiles
+    uint32_t tiles;
+};
+
+// Pending particle update applied by the rebuild (the second phase of the
+// reference's two-phase stages, which divideCell always follows).
+enum ApplyMode : int {
+    APPLY_NONE = 0,
+    APPLY_SET_VEL = 1,  // fluid: u = tmp, x = x + dt*tmp      (calVisc_expl)
+    APPLY_ADD_VEL = 2,  // fluid: u = u + tmp, x = x + dt*tmp  (collision, calDash)
+};
+
+// Launchers (all asynchronous on `st`).
+// Stage 1: cell key of every active particle (after the pending update).
+void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
+                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st);
+// Stage 2: stable LSD radix sort of (keys[0], vals[0]) over sc->np keys;
+// returns the buffer index (0/1) that holds the result.
+int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st);
+// Stage 3: cell_start[0..ncells] from the sorted keys; writes sc->np_new.
+void launch_cell_start(const uint32_t* keys_sorted, const Grid& g, Scalars* sc, uint32_t* cell_start,
+                       uint32_t cap, cudaStream_t st);
+
+// Same pieces with n given on the host (for the device-pointer primitive).
+void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32_t* keys, uint32_t* vals,
+                            cudaStream_t st);
+void launch_cell_start_plain(const uint32_t* keys_sorted, uint32_t n, const Grid& g, uint32_t* cell_start,
+                             uint32_t* n_in_grid, cudaStream_t st);
+void launch_cell_end_from_start(const uint32_t* cell_start, uint32_t ncells, uint32_t* start_out,
+                                uint32_t* end_out, cudaStream_t st);
+
+}  // namespace mpsb

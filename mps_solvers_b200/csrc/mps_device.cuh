@@ -1,0 +1,125 @@
+// mps_device.cuh -- device-side types and helpers shared by the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpsb {
+
+// Cell grid of the reference's cell list (MPS_CAL_expl_v1.0/MPS.cpp:567-642).
+struct Grid {
+    float left, back, bottom, cell_size;
+    uint32_t cdx, cdy, cdz, sheet, ncells;
+    int dim;
+};
+
+// Per-scene constants, fixed after initialisation.
+struct Phys {
+    float rzero, rlap, col_dis, col_rate, niu, rho, one_over_rho;
+    float nzero, one_over_nzero, one_over_alpha, c_lap, dim_f;
+    float dt_max, dt_min, cfl_dp, beta;
+    float g[3];
+    // prefilter thresholds on r^2: any r^2 at or above them is certainly
+    // outside the corresponding test (see host set-up)
+    float rzero_thr, rlap_thr, col_thr, rzero2;
+    // PPE (semi-implicit)
+    float lambda, alpha, one_over_dt_fixed;
+};
+
+// Device-resident per-step scalars (one instance per handle).
+struct Scalars {
+    float dt;              // dt of the current step
+    float time;            // simulated time
+    uint32_t np;           // active particles (the reference's i_np)
+    uint32_t np_new;       // active particles after the running rebuild
+    uint32_t nexcl;        // total dropped particles
+    uint32_t vmax2_bits;   // max |u|^2 of the running update_dt (float bits)
+    uint32_t err;          // sticky error bits (ERR_*)
+    uint32_t done_blocks;  // last-block counter for reductions
+    int step;
+    int cg_iters;
+    double cg_relres;
+    double pad[4];
+};
+
+enum : uint32_t {
+    ERR_DT_TOO_SMALL = 1u,
+    ERR_NAN = 2u,
+    ERR_PARTICLE_OUT = 4u,
+    ERR_CG_NOT_CONVERGED = 8u,
+    ERR_DEVICE_TIMEOUT = 16u,
+};
+
+// particle types (pos.w carries the type as its bit pattern)
+enum : uint32_t { T_FLUID = 0, T_WALL = 1, T_DUMMY = 2, T_EXCL = 3 };
+
+__device__ __forceinline__ uint32_t ptype(const float4& p) { return __float_as_uint(p.w); }
+
+// ---- arithmetic: EX = true evaluates in IEEE float, one rounding per
+// operation, no contraction (the reference's SSE evaluation); EX = false lets
+// the compiler fuse and uses approximate reciprocals.
+template <bool EX> __device__ __forceinline__ float fmul(float a, float b) { return EX ? __fmul_rn(a, b) : a * b; }
+template <bool EX> __device__ __forceinline__ float fadd(float a, float b) { return EX ? __fadd_rn(a, b) : a + b; }
+template <bool EX> __device__ __forceinline__ float fsub(float a, float b) { return EX ? __fsub_rn(a, b) : a - b; }
+template <bool EX> __device__ __forceinline__ float fdiv(float a, float b) { return EX ? __fdiv_rn(a, b) : __fdividef(a, b); }
+
+// r.r summed x, y, z in that order (real3 operator*, typedef.h:103-106)
+template <bool EX> __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return fadd<EX>(fadd<EX>(fmul<EX>(ax, bx), fmul<EX>(ay, by)), fmul<EX>(az, bz));
+}
+
+// d_weight(re, sqrt(rr)) = re/r - 1 for r < re (MPS_CAL_expl_v1.0/MPS.cpp:412-417),
+// given rr below the prefilter threshold.  Returns 0 outside.
+template <bool EX> __device__ __forceinline__ float weight_rr(float re, float rr) {
+    if (EX) {
+        float r = __fsqrt_rn(rr);
+        return r < re ? __fsub_rn(__fdiv_rn(re, r), 1.0f) : 0.0f;
+    } else {
+        return rr < re * re ? fmaf(re, rsqrtf(rr), -1.0f) : 0.0f;
+    }
+}
+
+// Cell of a position: (x - left) / cell_size truncated through a signed 64-bit
+// integer and kept to 32 bits, as the reference's `integer c = expr;` does on
+// x86-64 (MPS_CAL_expl_v1.0/MPS_GPU.cpp:263-266).  Returns g.ncells (the
+// sentinel that sorts last) when the particle is outside the grid.
+__device__ __forceinline__ uint32_t cell_of_pos(const Grid& g, float x, float y, float z, bool* nan_flag) {
+    if (!(x == x) || !(y == y) || !(z == z)) {
+        *nan_flag = true;
+        return g.ncells;
+    }
+    uint32_t cx = (uint32_t)(long long)__fdiv_rn(__fsub_rn(x, g.left), g.cell_size);
+    uint32_t cy = (uint32_t)(long long)__fdiv_rn(__fsub_rn(y, g.back), g.cell_size);
+    uint32_t cz = (uint32_t)(long long)__fdiv_rn(__fsub_rn(z, g.bottom), g.cell_size);
+    if (cx >= g.cdx || cy >= g.cdy || cz >= g.cdz) return g.ncells;
+    return cz * g.sheet + cy * g.cdx + cx;
+}
+
+// The particles of the reference's 27 linked cells (MPS_GPU::makeLink,
+// MPS_CAL_expl_v1.0/MPS_GPU.cpp:168-243) as 9 rows (3 in 2D): row (dz, dy)
+// covers cells c0-1, c0, c0+1 with c0 = c + dz*sheet + dy*cdx, each kept when
+// its id (with unsigned wrap) is below ncells, exactly the reference's test.
+// The kept cells are consecutive, so their particles are one index range;
+// rows come in the reference's order, so visiting rows in order and indices
+// ascending reproduces the reference's summation order.
+struct RowRange { uint32_t lo, hi; };
+
+__device__ __forceinline__ RowRange link_row(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
+                                             int row) {
+    int dz, dy;
+    if (g.dim == 3) { dz = row / 3 - 1; dy = row % 3 - 1; }
+    else { dz = 0; dy = row - 1; }
+    uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
+    uint32_t a = c0 - 1u, b = c0 + 1u;
+    bool va = a < g.ncells, v0 = c0 < g.ncells, vb = b < g.ncells;
+    RowRange r{0u, 0u};
+    uint32_t first, last;
+    if (va) first = a; else if (v0) first = c0; else if (vb) first = b; else return r;
+    if (vb) last = b; else if (v0) last = c0; else last = a;
+    r.lo = __ldg(cell_start + first);
+    r.hi = __ldg(cell_start + last + 1u);
+    return r;
+}
+
+__device__ __forceinline__ int link_rows(const Grid& g) { return g.dim == 3 ? 9 : 3; }
+
+}  // namespace mpsb

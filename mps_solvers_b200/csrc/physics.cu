@@ -1,0 +1,501 @@
+// physics.cu -- particle stages of the MPS step on the sorted particles.
+//
+// One thread per particle walks the reference's 27 linked cells as 9 index
+// ranges (link_row) in the reference's order.  Every stage writes its result
+// to a separate array (tmp / n / press) and never to the positions or
+// velocities it reads, which is the two-phase form of the reference's CPU
+// stages; the second phase (u, x update) is applied by the following rebuild
+// gather.  With EX = true each float operation is rounded once, in the
+// reference's order, so the results equal the reference's CPU results.
+#include "physics.cuh"
+
+namespace mpsb {
+
+static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+// ---------------------------------------------------------------- gather
+// dst[p] = src[perm[p]]; the pending update of a fluid particle is applied
+// exactly as k_cell_keys applied it to find its cell; particles sorted past
+// np_new (outside the grid) become type 3 with zero velocity and leave the
+// active range (MPS_CAL_expl_v1.0/MPS_GPU.cpp:268-280, 329).
+__global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint32_t* __restrict__ perm,
+                                                const uint32_t* __restrict__ keys_sorted,
+                                                const float4* __restrict__ tmp, int apply,
+                                                uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np, nn = sc->np_new;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) {
+        const uint32_t old = perm[p];
+        float4 x = src.pos[old], u = src.vel[old];
+        if (apply != 0 && ptype(x) == T_FLUID) {
+            const float dt = sc->dt;
+            const float4 d = tmp[old];
+            if (apply == 1) {
+                u.x = d.x; u.y = d.y; u.z = d.z;
+            } else {
+                u.x = __fadd_rn(u.x, d.x); u.y = __fadd_rn(u.y, d.y); u.z = __fadd_rn(u.z, d.z);
+            }
+            x.x = __fadd_rn(x.x, __fmul_rn(dt, d.x));
+            x.y = __fadd_rn(x.y, __fmul_rn(dt, d.y));
+            x.z = __fadd_rn(x.z, __fmul_rn(dt, d.z));
+        }
+        if (p >= nn) {
+            x.w = __uint_as_float(T_EXCL);
+            u = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        dst.pos[p] = x;
+        dst.vel[p] = u;
+        dst.press[p] = src.press[old];
+        dst.n[p] = src.n[old];
+        const uint32_t id = src.id[old];
+        dst.id[p] = id;
+        dst.cell[p] = keys_sorted[p];
+        index_of_id[id] = p;
+    }
+    // the last block to finish publishes the new active count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&sc->done_blocks, 1u);
+        if (done == gridDim.x - 1) {
+            sc->nexcl += n - nn;
+            sc->np = nn;
+            sc->done_blocks = 0;
+            __threadfence();
+        }
+    }
+}
+
+void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
+                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st) {
+    k_gather<<<blocks_for(cap, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc);
+}
+
+// ---------------------------------------------------------------- update_dt
+// MPS_GPU::update_dt (MPS_CAL_expl_v1.0/MPS_GPU.cpp:761-777): dt = min over
+// particles of CFL*dp/|u| (float CFL*dp divided by the double square root,
+// rounded to float), capped at dt_max.  The minimum over particles is the
+// value at the largest |u|^2, so a max-reduction of |u|^2 gives the same dt.
+__global__ void __launch_bounds__(256) k_update_dt(const float4* __restrict__ vel, Phys P, Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t m = 0;
+    if (i < n) {
+        const float4 u = vel[i];
+        const float vv = dot3<true>(u.x, u.y, u.z, u.x, u.y, u.z);
+        if (vv == vv) m = __float_as_uint(vv);
+        else atomicOr(&sc->err, ERR_NAN);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(&sc->vmax2_bits, m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&sc->done_blocks, 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            const float vmax = __uint_as_float(atomicAdd(&sc->vmax2_bits, 0u));
+            const float t = __double2float_rn((double)P.cfl_dp / sqrt((double)vmax));
+            const float dt = t < P.dt_max ? t : P.dt_max;
+            if (dt < P.dt_min) atomicOr(&sc->err, ERR_DT_TOO_SMALL);
+            sc->dt = dt;
+            sc->vmax2_bits = 0;
+            sc->done_blocks = 0;
+            __threadfence();
+        }
+    }
+}
+
+void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    k_update_dt<<<blocks_for(cap, 256), 256, 0, st>>>(a.cur.vel, a.P, a.sc);
+}
+
+__global__ void k_step_end(Scalars* sc) {
+    sc->time = __fadd_rn(sc->time, sc->dt);
+    sc->step += 1;
+}
+
+void launch_step_end(Scalars* sc, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(sc); }
+
+// ---------------------------------------------------------------- viscosity
+// calVisc_expl + d3_LapVel (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:344-386,
+// MPS_GPU.cpp:683-717): for a fluid particle,
+//   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
+template <bool EX>
+__global__ void __launch_bounds__(256) k_visc(StageArgs a) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const float4 ui = vel[i];
+    const float re = a.P.rlap, thr = a.P.rlap_thr;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            const float4 pj = __ldg(pos + j);
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            if (rr < thr && j != i) {
+                const float w = weight_rr<EX>(re, rr);
+                if (w != 0.f) {
+                    const float4 uj = __ldg(vel + j);
+                    ax = fadd<EX>(ax, fmul<EX>(w, fsub<EX>(uj.x, ui.x)));
+                    ay = fadd<EX>(ay, fmul<EX>(w, fsub<EX>(uj.y, ui.y)));
+                    az = fadd<EX>(az, fmul<EX>(w, fsub<EX>(uj.z, ui.z)));
+                }
+            }
+        }
+    }
+    const float dt = a.sc->dt;
+    const float lx = fmul<EX>(a.P.c_lap, ax), ly = fmul<EX>(a.P.c_lap, ay), lz = fmul<EX>(a.P.c_lap, az);
+    float4 t;
+    t.x = fadd<EX>(ui.x, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lx), a.P.g[0])));
+    t.y = fadd<EX>(ui.y, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, ly), a.P.g[1])));
+    t.z = fadd<EX>(ui.z, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lz), a.P.g[2])));
+    t.w = 0.f;
+    a.tmp[i] = t;
+}
+
+void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    if (a.exact) k_visc<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    else k_visc<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------- collision
+// MPS_GPU::collision (MPS_CAL_expl_v1.0/MPS_GPU.cpp:892-986): for a fluid
+// particle, over neighbours of any type with ds <= col_dis that approach
+// (vabs = (0.5 du).dr / ds <= 0): crt += col_rate * vabs / ds * dr.
+template <bool EX>
+__global__ void __launch_bounds__(256) k_collision(StageArgs a) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const float4 ui = vel[i];
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            const float4 pj = __ldg(pos + j);
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            if (rr < a.P.col_thr && j != i) {
+                float ds, ood;
+                if (EX) { ds = __fsqrt_rn(rr); ood = __fdiv_rn(1.0f, ds); }
+                else { ood = rsqrtf(rr); ds = rr * ood; }
+                const float4 uj = __ldg(vel + j);
+                const float hx = fmul<EX>(0.5f, fsub<EX>(uj.x, ui.x));
+                const float hy = fmul<EX>(0.5f, fsub<EX>(uj.y, ui.y));
+                const float hz = fmul<EX>(0.5f, fsub<EX>(uj.z, ui.z));
+                const float vabs = fmul<EX>(dot3<EX>(hx, hy, hz, dx, dy, dz), ood);
+                if (ds <= a.P.col_dis && vabs <= 0.f) {
+                    const float k = fmul<EX>(fmul<EX>(a.P.col_rate, vabs), ood);
+                    cx = fadd<EX>(cx, fmul<EX>(k, dx));
+                    cy = fadd<EX>(cy, fmul<EX>(k, dy));
+                    cz = fadd<EX>(cz, fmul<EX>(k, dz));
+                }
+            }
+        }
+    }
+    a.tmp[i] = make_float4(cx, cy, cz, 0.f);
+}
+
+void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    if (a.exact) k_collision<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    else k_collision<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------- PND (+EOS)
+// cal_n (MPS_CAL_expl_v1.0/MPS_GPU.cpp:830-887): n_i = sum_{j != i} w(r; r0)
+// for type != 2 (all types during initialisation, MPS.cpp:433-497), and the
+// equation of state of calPres_expl (MPS_GPU_EXPL.cpp:391-415):
+//   p = max(0, rho c^2 (n - n0) / n0).
+template <bool EX>
+__global__ void __launch_bounds__(256) k_pnd(StageArgs a, int eos, int all_types) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4 pi = pos[i];
+    if (!all_types && ptype(pi) == T_DUMMY) return;
+    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    float acc = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            const float4 pj = __ldg(pos + j);
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            if (rr < thr && j != i) acc = fadd<EX>(acc, weight_rr<EX>(re, rr));
+        }
+    }
+    a.cur.n[i] = acc;
+    if (eos) {
+        const float t = fmul<EX>(fmul<EX>(a.P.one_over_alpha, fsub<EX>(acc, a.P.nzero)), a.P.one_over_nzero);
+        a.cur.press[i] = t > 0.f ? t : 0.f;
+    }
+}
+
+void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
+    if (a.exact) k_pnd<true><<<blocks_for(cap, 256), 256, 0, st>>>(a, eos, all_types);
+    else k_pnd<false><<<blocks_for(cap, 256), 256, 0, st>>>(a, eos, all_types);
+}
+
+// calPres_expl second loop (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:417-426): a
+// type-2 particle takes the pressure of its wall particle i_normal.
+__global__ void __launch_bounds__(256) k_dummy_press(State s, const uint32_t* __restrict__ normal_id_of,
+                                                     const uint32_t* __restrict__ index_of_id,
+                                                     const Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (ptype(s.pos[i]) != T_DUMMY) return;
+    const uint32_t j = index_of_id[normal_id_of[s.id[i]]];
+    s.press[i] = s.press[j];
+}
+
+void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const uint32_t* index_of_id, uint32_t cap,
+                        cudaStream_t st) {
+    k_dummy_press<<<blocks_for(cap, 256), 256, 0, st>>>(a.cur, normal_id_of, index_of_id, a.sc);
+}
+
+// ---------------------------------------------------------------- gradient
+// calDash + d3_GradPres (MPS_CAL_expl_v1.0/MPS_GPU.cpp:571-638, 782-825): for
+// a fluid particle, p_hat = min p over type != 2 neighbours with r^2 <= r0^2
+// (itself included), grad = d/n0 * sum_{j != i} (p_j - p_hat)/r^2 w(r; r0) dr
+// over every type (semi-implicit: type 2 excluded, MPS_CAL_v4.0/MPS_CPU.cpp:384-445),
+// tmp = -dt/rho * grad.
+template <bool EX>
+__global__ void __launch_bounds__(256) k_dash(StageArgs a) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float* __restrict__ press = a.cur.press;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    float hat = press[i];
+    const float r02 = a.P.rzero2;
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            const float4 pj = __ldg(pos + j);
+            if (ptype(pj) == T_DUMMY) continue;
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            if (rr <= r02) {
+                const float pjv = __ldg(press + j);
+                if (pjv < hat) hat = pjv;
+            }
+        }
+    }
+    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    const bool skip_dummy = a.semi != 0;
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            const float4 pj = __ldg(pos + j);
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            if (rr < thr && j != i && !(skip_dummy && ptype(pj) == T_DUMMY)) {
+                const float w = weight_rr<EX>(re, rr);
+                if (w != 0.f) {
+                    const float k = fmul<EX>(fdiv<EX>(fsub<EX>(__ldg(press + j), hat), rr), w);
+                    gx = fadd<EX>(gx, fmul<EX>(k, dx));
+                    gy = fadd<EX>(gy, fmul<EX>(k, dy));
+                    gz = fadd<EX>(gz, fmul<EX>(k, dz));
+                }
+            }
+        }
+    }
+    const float cg = fmul<EX>(a.P.dim_f, a.P.one_over_nzero);
+    const float kk = fmul<EX>(-a.sc->dt, a.P.one_over_rho);
+    a.tmp[i] = make_float4(fmul<EX>(kk, fmul<EX>(cg, gx)), fmul<EX>(kk, fmul<EX>(cg, gy)),
+                           fmul<EX>(kk, fmul<EX>(cg, gz)), 0.f);
+}
+
+void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    if (a.exact) k_dash<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    else k_dash<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------- staging
+__global__ void __launch_bounds__(256) k_fill_excluded(Staging o, uint32_t np0) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= np0) return;
+    o.id[k] = k;
+    o.type[k] = T_EXCL;
+    o.press[k] = 0.f;
+    o.n[k] = 0.f;
+    for (int c = 0; c < 3; c++) {
+        o.pos3[3 * k + c] = 0.f;
+        o.vel3[3 * k + c] = 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_unpack(State s, Staging o, int by_id, uint32_t np0,
+                                                const Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 x = s.pos[i], u = s.vel[i];
+    const uint32_t id = s.id[i];
+    uint32_t k = i;
+    if (by_id) {
+        if (id >= np0) return;
+        k = id;
+    }
+    o.id[k] = id;
+    o.type[k] = ptype(x);
+    o.pos3[3 * k] = x.x; o.pos3[3 * k + 1] = x.y; o.pos3[3 * k + 2] = x.z;
+    o.vel3[3 * k] = u.x; o.vel3[3 * k + 1] = u.y; o.vel3[3 * k + 2] = u.z;
+    o.press[k] = s.press[i];
+    o.n[k] = s.n[i];
+}
+
+__global__ void __launch_bounds__(256) k_pack(State s, Staging in, int mask, const Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (mask & 1) {
+        float4 x = s.pos[i];
+        x.x = in.pos3[3 * i]; x.y = in.pos3[3 * i + 1]; x.z = in.pos3[3 * i + 2];
+        s.pos[i] = x;
+    }
+    if (mask & 2) {
+        float4 u = s.vel[i];
+        u.x = in.vel3[3 * i]; u.y = in.vel3[3 * i + 1]; u.z = in.vel3[3 * i + 2];
+        s.vel[i] = u;
+    }
+    if (mask & 4) s.press[i] = in.press[i];
+    if (mask & 8) s.n[i] = in.n[i];
+}
+
+void launch_unpack(const State& s, const Staging& out, int by_id, uint32_t np0, const Scalars* sc, uint32_t cap,
+                   cudaStream_t st) {
+    if (by_id) k_fill_excluded<<<blocks_for(np0, 256), 256, 0, st>>>(out, np0);
+    k_unpack<<<blocks_for(cap, 256), 256, 0, st>>>(s, out, by_id, np0, sc);
+}
+
+void launch_pack(const State& s, const Staging& in, int mask, const Scalars* sc, uint32_t cap, cudaStream_t st) {
+    k_pack<<<blocks_for(cap, 256), 256, 0, st>>>(s, in, mask, sc);
+}
+
+// ---------------------------------------------------------------- init
+// n0 = first maximum of n in index order (MPS_CAL_expl_v1.0/MPS.cpp:487-496):
+// max over (n bits << 32 | ~index), n >= 0 so its bits order like its value.
+__global__ void __launch_bounds__(256) k_nzero(const float* __restrict__ n, const Scalars* __restrict__ sc,
+                                               unsigned long long* best) {
+    const uint32_t np = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = 0ull;
+    if (i < np) v = ((unsigned long long)__float_as_uint(n[i]) << 32) | (unsigned long long)(0xffffffffu - i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    if ((threadIdx.x & 31) == 0 && v) atomicMax(best, v);
+}
+
+void launch_nzero(const float* n, Scalars* sc, unsigned long long* best, uint32_t cap, cudaStream_t st) {
+    k_nzero<<<blocks_for(cap, 256), 256, 0, st>>>(n, sc, best);
+}
+
+// lambda (MPS_CAL_expl_v1.0/MPS.cpp:500-515): sum over i != t of
+// r^2 w(r; r0), r = |x_i - x_t|, in index order; only the linked cells of t
+// can hold non-zero terms and they are visited in ascending index order.
+__global__ void k_lambda(StageArgs a, const unsigned long long* best, float* out) {
+    const uint32_t t = 0xffffffffu - (uint32_t)(*best & 0xffffffffull);
+    const float4 pt = a.cur.pos[t];
+    const uint32_t c = a.cur.cell[t];
+    float lam = 0.f;
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            if (j == t) continue;
+            const float4 pj = a.cur.pos[j];
+            const float dx = __fsub_rn(pj.x, pt.x), dy = __fsub_rn(pj.y, pt.y), dz = __fsub_rn(pj.z, pt.z);
+            const float rr = dot3<true>(dx, dy, dz, dx, dy, dz);
+            const float r = __fsqrt_rn(rr);
+            const float w = r < a.P.rzero ? __fsub_rn(__fdiv_rn(a.P.rzero, r), 1.0f) : 0.f;
+            lam = __fadd_rn(lam, __fmul_rn(__fmul_rn(r, r), w));
+        }
+    }
+    *out = lam;
+}
+
+void launch_lambda(const StageArgs& a, const unsigned long long* best, float* lambda_out, cudaStream_t st) {
+    k_lambda<<<1, 1, 0, st>>>(a, best, lambda_out);
+}
+
+// i_normal (MPS_CAL_expl_v1.0/MPS.cpp:531-555): for a type-2 particle the
+// first type-1 particle in index order that improves r^2 below 2 r0^2.
+// `reach` cells in each direction cover sqrt(2) r0; rows are visited in
+// ascending cell order, so candidates come in ascending index order.
+__global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_t* __restrict__ normal_id_of) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 pi = a.cur.pos[i];
+    const uint32_t idi = a.cur.id[i];
+    if (ptype(pi) != T_DUMMY) {
+        normal_id_of[idi] = idi;
+        return;
+    }
+    float dis = __fmul_rn(__fmul_rn(2.0f, a.P.rzero), a.P.rzero);
+    uint32_t best = 0xffffffffu;
+    const uint32_t c = a.cur.cell[i];
+    const Grid& g = a.g;
+    const int nz = g.dim == 3 ? reach : 0;
+    for (int dz = -nz; dz <= nz; dz++) {
+        for (int dy = -reach; dy <= reach; dy++) {
+            const uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
+            uint32_t first = 0xffffffffu, last = 0;
+            for (int dx = -reach; dx <= reach; dx++) {
+                const uint32_t cc = c0 + (uint32_t)dx;
+                if (cc < g.ncells) {
+                    if (first == 0xffffffffu) first = cc;
+                    last = cc;
+                }
+            }
+            if (first == 0xffffffffu) continue;
+            const uint32_t lo = a.cell_start[first], hi = a.cell_start[last + 1];
+            for (uint32_t j = lo; j < hi; j++) {
+                const float4 pj = a.cur.pos[j];
+                if (ptype(pj) != T_WALL) continue;
+                const float dx = __fsub_rn(pj.x, pi.x), dy2 = __fsub_rn(pj.y, pi.y), dz2 = __fsub_rn(pj.z, pi.z);
+                const float rr = dot3<true>(dx, dy2, dz2, dx, dy2, dz2);
+                if (rr < dis) {
+                    dis = rr;
+                    best = j;
+                }
+            }
+        }
+    }
+    normal_id_of[idi] = best == 0xffffffffu ? idi : a.cur.id[best];
+}
+
+void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint32_t cap, cudaStream_t st) {
+    k_normals<<<blocks_for(cap, 256), 256, 0, st>>>(a, reach, normal_id_of);
+}
+
+}  // namespace mpsb

@@ -1,0 +1,71 @@
+// physics.cuh -- launchers of the particle-stage kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mps_device.cuh"
+
+namespace mpsb {
+
+// Particle state in one buffer set (sorted order).
+struct State {
+    float4* pos;      // x y z, w = type bits
+    float4* vel;      // u v w, w unused (0)
+    float* press;
+    float* n;
+    uint32_t* id;     // GEO.dat index
+    uint32_t* cell;   // cell id from the last rebuild (i_cell_list)
+};
+
+struct StageArgs {
+    State cur;                 // current state
+    const uint32_t* cell_start;  // ncells + 1 entries
+    float4* tmp;               // pending update (one float4 per particle)
+    Scalars* sc;
+    Grid g;
+    Phys P;
+    bool exact;
+    int semi;                  // semi-implicit (v4.0) rules
+};
+
+// reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
+void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
+                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st);
+
+// update_dt: max |u|^2, then dt on the device
+void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st);
+// stage kernels
+void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st);
+void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st);
+void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st);
+void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const uint32_t* index_of_id, uint32_t cap,
+                        cudaStream_t st);
+void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st);
+void launch_step_end(Scalars* sc, cudaStream_t st);
+
+// host-layout staging (x y z per particle) <-> the float4 state
+struct Staging {
+    float* pos3;
+    float* vel3;
+    float* press;
+    float* n;
+    uint32_t* id;
+    uint32_t* type;
+};
+// sorted order (by_id = 0) or by GEO index into np0 entries (by_id = 1)
+void launch_unpack(const State& s, const Staging& out, int by_id, uint32_t np0, const Scalars* sc, uint32_t cap,
+                   cudaStream_t st);
+// overwrite the selected fields of the active particles (mask bits: 1 pos,
+// 2 vel, 4 press, 8 n)
+void launch_pack(const State& s, const Staging& in, int mask, const Scalars* sc, uint32_t cap, cudaStream_t st);
+
+// initialisation
+// n0 and the particle it belongs to: max n with the lowest index on ties
+void launch_nzero(const float* n, Scalars* sc, unsigned long long* best, uint32_t cap, cudaStream_t st);
+// lambda = sum over j of r^2 w(r0) around particle `best`, in index order
+void launch_lambda(const StageArgs& a, const unsigned long long* best, float* lambda_out, cudaStream_t st);
+// nearest type-1 particle (first in index order) within sqrt(2) r0 of each
+// type-2 particle, stored by GEO.dat index
+void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint32_t cap, cudaStream_t st);
+
+}  // namespace mpsb
