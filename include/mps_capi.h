@@ -84,7 +84,8 @@ typedef struct {
     int use_graph;       /* capture each step in a CUDA graph (1) or launch   */
     double cg_tol;       /* PPE: stop when |r| <= cg_tol * |b| (FP64 norms)   */
     int cg_max_iter;     /* PPE: iteration limit (0: 10000)                   */
-    int cg_check_every;  /* PPE: iterations between FP64 true-residual checks */
+    int cg_check_every;  /* PPE: most FP32 CG iterations between two FP64
+                            true-residual checks (0: 1000)                   */
     int precond;         /* MPS_PRECOND_*                                     */
     uint32_t capacity;   /* particle capacity (0: the scene's np)             */
     uint32_t reserved[8];

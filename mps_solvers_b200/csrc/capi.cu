@@ -38,6 +38,9 @@ struct mps_handle {
     uint32_t* index_of_id = nullptr;
     uint32_t* normal_id_of = nullptr;
     uint32_t* cell_start = nullptr;
+    uint32_t* list_fluid = nullptr;
+    uint32_t* list_solid = nullptr;
+    uint32_t cap_fluid = 0, cap_solid = 0;
     SortScratch sort{};
     Scalars* sc = nullptr;
     unsigned long long* best = nullptr;
@@ -54,6 +57,7 @@ struct mps_handle {
     std::vector<int> prof_tag;
     size_t prof_used = 0;
     int launches = 0;  // kernels enqueued by the last enqueue_step
+    cudaError_t launch_err = cudaSuccess;  // first failed launch not seen by cudaGetLastError
     std::string err;
     std::vector<void*> allocs;
 };
@@ -108,6 +112,12 @@ static StageArgs stage_args(mps_handle* h) {
     a.P = h->P;
     a.exact = h->opt.arith == MPS_ARITH_EXACT;
     a.semi = h->opt.method == MPS_METHOD_SEMI_IMPLICIT;
+    a.list_fluid = h->list_fluid;
+    a.n_fluid = &h->sc->n_fluid;
+    a.cap_fluid = h->cap_fluid;
+    a.list_solid = h->list_solid;
+    a.n_solid = &h->sc->n_solid;
+    a.cap_solid = h->cap_solid;
     return a;
 }
 
@@ -143,7 +153,8 @@ static void rebuild(mps_handle* h, int apply) {
     mark(h, ST_CELLS);
     launch_cell_start(h->sort.keys[r], h->g, h->sc, h->cell_start, h->cap, st);
     mark(h, ST_GATHER);
-    launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st);
+    launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
+                  h->list_fluid, h->list_solid);
     h->launches += 3 + 3 * h->passes;
     h->cur ^= 1;
 }
@@ -173,6 +184,7 @@ static void enqueue_step(mps_handle* h) {
         launch_pnd(stage_args(h), 0, 0, cap, st);
         mark(h, ST_PRESSURE);
         h->launches += 1 + ppe_enqueue(h->ppe, stage_args(h), h->opt, cap, st);
+        if (h->ppe.launch_err != cudaSuccess) h->launch_err = h->ppe.launch_err;
     }
     mark(h, ST_DASH);
     launch_dash(stage_args(h), cap, st);
@@ -196,6 +208,7 @@ static mps_status read_status(mps_handle* h, Scalars* out) {
     if (s.err & ERR_DEVICE_TIMEOUT) { h->err = "device wait timed out"; return MPS_ERR_DEVICE_TIMEOUT; }
     if (s.err & ERR_CG_NOT_CONVERGED) { h->err = "PPE CG did not reach its tolerance"; return MPS_ERR_CG_NOT_CONVERGED; }
     if (s.err & ERR_PARTICLE_OUT) { h->err = "particle left the grid"; return MPS_ERR_PARTICLE_OUT; }
+    if (s.err & ERR_CAPACITY) { h->err = "a particle has more PPE neighbours than the matrix stride holds"; return MPS_ERR_CAPACITY; }
     return MPS_OK;
 }
 
@@ -208,7 +221,7 @@ extern "C" void mps_default_options(mps_options* o) {
     o->use_graph = 1;
     o->cg_tol = 1e-8;
     o->cg_max_iter = 10000;
-    o->cg_check_every = 50;
+    o->cg_check_every = 1000;
     o->precond = MPS_PRECOND_DIAGONAL;
     o->capacity = 0;
 }
@@ -259,6 +272,12 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     CK(dalloc(h, &h->tmp, cap));
     CK(dalloc(h, &h->index_of_id, cap));
     CK(dalloc(h, &h->normal_id_of, cap));
+    // fluid and wall particles never change type (only drop out), so the
+    // lists never outgrow the initial counts
+    h->cap_fluid = np - nb2 - nb1;
+    h->cap_solid = np - nb2;
+    CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
+    CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
     CK(dalloc(h, &h->cell_start, (size_t)g.ncells + 1));
     h->sort.tiles = sort_tiles(cap);
     for (int b = 0; b < 2; b++) {
@@ -326,7 +345,38 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
 
     // MPS_GPU::Initial (MPS_CAL_expl_v1.0/MPS_GPU.cpp:63-115): divideCell, then calOnce.
     rebuild(h, APPLY_NONE);
-    {
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        // MPS_CPU::Initial / MPS::calOnce of MPS_CAL_v4.0 (MPS_CPU.cpp:54-122,
+        // MPS.cpp:305-370): n of every particle, n0, lambda, in double
+        double* n64 = nullptr;
+        double* res = nullptr;
+        CK(dalloc(h, &n64, cap));
+        CK(dalloc(h, &res, 2));
+        StageArgs a = stage_args(h);
+        launch_pnd64(a, n64, h->cap, h->stream);
+        launch_n0_lambda64(a, n64, res, h->stream);
+        launch_normals(a, h->normal_reach, h->normal_id_of, h->cap, h->stream);
+        double hr[2] = {0, 0};
+        CK(cudaMemcpyAsync(hr, res, sizeof hr, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaGetLastError());
+        if (!(hr[0] > 0.0)) {
+            h->err = "n0 is not positive: no particle has a neighbour within r0";
+            return MPS_ERR_INVALID;
+        }
+        h->ppe.n0_64 = hr[0];
+        h->ppe.lambda64 = hr[1];
+        HostConst& c = h->hc;
+        c.nzero = (float)hr[0];
+        c.lambda = (float)hr[1];
+        c.alpha = (float)(1.0 / ((double)prm.rho * prm.cs * prm.cs));
+        c.one_over_alpha = (float)((double)prm.rho * prm.cs * prm.cs);
+        c.one_over_rho = (float)(1.0 / (double)prm.rho);
+        c.one_over_nzero = (float)(1.0 / hr[0]);
+        c.one_over_dim = (float)(1.0 / (double)prm.dim);
+        c.one_over_dt = (float)(1.0 / (double)prm.dt_max);
+        c.c_lap = (float)((2.0 * prm.dim) / (hr[0] * hr[1]));
+    } else {
         StageArgs a = stage_args(h);
         launch_pnd(a, 0, 1, h->cap, h->stream);  // n of every particle
         launch_nzero(h->S[h->cur].n, h->sc, h->best, h->cap, h->stream);
@@ -369,7 +419,7 @@ static mps_status create_common(mps_handle** out, const mps_options* opt) {
     if (opt) h->opt = *opt;
     else mps_default_options(&h->opt);
     if (h->opt.cg_max_iter <= 0) h->opt.cg_max_iter = 10000;
-    if (h->opt.cg_check_every <= 0) h->opt.cg_check_every = 50;
+    if (h->opt.cg_check_every <= 0) h->opt.cg_check_every = 1000;
     if (h->opt.cg_tol <= 0) h->opt.cg_tol = 1e-8;
     *out = h;
     return MPS_OK;
@@ -463,6 +513,12 @@ static mps_status step_async(mps_handle* h, int nsteps) {
         }
     }
     CK(cudaGetLastError());
+    if (h->launch_err != cudaSuccess) {
+        const cudaError_t e = h->launch_err;
+        h->launch_err = cudaSuccess;
+        h->err = std::string("cooperative PPE launch: ") + cudaGetErrorString(e);
+        return MPS_ERR_CUDA;
+    }
     return MPS_OK;
 }
 

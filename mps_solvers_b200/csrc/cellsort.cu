@@ -16,6 +16,11 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ po
                                                    uint32_t* __restrict__ vals) {
     const uint32_t n = sc->np;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        // the gather of this rebuild refills the particle lists
+        sc->n_fluid = 0;
+        sc->n_solid = 0;
+    }
     if (i >= n) return;
     float4 p = pos[i];
     if (apply != APPLY_NONE && ptype(p) == T_FLUID) {
@@ -231,6 +236,10 @@ int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_
         cur ^= 1;
     }
     return cur;
+}
+
+void launch_scan_exclusive(uint32_t* a, uint32_t total, cudaStream_t st) {
+    k_scan_exclusive<<<1, 1024, 0, st>>>(a, total);
 }
 
 void launch_cell_start(const uint32_t* keys_sorted, const Grid& g, Scalars* sc, uint32_t* cell_start, uint32_t cap,

@@ -54,6 +54,8 @@ void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32
                             cudaStream_t st);
 void launch_cell_start_plain(const uint32_t* keys_sorted, uint32_t n, const Grid& g, uint32_t* cell_start,
                              uint32_t* n_in_grid, cudaStream_t st);
+// exclusive scan of `total` uint32 counters in place (one block)
+void launch_scan_exclusive(uint32_t* a, uint32_t total, cudaStream_t st);
 void launch_cell_end_from_start(const uint32_t* cell_start, uint32_t ncells, uint32_t* start_out,
                                 uint32_t* end_out, cudaStream_t st);
 

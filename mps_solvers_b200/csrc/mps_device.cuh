@@ -38,7 +38,9 @@ struct Scalars {
     int step;
     int cg_iters;
     double cg_relres;
-    double pad[4];
+    uint32_t n_fluid;      // entries of the fluid list built by the last rebuild
+    uint32_t n_solid;      // entries of the fluid + wall list
+    double pad[3];
 };
 
 enum : uint32_t {
@@ -47,6 +49,7 @@ enum : uint32_t {
     ERR_PARTICLE_OUT = 4u,
     ERR_CG_NOT_CONVERGED = 8u,
     ERR_DEVICE_TIMEOUT = 16u,
+    ERR_CAPACITY = 32u,
 };
 
 // particle types (pos.w carries the type as its bit pattern)

@@ -21,9 +21,11 @@ static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) /
 __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint32_t* __restrict__ perm,
                                                 const uint32_t* __restrict__ keys_sorted,
                                                 const float4* __restrict__ tmp, int apply,
-                                                uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc) {
+                                                uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc,
+                                                uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid) {
     const uint32_t n = sc->np, nn = sc->np_new;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ty = T_EXCL;
     if (p < n) {
         const uint32_t old = perm[p];
         float4 x = src.pos[old], u = src.vel[old];
@@ -51,6 +53,23 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
         dst.id[p] = id;
         dst.cell[p] = keys_sorted[p];
         index_of_id[id] = p;
+        ty = ptype(x);
+    }
+    // compact lists of the active fluid and non-dummy particles (order within
+    // a list does not matter: every particle's stage result is independent)
+    if (list_fluid) {
+        const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+        const bool f = ty == T_FLUID, s2 = ty == T_FLUID || ty == T_WALL;
+        const uint32_t mf = __ballot_sync(0xffffffffu, f), ms = __ballot_sync(0xffffffffu, s2);
+        uint32_t bf = 0, bs = 0;
+        if (lane == 0) {
+            if (mf) bf = atomicAdd(&sc->n_fluid, __popc(mf));
+            if (ms) bs = atomicAdd(&sc->n_solid, __popc(ms));
+        }
+        bf = __shfl_sync(0xffffffffu, bf, 0);
+        bs = __shfl_sync(0xffffffffu, bs, 0);
+        if (f) list_fluid[bf + __popc(mf & lt)] = p;
+        if (s2) list_solid[bs + __popc(ms & lt)] = p;
     }
     // the last block to finish publishes the new active count
     __syncthreads();
@@ -67,8 +86,10 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
 }
 
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
-                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st) {
-    k_gather<<<blocks_for(cap, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc);
+                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
+                   uint32_t* list_fluid, uint32_t* list_solid) {
+    k_gather<<<blocks_for(cap, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc,
+                                                    list_fluid, list_solid);
 }
 
 // ---------------------------------------------------------------- update_dt
@@ -118,7 +139,286 @@ __global__ void k_step_end(Scalars* sc) {
 
 void launch_step_end(Scalars* sc, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(sc); }
 
-// ---------------------------------------------------------------- viscosity
+// ---------------------------------------------------------------- warp per particle
+// One warp per particle; lane l takes candidate j = base + l of each row
+// chunk.  ORD (explicit method, exact arithmetic): the warp adds the non-zero
+// terms one by one in ascending lane (= ascending j) order, which is the
+// reference's summation order, so the sums are bit-identical to its
+// sequential loop.  Otherwise: lane-private partial sums and a fixed shuffle
+// tree (deterministic, not the reference's order).
+struct WarpTask {
+    uint32_t i;      // particle
+    bool ok;
+};
+
+__device__ __forceinline__ WarpTask warp_task(const StageArgs& a, const uint32_t* __restrict__ list,
+                                              const uint32_t* __restrict__ list_n) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    WarpTask t;
+    if (list) {
+        const uint32_t n = *list_n;
+        t.ok = w < n;
+        t.i = t.ok ? list[w] : 0u;
+    } else {
+        t.ok = w < a.sc->np;
+        t.i = w;
+    }
+    return t;
+}
+
+template <bool EX>
+__device__ __forceinline__ float warp_ordered_add(float acc, float term, uint32_t m) {
+    while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1u;
+        acc = fadd<EX>(acc, __shfl_sync(0xffffffffu, term, b));
+    }
+    return acc;
+}
+
+__device__ __forceinline__ float warp_tree_add(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <bool EX, bool ORD>
+__global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __restrict__ list,
+                                                const uint32_t* __restrict__ list_n) {
+    const WarpTask tk = warp_task(a, list, list_n);
+    if (!tk.ok) return;
+    const uint32_t i = tk.i, lane = threadIdx.x & 31;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const float4 ui = vel[i];
+    const float re = a.P.rlap, thr = a.P.rlap_thr;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            float tx = 0.f, ty = 0.f, tz = 0.f;
+            bool hit = false;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                if (rr < thr) {
+                    const float w = weight_rr<EX>(re, rr);
+                    if (w != 0.f) {
+                        const float4 uj = __ldg(vel + j);
+                        tx = fmul<EX>(w, fsub<EX>(uj.x, ui.x));
+                        ty = fmul<EX>(w, fsub<EX>(uj.y, ui.y));
+                        tz = fmul<EX>(w, fsub<EX>(uj.z, ui.z));
+                        hit = true;
+                    }
+                }
+            }
+            if (ORD) {
+                uint32_t m = __ballot_sync(0xffffffffu, hit);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1u;
+                    ax = __fadd_rn(ax, __shfl_sync(0xffffffffu, tx, b));
+                    ay = __fadd_rn(ay, __shfl_sync(0xffffffffu, ty, b));
+                    az = __fadd_rn(az, __shfl_sync(0xffffffffu, tz, b));
+                }
+            } else {
+                ax += tx; ay += ty; az += tz;
+            }
+        }
+    }
+    if (!ORD) { ax = warp_tree_add(ax); ay = warp_tree_add(ay); az = warp_tree_add(az); }
+    if (lane != 0) return;
+    const float dt = a.sc->dt;
+    const float lx = fmul<EX>(a.P.c_lap, ax), ly = fmul<EX>(a.P.c_lap, ay), lz = fmul<EX>(a.P.c_lap, az);
+    float4 t;
+    t.x = fadd<EX>(ui.x, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lx), a.P.g[0])));
+    t.y = fadd<EX>(ui.y, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, ly), a.P.g[1])));
+    t.z = fadd<EX>(ui.z, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lz), a.P.g[2])));
+    t.w = 0.f;
+    a.tmp[i] = t;
+}
+
+template <bool EX, bool ORD>
+__global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t* __restrict__ list,
+                                                     const uint32_t* __restrict__ list_n) {
+    const WarpTask tk = warp_task(a, list, list_n);
+    if (!tk.ok) return;
+    const uint32_t i = tk.i, lane = threadIdx.x & 31;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const float4 ui = vel[i];
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            float tx = 0.f, ty = 0.f, tz = 0.f;
+            bool hit = false;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                if (rr < a.P.col_thr) {
+                    float ds, ood;
+                    if (EX) { ds = __fsqrt_rn(rr); ood = __fdiv_rn(1.0f, ds); }
+                    else { ood = rsqrtf(rr); ds = rr * ood; }
+                    const float4 uj = __ldg(vel + j);
+                    const float hx = fmul<EX>(0.5f, fsub<EX>(uj.x, ui.x));
+                    const float hy = fmul<EX>(0.5f, fsub<EX>(uj.y, ui.y));
+                    const float hz = fmul<EX>(0.5f, fsub<EX>(uj.z, ui.z));
+                    const float vabs = fmul<EX>(dot3<EX>(hx, hy, hz, dx, dy, dz), ood);
+                    if (ds <= a.P.col_dis && vabs <= 0.f) {
+                        const float k = fmul<EX>(fmul<EX>(a.P.col_rate, vabs), ood);
+                        tx = fmul<EX>(k, dx);
+                        ty = fmul<EX>(k, dy);
+                        tz = fmul<EX>(k, dz);
+                        hit = true;
+                    }
+                }
+            }
+            uint32_t m = __ballot_sync(0xffffffffu, hit);
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1u;
+                cx = fadd<EX>(cx, __shfl_sync(0xffffffffu, tx, b));
+                cy = fadd<EX>(cy, __shfl_sync(0xffffffffu, ty, b));
+                cz = fadd<EX>(cz, __shfl_sync(0xffffffffu, tz, b));
+            }
+        }
+    }
+    if (lane == 0) a.tmp[i] = make_float4(cx, cy, cz, 0.f);
+}
+
+template <bool EX, bool ORD>
+__global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_types, const uint32_t* __restrict__ list,
+                                               const uint32_t* __restrict__ list_n) {
+    const WarpTask tk = warp_task(a, list, list_n);
+    if (!tk.ok) return;
+    const uint32_t i = tk.i, lane = threadIdx.x & 31;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4 pi = pos[i];
+    if (!all_types && ptype(pi) == T_DUMMY) return;
+    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    float acc = 0.f;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            float w = 0.f;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                if (rr < thr) w = weight_rr<EX>(re, rr);
+            }
+            if (ORD) acc = warp_ordered_add<true>(acc, w, __ballot_sync(0xffffffffu, w != 0.f));
+            else acc += w;
+        }
+    }
+    if (!ORD) acc = warp_tree_add(acc);
+    if (lane != 0) return;
+    a.cur.n[i] = acc;
+    if (eos) {
+        const float t = fmul<EX>(fmul<EX>(a.P.one_over_alpha, fsub<EX>(acc, a.P.nzero)), a.P.one_over_nzero);
+        a.cur.press[i] = t > 0.f ? t : 0.f;
+    }
+}
+
+template <bool EX, bool ORD>
+__global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __restrict__ list,
+                                                const uint32_t* __restrict__ list_n) {
+    const WarpTask tk = warp_task(a, list, list_n);
+    if (!tk.ok) return;
+    const uint32_t i = tk.i, lane = threadIdx.x & 31;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float* __restrict__ press = a.cur.press;
+    const float4 pi = pos[i];
+    if (ptype(pi) != T_FLUID) return;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    const float r02 = a.P.rzero2;
+    // p_hat: a minimum, independent of order
+    float hat = press[i];
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            if (j < rg.hi) {
+                const float4 pj = __ldg(pos + j);
+                if (ptype(pj) != T_DUMMY) {
+                    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                    if (rr <= r02) {
+                        const float pjv = __ldg(press + j);
+                        if (pjv < hat) hat = pjv;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, o));
+    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    const bool skip_dummy = a.semi != 0;
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            float tx = 0.f, ty = 0.f, tz = 0.f;
+            bool hit = false;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                if (!(skip_dummy && ptype(pj) == T_DUMMY)) {
+                    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                    if (rr < thr) {
+                        const float w = weight_rr<EX>(re, rr);
+                        if (w != 0.f) {
+                            const float k = fmul<EX>(fdiv<EX>(fsub<EX>(__ldg(press + j), hat), rr), w);
+                            tx = fmul<EX>(k, dx);
+                            ty = fmul<EX>(k, dy);
+                            tz = fmul<EX>(k, dz);
+                            hit = true;
+                        }
+                    }
+                }
+            }
+            if (ORD) {
+                uint32_t m = __ballot_sync(0xffffffffu, hit);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1u;
+                    gx = __fadd_rn(gx, __shfl_sync(0xffffffffu, tx, b));
+                    gy = __fadd_rn(gy, __shfl_sync(0xffffffffu, ty, b));
+                    gz = __fadd_rn(gz, __shfl_sync(0xffffffffu, tz, b));
+                }
+            } else {
+                gx += tx; gy += ty; gz += tz;
+            }
+        }
+    }
+    if (!ORD) { gx = warp_tree_add(gx); gy = warp_tree_add(gy); gz = warp_tree_add(gz); }
+    if (lane != 0) return;
+    const float cg = fmul<EX>(a.P.dim_f, a.P.one_over_nzero);
+    const float kk = fmul<EX>(-a.sc->dt, a.P.one_over_rho);
+    a.tmp[i] = make_float4(fmul<EX>(kk, fmul<EX>(cg, gx)), fmul<EX>(kk, fmul<EX>(cg, gy)),
+                           fmul<EX>(kk, fmul<EX>(cg, gz)), 0.f);
+}
+
+// ---------------------------------------------------------------- viscosity (thread per particle)
 // calVisc_expl + d3_LapVel (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:344-386,
 // MPS_GPU.cpp:683-717): for a fluid particle,
 //   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
@@ -164,8 +464,11 @@ __global__ void __launch_bounds__(256) k_visc(StageArgs a) {
 }
 
 void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (a.exact) k_visc<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
-    else k_visc<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const bool ord = a.exact && !a.semi;
+    if (a.exact && ord) k_visc_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else if (a.exact) k_visc_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else k_visc_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
 }
 
 // ---------------------------------------------------------------- collision
@@ -213,8 +516,11 @@ __global__ void __launch_bounds__(256) k_collision(StageArgs a) {
 }
 
 void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (a.exact) k_collision<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
-    else k_collision<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const bool ord = a.exact && !a.semi;
+    if (a.exact && ord) k_collision_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else if (a.exact) k_collision_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else k_collision_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
 }
 
 // ---------------------------------------------------------------- PND (+EOS)
@@ -251,8 +557,13 @@ __global__ void __launch_bounds__(256) k_pnd(StageArgs a, int eos, int all_types
 }
 
 void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
-    if (a.exact) k_pnd<true><<<blocks_for(cap, 256), 256, 0, st>>>(a, eos, all_types);
-    else k_pnd<false><<<blocks_for(cap, 256), 256, 0, st>>>(a, eos, all_types);
+    const bool use_list = a.list_solid && !all_types;
+    const uint32_t* list = use_list ? a.list_solid : nullptr;
+    const uint32_t nb = blocks_for((use_list ? a.cap_solid : cap) * 32u, 256);
+    const bool ord = a.exact && !a.semi;
+    if (a.exact && ord) k_pnd_w<true, true><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
+    else if (a.exact) k_pnd_w<true, false><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
+    else k_pnd_w<false, false><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
 }
 
 // calPres_expl second loop (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:417-426): a
@@ -332,8 +643,11 @@ __global__ void __launch_bounds__(256) k_dash(StageArgs a) {
 }
 
 void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (a.exact) k_dash<true><<<blocks_for(cap, 256), 256, 0, st>>>(a);
-    else k_dash<false><<<blocks_for(cap, 256), 256, 0, st>>>(a);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const bool ord = a.exact && !a.semi;
+    if (a.exact && ord) k_dash_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else if (a.exact) k_dash_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    else k_dash_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
 }
 
 // ---------------------------------------------------------------- staging

@@ -26,11 +26,19 @@ struct StageArgs {
     Phys P;
     bool exact;
     int semi;                  // semi-implicit (v4.0) rules
+    // compact particle lists from the last rebuild (nullptr: all particles)
+    const uint32_t* list_fluid = nullptr;
+    const uint32_t* n_fluid = nullptr;
+    uint32_t cap_fluid = 0;
+    const uint32_t* list_solid = nullptr;  // fluid + wall (type != 2)
+    const uint32_t* n_solid = nullptr;
+    uint32_t cap_solid = 0;
 };
 
 // reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
-                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st);
+                   const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
+                   uint32_t* list_fluid, uint32_t* list_solid);
 
 // update_dt: max |u|^2, then dt on the device
 void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st);

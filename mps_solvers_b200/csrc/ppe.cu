@@ -1,14 +1,712 @@
-// ppe.cu -- pressure Poisson equation of the semi-implicit step.
+// ppe.cu -- assembly and persistent CG solve of the pressure Poisson equation.
+//
+// The reference builds a dense np x np matrix and runs CG with cuBLAS gemv/dot
+// calls driven from the host, one host sync per dot product
+// (MPS_CAL_v4.0/cuda_ker.cu:171-297), or a dense CPU CG
+// (MPS_CAL_v4.0/MPS_CPU.cpp:829-888).  Here the matrix holds only the
+// neighbour stencil, and the whole solve is one cooperative kernel:
+//
+//   outer (defect correction, FP64): r64 = b - A x64; stop when
+//       |r64| <= tol |b| (FP64 norms of the true residual)
+//   inner (FP32 vectors, FP64 dot products): Jacobi-preconditioned CG on
+//       A d = r64 from d = 0 until |r| <= eta |r64|, with x64 += alpha p
+//       accumulated in FP64 as it goes.
+//
+// Grid-wide reductions are fused with a counter + generation barrier with a
+// bounded spin: a barrier that does not complete within ~1 s sets
+// ERR_DEVICE_TIMEOUT and the kernel returns.  Partial sums are added in a
+// fixed order, so the solve is bit-reproducible for a given device and grid.
+#include <cstring>
+#include <vector>
+
+#include "cellsort.cuh"
 #include "ppe.cuh"
 
 namespace mpsb {
 
-int ppe_setup(PpeWork& w, uint32_t, const Grid&, const Phys&, const mps_params&, cudaStream_t, std::string* err) {
-    w.ready = false;
-    *err = "semi-implicit method not available in this build";
-    return MPS_ERR_INVALID;
+static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;  // every lane's value is used only from lane 0
 }
-int ppe_enqueue(PpeWork&, const StageArgs&, const mps_options&, uint32_t, cudaStream_t) { return 0; }
-void ppe_free(PpeWork& w) { w.ready = false; }
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// fixed-order block sum of up to PPE_PARTS doubles, written to part[block]
+template <int K>
+__device__ void block_partials(const double (&v)[K], double* part) {
+    __shared__ double sm[K][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double t = warp_sum_d(v[k]);
+        if (lane == 0) sm[k][warp] = t;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double t = lane < nw ? sm[k][lane] : 0.0;
+            t = warp_sum_d(t);
+            if (lane == 0) part[blockIdx.x * PPE_PARTS + k] = t;
+        }
+    }
+    __syncthreads();
+}
+
+// Grid-wide sum of K doubles fused with a grid barrier.  Every block writes
+// its fixed-order block sum to part[block]; the last block to arrive adds the
+// partials in block order (lane-strided, then a fixed shuffle tree), writes
+// the totals to result[] and releases the others, which then read result[].
+// The totals are therefore identical in every block and on every run.  The
+// wait is bounded: after ~1 s it sets ERR_DEVICE_TIMEOUT and returns false.
+template <int K>
+__device__ bool grid_reduce(const double (&v)[K], double* part, double* result, unsigned* bar, Scalars* sc,
+                            double (&out)[K]) {
+    block_partials<K>(v, part);
+    __shared__ int last, ok;
+    __shared__ unsigned gen0;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned* gen = bar + 1;
+        gen0 = *gen;
+        __threadfence();
+        last = atomicAdd(bar, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+        if (threadIdx.x < 32) {
+            __threadfence();
+            const int lane = threadIdx.x;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                double t = 0.0;
+                for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(part + b * PPE_PARTS + k);
+                t = warp_sum_d(t);
+                if (lane == 0) result[k] = t;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        unsigned long long it = 0;
+        while (*gen == gen0) {
+            if (++it > (1ull << 24)) {
+                atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) out[k] = __ldcg(result + k);
+    const bool good = ok != 0;
+    __syncthreads();
+    return good;
+}
+
+// ---------------------------------------------------------------- assembly
+struct AsmArgs {
+    StageArgs a;
+    uint32_t* cols;
+    float* vals;
+    uint32_t* rlen;
+    double* diag64;
+    float* diag32;
+    float* inv_diag;
+    double* b64;
+    double* x64;
+    unsigned* bar;
+    double n0, lambda, beta, b_tmp, rho_lambda_alpha_n0, dim2;
+};
+
+// One warp per particle: scan the reference's 27 linked cells for rlap
+// neighbours of type != 2, accumulate the diagonal, append the non-Dirichlet
+// ones in ascending index order (MPS_CAL_v4.0/MPS_CPU.cpp:651-698).
+template <bool EX>
+__global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
+    const StageArgs& a = A.a;
+    const uint32_t n = a.sc->np;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.bar[0] = 0u;  // the solver's barrier starts empty
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float* __restrict__ nn = a.cur.n;
+    const float4 pi = pos[i];
+    const double ni = (double)nn[i];
+    const bool dir_i = ptype(pi) == T_DUMMY || ni < A.beta * A.n0;
+    if (dir_i) {
+        if (lane == 0) {
+            A.rlen[i] = PPE_DIRICHLET;
+            A.diag64[i] = 1.0;
+            A.diag32[i] = 1.0f;
+            A.inv_diag[i] = 1.0f;
+            A.b64[i] = 0.0;
+            A.x64[i] = 0.0;
+        }
+        return;
+    }
+    const double dt = (double)a.sc->dt;
+    const double Aii = A.rho_lambda_alpha_n0 / (A.dim2 * dt * dt);
+    const float re = a.P.rlap, thr = a.P.rlap_thr;
+    const double bthr = A.beta * A.n0;
+    uint32_t* cols = A.cols + (size_t)i * PPE_W;
+    float* vals = A.vals + (size_t)i * PPE_W;
+    uint32_t count = 0;
+    double diag = 0.0;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            bool app = false;
+            float w = 0.f;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                if (ptype(pj) != T_DUMMY) {
+                    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                    if (rr < thr) {
+                        w = weight_rr<EX>(re, rr);
+                        if (w > 0.f) app = !((double)__ldg(nn + j) < bthr);
+                    }
+                }
+            }
+            diag += (double)w;
+            const uint32_t m = __ballot_sync(0xffffffffu, app);
+            if (app) {
+                const uint32_t k = count + __popc(m & lt);
+                if (k < PPE_W) {
+                    cols[k] = j;
+                    vals[k] = w;
+                }
+            }
+            count += __popc(m);
+        }
+    }
+    diag = warp_sum_d(diag);
+    if (lane == 0) {
+        if (count > PPE_W) {
+            atomicOr(&a.sc->err, ERR_CAPACITY);  // more than PPE_W neighbours
+            count = PPE_W;
+        }
+        const double dg = -diag - Aii;
+        A.rlen[i] = count;
+        A.diag64[i] = dg;
+        A.diag32[i] = (float)dg;
+        A.inv_diag[i] = (float)(1.0 / dg);
+        A.b64[i] = A.b_tmp * (A.n0 - ni);
+        A.x64[i] = (double)a.cur.press[i];
+    }
+}
+
+// ---------------------------------------------------------------- solve
+struct SolveArgs {
+    const uint32_t* cols;
+    const float* vals;
+    const uint32_t* rlen;
+    const double* diag64;
+    const float* diag32;
+    const float* inv_diag;
+    const double* b64;
+    double* x64;
+    float* r;
+    float* z;
+    float* q;
+    float* p0;
+    float* p1;
+    double* part;
+    double* result;
+    unsigned* bar;
+    const uint32_t* rowlist;
+    const uint32_t* nrows;
+    const uint32_t* off;
+    const uint32_t* scols;
+    const float* svals;
+    Scalars* sc;
+    double tol;
+    int max_iter;
+    int inner_cap;
+    int max_outer;
+};
+
+__global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
+    // Rows are the ordered list of non-Dirichlet rows; slices of 32 of them
+    // are dealt to warps round-robin (one thread per row inside a slice),
+    // and each block owns an equal contiguous range of the list for the
+    // row-wise vector updates.
+    const uint32_t R = *S.nrows;
+    const uint32_t nslices = (R + 31) / 32;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t* __restrict__ rowlist = S.rowlist;
+    int total = 0;
+    double relres = 0.0;
+    bool converged = false;
+    float* pcur = S.p0;
+    float* pnew = S.p1;
+    for (int outer = 0; outer < S.max_outer; outer++) {
+        // ---- true residual r64 = b - A x64 (FP64), inner start: z = M^-1 r, p = 0
+        double acc[3] = {0.0, 0.0, 0.0};  // |r64|^2, |b|^2, r.z
+        for (uint32_t sl = gw; sl < nslices; sl += nw) {
+            const uint32_t k = sl * 32 + lane;
+            const uint32_t base = __ldg(S.off + sl);
+            const uint32_t W = (__ldg(S.off + sl + 1) - base) >> 5;
+            const uint32_t* cols = S.scols + base + lane;
+            const float* vals = S.svals + base + lane;
+            double s = 0.0;
+            for (uint32_t e = 0; e < W; e++) s += (double)__ldg(vals + 32 * e) * S.x64[__ldg(cols + 32 * e)];
+            if (k < R) {
+                const uint32_t i = __ldg(rowlist + k);
+                const double bi = S.b64[i];
+                const double ri = bi - (S.diag64[i] * S.x64[i] + s);
+                const float rf = (float)ri;
+                const float zf = rf * S.inv_diag[i];
+                S.r[i] = rf;
+                S.z[i] = zf;
+                pcur[i] = 0.f;
+                acc[0] += ri * ri;
+                acc[1] += bi * bi;
+                acc[2] += (double)rf * (double)zf;
+            }
+        }
+        double tot[3];
+        if (!grid_reduce<3>(acc, S.part, S.result, S.bar, S.sc, tot)) return;
+        const double rr64 = tot[0], bb = tot[1];
+        relres = bb > 0.0 ? sqrt(rr64 / bb) : 0.0;
+        if (relres <= S.tol) {
+            converged = true;
+            break;
+        }
+        if (total >= S.max_iter) break;
+        // inner target |r| <= eta |r64|
+        double eta = 0.3 * S.tol / relres;
+        if (eta < 1e-4) eta = 1e-4;
+        if (eta > 0.5) eta = 0.5;
+        const double stop = eta * eta * rr64;
+        double rz = tot[2];
+        float beta = 0.f;
+        for (int it = 0; it < S.inner_cap && total < S.max_iter; it++) {
+            // ---- q = A p_new with p_new = z + beta p (fused), p.q
+            double pq[1] = {0.0};
+            for (uint32_t sl = gw; sl < nslices; sl += nw) {
+                const uint32_t k = sl * 32 + lane;
+                const uint32_t base = __ldg(S.off + sl);
+                const uint32_t W = (__ldg(S.off + sl + 1) - base) >> 5;
+                const uint32_t* cols = S.scols + base + lane;
+                const float* vals = S.svals + base + lane;
+                float s0 = 0.f, s1 = 0.f;
+                uint32_t e = 0;
+                for (; e + 8 <= W; e += 8) {
+                    uint32_t j[8];
+                    float w[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        j[u] = __ldg(cols + 32 * (e + u));
+                        w[u] = __ldg(vals + 32 * (e + u));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u += 2) {
+                        s0 = fmaf(w[u], fmaf(beta, pcur[j[u]], S.z[j[u]]), s0);
+                        s1 = fmaf(w[u + 1], fmaf(beta, pcur[j[u + 1]], S.z[j[u + 1]]), s1);
+                    }
+                }
+                for (; e < W; e++) {
+                    const uint32_t jj = __ldg(cols + 32 * e);
+                    s0 = fmaf(__ldg(vals + 32 * e), fmaf(beta, pcur[jj], S.z[jj]), s0);
+                }
+                if (k < R) {
+                    const uint32_t i = __ldg(rowlist + k);
+                    const float pn = fmaf(beta, pcur[i], S.z[i]);
+                    const float qi = fmaf(S.diag32[i], pn, s0 + s1);
+                    pnew[i] = pn;
+                    S.q[i] = qi;
+                    pq[0] += (double)pn * (double)qi;
+                }
+            }
+            double totp[1];
+            if (!grid_reduce<1>(pq, S.part, S.result, S.bar, S.sc, totp)) return;
+            const double alpha = rz / totp[0];
+            const float alpha_f = (float)alpha;
+            // ---- x64 += alpha p, r -= alpha q, z = M^-1 r, r.z, r.r
+            double acc2[2] = {0.0, 0.0};
+            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                const uint32_t i = __ldg(rowlist + kk);
+                const float pn = pnew[i];
+                S.x64[i] += alpha * (double)pn;
+                const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
+                const float zi = ri * S.inv_diag[i];
+                S.r[i] = ri;
+                S.z[i] = zi;
+                acc2[0] += (double)ri * (double)zi;
+                acc2[1] += (double)ri * (double)ri;
+            }
+            double tot2[2];
+            if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
+            total++;
+            beta = (float)(tot2[0] / rz);
+            rz = tot2[0];
+            float* t = pcur;
+            pcur = pnew;
+            pnew = t;
+            if (tot2[1] <= stop) break;
+        }
+        // the last inner iteration ended on a grid-wide reduction, so every
+        // x64 update is visible to the residual pass of the next round
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S.sc->cg_iters = total;
+        S.sc->cg_relres = relres;
+        if (!converged) atomicOr(&S.sc->err, ERR_CG_NOT_CONVERGED);
+    }
+}
+
+// ---------------------------------------------------------------- row list
+// Ordered list of the non-Dirichlet rows: the solver splits it into equal
+// contiguous slices per block (Dirichlet and dummy rows cluster in space, so
+// slicing the particle range would leave some blocks idle).
+constexpr uint32_t ROW_TILE = 2048;
+
+__global__ void __launch_bounds__(256) k_rows_count(const uint32_t* __restrict__ rlen, const Scalars* __restrict__ sc,
+                                                    uint32_t* __restrict__ tilecnt) {
+    const uint32_t n = sc->np;
+    const uint32_t base = blockIdx.x * ROW_TILE;
+    uint32_t c = 0;
+    for (uint32_t k = threadIdx.x; k < ROW_TILE; k += blockDim.x) {
+        const uint32_t i = base + k;
+        if (i < n && rlen[i] != PPE_DIRICHLET) c++;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    __shared__ uint32_t ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; w++) t += ws[w];
+        tilecnt[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_rows_scatter(const uint32_t* __restrict__ rlen, const Scalars* __restrict__ sc,
+                                                      const uint32_t* __restrict__ tileoff, uint32_t ntiles,
+                                                      uint32_t* __restrict__ rowlist, uint32_t* __restrict__ nrows) {
+    const uint32_t n = sc->np;
+    const uint32_t base = blockIdx.x * ROW_TILE;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ uint32_t ws[8];
+    __shared__ uint32_t run;
+    if (threadIdx.x == 0) run = tileoff[blockIdx.x];
+    __syncthreads();
+    for (uint32_t k0 = 0; k0 < ROW_TILE; k0 += blockDim.x) {
+        const uint32_t i = base + k0 + threadIdx.x;
+        const bool f = i < n && rlen[i] != PPE_DIRICHLET;
+        const uint32_t m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) ws[warp] = __popc(m);
+        __syncthreads();
+        uint32_t off = run;
+        for (uint32_t w = 0; w < warp; w++) off += ws[w];
+        if (f) rowlist[off + __popc(m & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int w = 0; w < 8; w++) t += ws[w];
+            run += t;
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) *nrows = run;
+}
+
+// ---------------------------------------------------------------- SELL-32
+// Sliced ELL: slice s holds rows rowlist[32s .. 32s+31], width W_s = the
+// longest of them, entries column-major (entry k of lane l at
+// sell_off[s] + 32k + l), padded with the row's own index and weight 0.
+__global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__ rlen,
+                                                    const uint32_t* __restrict__ rowlist,
+                                                    const uint32_t* __restrict__ nrows, uint32_t* __restrict__ width32) {
+    const uint32_t R = *nrows;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
+    const uint32_t nslices = (R + 31) / 32;
+    const uint32_t slice = k >> 5;
+    if (slice >= nslices) {
+        if ((k & 31) == 0) width32[slice] = 0u;
+        return;
+    }
+    const uint32_t len = k < R ? rlen[rowlist[k]] : 0u;
+    const uint32_t m = __reduce_max_sync(0xffffffffu, len);
+    if ((k & 31) == 0) width32[slice] = 32u * m;
+}
+
+__global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm, const float* __restrict__ vals_rm,
+                                                   const uint32_t* __restrict__ rlen, const uint32_t* __restrict__ rowlist,
+                                                   const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
+                                                   uint32_t* __restrict__ scols, float* __restrict__ svals) {
+    const uint32_t R = *nrows;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slice = k >> 5, lane = k & 31;
+    if (slice >= (R + 31) / 32) return;
+    const uint32_t base = off[slice];
+    const uint32_t W = (off[slice + 1] - base) >> 5;
+    const bool has = k < R;
+    const uint32_t i = has ? rowlist[k] : 0u;
+    const uint32_t len = has ? rlen[i] : 0u;
+    const uint32_t* rc = cols_rm + (size_t)i * PPE_W;
+    const float* rv = vals_rm + (size_t)i * PPE_W;
+    for (uint32_t e = 0; e < W; e++) {
+        const bool real = e < len;
+        scols[base + 32u * e + lane] = real ? rc[e] : i;
+        svals[base + 32u * e + lane] = real ? rv[e] : 0.f;
+    }
+}
+
+// p = max(x, 0) (pressCorr, MPS_CAL_v4.0/MPS_CPU.cpp:734-743); Dirichlet rows 0.
+__global__ void __launch_bounds__(256) k_ppe_finish(const double* __restrict__ x64, const uint32_t* __restrict__ rlen,
+                                                    float* __restrict__ press, const Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float p = 0.f;
+    if (rlen[i] != PPE_DIRICHLET) {
+        p = (float)x64[i];
+        if (p < 0.f) p = 0.f;
+    }
+    press[i] = p;
+}
+
+// ---------------------------------------------------------------- FP64 init
+// n of every particle in double (weights from the float positions in double)
+__global__ void __launch_bounds__(256) k_pnd64(StageArgs a, double* __restrict__ n64) {
+    const uint32_t n = a.sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4 pi = pos[i];
+    const double re = (double)a.P.rzero;
+    double acc = 0.0;
+    const uint32_t c = a.cur.cell[i];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            if (j == i) continue;
+            const float4 pj = __ldg(pos + j);
+            const double dx = (double)pj.x - pi.x, dy = (double)pj.y - pi.y, dz = (double)pj.z - pi.z;
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (r < re) acc += re / r - 1.0;
+        }
+    }
+    n64[i] = acc;
+    a.cur.n[i] = (float)acc;
+}
+
+void launch_pnd64(const StageArgs& a, double* n64, uint32_t cap, cudaStream_t st) {
+    k_pnd64<<<blocks_for(cap, 256), 256, 0, st>>>(a, n64);
+}
+
+// n0 = the first maximum of n in GEO.dat order (the reference's calOnce
+// runs before the first sort, MPS_CAL_v4.0/MPS.cpp:316-333): the largest n64,
+// smallest id on ties; then lambda = sum r^2 w(r; r0) / n0 around it
+// (MPS.cpp:335-348).  One block.
+__global__ void __launch_bounds__(1024) k_n0_lambda64(StageArgs a, const double* __restrict__ n64, double* out) {
+    __shared__ double sn[1024];
+    __shared__ uint32_t sid[1024], sidx[1024];
+    const uint32_t np = a.sc->np;
+    double bn = -1.0;
+    uint32_t bid = 0xffffffffu, bix = 0xffffffffu;
+    for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) {
+        const double v = n64[i];
+        const uint32_t id = a.cur.id[i];
+        if (v > bn || (v == bn && id < bid)) { bn = v; bid = id; bix = i; }
+    }
+    sn[threadIdx.x] = bn; sid[threadIdx.x] = bid; sidx[threadIdx.x] = bix;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            const double v = sn[threadIdx.x + o];
+            const uint32_t id = sid[threadIdx.x + o];
+            if (v > sn[threadIdx.x] || (v == sn[threadIdx.x] && id < sid[threadIdx.x])) {
+                sn[threadIdx.x] = v; sid[threadIdx.x] = id; sidx[threadIdx.x] = sidx[threadIdx.x + o];
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const uint32_t t = sidx[0];
+    const double n0 = sn[0];
+    if (t == 0xffffffffu || !(n0 > 0.0)) { out[0] = 0.0; out[1] = 0.0; return; }
+    const float4 pt = a.cur.pos[t];
+    const double re = (double)a.P.rzero;
+    double lam = 0.0;
+    const uint32_t c = a.cur.cell[t];
+    const int rows = link_rows(a.g);
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        for (uint32_t j = rg.lo; j < rg.hi; j++) {
+            if (j == t) continue;
+            const float4 pj = a.cur.pos[j];
+            const double dx = (double)pj.x - pt.x, dy = (double)pj.y - pt.y, dz = (double)pj.z - pt.z;
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (r < re) lam += r * r * (re / r - 1.0);
+        }
+    }
+    out[0] = n0;
+    out[1] = lam / n0;
+}
+
+void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st) {
+    k_n0_lambda64<<<1, 1024, 0, st>>>(a, n64, out);
+}
+
+// ---------------------------------------------------------------- host side
+int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_params& prm, cudaStream_t st,
+              std::string* err) {
+    w.cap = cap;
+    w.alpha64 = 1.0 / ((double)prm.rho * (double)prm.cs * (double)prm.cs);
+    auto al = [&](void** p, size_t bytes) -> bool {
+        if (cudaMalloc(p, bytes + 64) != cudaSuccess) return false;
+        cudaMemsetAsync(*p, 0, bytes + 64, st);
+        return true;
+    };
+    bool ok = true;
+    ok &= al((void**)&w.cols, (size_t)cap * PPE_W * sizeof(uint32_t));
+    ok &= al((void**)&w.vals, (size_t)cap * PPE_W * sizeof(float));
+    ok &= al((void**)&w.rlen, (size_t)cap * sizeof(uint32_t));
+    ok &= al((void**)&w.diag64, (size_t)cap * sizeof(double));
+    ok &= al((void**)&w.diag32, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.inv_diag, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.b64, (size_t)cap * sizeof(double));
+    ok &= al((void**)&w.x64, (size_t)cap * sizeof(double));
+    ok &= al((void**)&w.r, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.z, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.p[0], (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.p[1], (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_off, ((size_t)cap / 32 + 4) * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_cols, ((size_t)cap + 32) * PPE_W * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_vals, ((size_t)cap + 32) * PPE_W * sizeof(float));
+    ok &= al((void**)&w.tilecnt, ((size_t)cap / 2048 + 2) * sizeof(uint32_t));
+    ok &= al((void**)&w.nrows, sizeof(uint32_t));
+    if (!ok) {
+        *err = "cudaMalloc failed for the PPE matrix";
+        return MPS_ERR_CUDA;
+    }
+    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppe_solve, PPE_THREADS, 0);
+    if (!coop || per_sm < 1) {
+        *err = "device cannot run the cooperative PPE solver";
+        return MPS_ERR_CUDA;
+    }
+    if (per_sm > 2) per_sm = 2;
+    w.blocks = sms * per_sm;
+    ok &= al((void**)&w.part, (size_t)w.blocks * PPE_PARTS * sizeof(double));
+    ok &= al((void**)&w.result, PPE_PARTS * sizeof(double));
+    ok &= al((void**)&w.bar, 2 * sizeof(unsigned));
+    if (!ok) {
+        *err = "cudaMalloc failed for the PPE scratch";
+        return MPS_ERR_CUDA;
+    }
+    w.ready = true;
+    return MPS_OK;
+}
+
+int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
+    AsmArgs A;
+    A.a = a;
+    A.cols = w.cols;
+    A.vals = w.vals;
+    A.rlen = w.rlen;
+    A.diag64 = w.diag64;
+    A.diag32 = w.diag32;
+    A.inv_diag = w.inv_diag;
+    A.b64 = w.b64;
+    A.x64 = w.x64;
+    A.bar = w.bar;
+    A.n0 = w.n0_64;
+    A.lambda = w.lambda64;
+    A.beta = (double)a.P.beta;
+    const double rho = (double)a.P.rho, dim = (double)a.P.dim_f;
+    const double alpha = w.alpha64;
+    const double one_over_dt = 1.0 / (double)a.P.dt_max;
+    A.b_tmp = w.lambda64 * rho * (0.5 * (1.0 / dim) * one_over_dt * one_over_dt);
+    A.rho_lambda_alpha_n0 = rho * w.lambda64 * alpha * w.n0_64;
+    A.dim2 = 2.0 * dim;
+    const uint32_t warps_blocks = blocks_for(cap * 32u, 256);
+    if (a.exact) k_ppe_assemble<true><<<warps_blocks, 256, 0, st>>>(A);
+    else k_ppe_assemble<false><<<warps_blocks, 256, 0, st>>>(A);
+
+    SolveArgs S;
+    S.cols = w.cols;
+    S.vals = w.vals;
+    S.rlen = w.rlen;
+    S.diag64 = w.diag64;
+    S.diag32 = w.diag32;
+    S.inv_diag = w.inv_diag;
+    S.b64 = w.b64;
+    S.x64 = w.x64;
+    S.r = w.r;
+    S.z = w.z;
+    S.q = w.q;
+    S.p0 = w.p[0];
+    S.p1 = w.p[1];
+    S.part = w.part;
+    S.result = w.result;
+    S.bar = w.bar;
+    S.rowlist = w.rowlist;
+    S.nrows = w.nrows;
+    S.off = w.sell_off;
+    S.scols = w.sell_cols;
+    S.svals = w.sell_vals;
+    S.sc = a.sc;
+    S.tol = opt.cg_tol;
+    S.max_iter = opt.cg_max_iter;
+    S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
+    S.max_outer = 40;
+    const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
+    k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
+    launch_scan_exclusive(w.tilecnt, ntiles, st);
+    k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
+    // SELL-32 layout of the non-Dirichlet rows
+    const uint32_t maxslices = (cap + 31) / 32;
+    k_sell_width<<<blocks_for((maxslices + 1) * 32u, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off);
+    launch_scan_exclusive(w.sell_off, maxslices + 1, st);
+    k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.vals, w.rlen, w.rowlist, w.nrows,
+                                                                  w.sell_off, w.sell_cols, w.sell_vals);
+    void* args[] = {&S};
+    w.launch_err = cudaLaunchCooperativeKernel((const void*)k_ppe_solve, w.blocks, PPE_THREADS, args, 0, st);
+    k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
+    return 9;
+}
+
+void ppe_free(PpeWork& w) {
+    void* ps[] = {w.cols, w.vals, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
+                  w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar, w.gvals,
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_vals};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    w = PpeWork();
+}
 
 }  // namespace mpsb

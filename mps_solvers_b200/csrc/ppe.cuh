@@ -1,4 +1,15 @@
 // ppe.cuh -- pressure Poisson equation of the semi-implicit step.
+//
+// MPS_CPU::buildPoisson + solvePoisson + pressCorr (MPS_CAL_v4.0/MPS_CPU.cpp:619-743):
+// for a particle i of type != 2 with n_i >= beta n0 (not Dirichlet)
+//   A_ij = w(r_ij; rlap)            for neighbours j of type != 2, not Dirichlet
+//   A_ii = -sum_j w(r_ij; rlap) - rho lambda alpha n0 / (2 d dt^2)   (all type != 2 neighbours)
+//   b_i  = lambda rho / (2 d dt_max^2) (n0 - n_i)
+// Dirichlet rows (n_i < beta n0 or type 2) are identity rows with b = 0, so
+// their solution is 0 and they are left out of the solve.  Then p = max(x, 0).
+//
+// Storage: row-major with a fixed stride of PPE_W entries per particle
+// (column index + float weight), the diagonal in double.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -9,8 +20,37 @@
 
 namespace mpsb {
 
+constexpr uint32_t PPE_W = 352;        // stride: > the 256 lattice neighbours within 4 l0
+constexpr uint32_t PPE_DIRICHLET = 0xffffffffu;
+constexpr int PPE_THREADS = 512;
+constexpr int PPE_PARTS = 4;           // FP64 partial sums per block
+
 struct PpeWork {
     bool ready = false;
+    uint32_t cap = 0;
+    int blocks = 0;                    // co-resident blocks of the persistent solver
+    uint32_t* cols = nullptr;          // cap * PPE_W
+    float* vals = nullptr;             // cap * PPE_W
+    uint32_t* rlen = nullptr;          // off-diagonal count, PPE_DIRICHLET for Dirichlet rows
+    double* diag64 = nullptr;
+    float* diag32 = nullptr;
+    float* inv_diag = nullptr;
+    double* b64 = nullptr;
+    double* x64 = nullptr;
+    float *r = nullptr, *z = nullptr, *q = nullptr, *p[2] = {nullptr, nullptr};
+    double* part = nullptr;            // blocks * PPE_PARTS
+    double* result = nullptr;          // PPE_PARTS grid totals
+    uint32_t* rowlist = nullptr;       // non-Dirichlet rows in particle order
+    uint32_t* tilecnt = nullptr;
+    uint32_t* nrows = nullptr;
+    uint32_t* sell_off = nullptr;      // slice offsets (exclusive scan of 32 * width)
+    uint32_t* sell_cols = nullptr;
+    float* sell_vals = nullptr;
+    unsigned* bar = nullptr;           // [0] arrival count, [1] generation
+    // preconditioner (learned factor G); unused for the diagonal one
+    float* gvals = nullptr;
+    double n0_64 = 0.0, lambda64 = 0.0, alpha64 = 0.0;
+    cudaError_t launch_err = cudaSuccess;  // of the last cooperative launch
 };
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
@@ -18,5 +58,11 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_
 // returns the number of kernels enqueued
 int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);
+
+// FP64 particle number density of every particle (initialisation of the
+// semi-implicit method: n0 and lambda in double, MPS_CAL_v4.0/MPS.cpp:305-361)
+void launch_pnd64(const StageArgs& a, double* n64, uint32_t cap, cudaStream_t st);
+// out[0] = n0, out[1] = lambda (double)
+void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st);
 
 }  // namespace mpsb

@@ -1,0 +1,107 @@
+"""Semi-implicit step (PPE + CG) on the GPU through the C ABI.
+
+The GPU keeps particles in float (FP32 sums and SpMV) and solves the PPE to
+|b - Ax| <= 1e-8 |b| measured in FP64 (defect correction); the oracle runs
+the same two-phase rules in double with CG to 1e-12.  Stated tolerances,
+relative to each field's largest magnitude after 8 steps: pressure 2e-3,
+velocity 1e-3, positions 1e-6 of the domain size.
+"""
+import numpy as np
+import pytest
+
+from helpers import load_golden, rel_err, write_golden_case
+
+pytestmark = pytest.mark.gpu
+
+P_TOL, U_TOL, X_TOL = 2e-3, 1e-3, 1e-6
+
+
+def by_id(st):
+    o = np.argsort(st["id"], kind="stable")
+    return {k: v[o] for k, v in st.items()}
+
+
+def compare(a, b):
+    a, b = by_id(a), by_id(b)
+    assert np.array_equal(a["id"], b["id"])
+    assert np.array_equal(a["type"], b["type"])
+    ext = np.abs(b["pos"]).max()
+    ex = np.abs(a["pos"] - b["pos"]).max() / ext
+    ep = rel_err(a["press"], b["press"])
+    eu = rel_err(a["vel"], b["vel"])
+    return ex, eu, ep
+
+
+def test_semi_steps_vs_fp64_oracle(capi, oracle_mod, tmp_path):
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    orc = oracle_mod.Oracle(d, oracle_mod.SEMI_JACOBI, 64)
+    orc.set_cg(True, 1e-12, 100000)
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
+        for k in range(8):
+            st = s.step(1)
+            orc.step(1)
+            assert st.cg_relres <= 1e-8 and st.cg_iters > 0
+        ex, eu, ep = compare(s.state(), orc.state())
+        assert orc.state()["press"].max() > 100.0
+    assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
+
+
+def test_semi_steps_vs_reference_golden(capi, tmp_path):
+    """Against the reference's own sequential build (MPS_CAL_v4.0, double,
+    dense CG): the two-phase form differs from it by ~2e-5 in velocity (see
+    tests/test_oracle_golden.py), within the same stated tolerances."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
+        s.step(8)
+        a = s.state()
+    ref = {f: g[f"s8_{f}"] for f in ("id", "type", "pos", "vel", "press", "n")}
+    ex, eu, ep = compare(a, ref)
+    assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
+
+
+def test_ppe_solution_meets_fp64_tolerance_and_is_reproducible(capi, tmp_path):
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    out = []
+    for _ in range(2):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, cg_tol=1e-10) as s:
+            st = s.step(6)
+            assert st.cg_relres <= 1e-10
+            out.append(s.state())
+    for f in ("pos", "vel", "press"):
+        assert np.array_equal(out[0][f], out[1][f]), f
+
+
+def test_cg_not_converged_is_reported(capi, tmp_path):
+    """An iteration limit too small for the tolerance returns
+    MPS_ERR_CG_NOT_CONVERGED instead of a silent result."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, cg_max_iter=2) as s:
+        s.step(5, check=False)
+        st = s.step(1, check=False)
+        assert st.status == 5
+
+
+def test_full_size_semi_dam_break(capi, oracle_mod, tmp_path):
+    """310,912-particle semi-implicit dam break: 2 steps against the FP64
+    oracle (same tolerances), then 20 more steps converging every PPE."""
+    from mps_solvers_b200 import scene
+    d = str(tmp_path / "c2")
+    scene.write_case(d, scene.dam_break_semi())
+    orc = oracle_mod.Oracle(d, oracle_mod.SEMI_JACOBI, 64)
+    orc.set_cg(True, 1e-12, 100000)
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
+        for _ in range(2):
+            st = s.step(1)
+            orc.step(1)
+            assert st.cg_relres <= 1e-8
+        ex, eu, ep = compare(s.state(), orc.state())
+        assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
+        for _ in range(20):
+            st = s.step(1)
+            assert st.cg_relres <= 1e-8 and st.status == 0
+        a = s.state()
+        assert np.isfinite(a["press"]).all() and a["press"].min() >= 0.0
