@@ -108,8 +108,13 @@ class ClockSampler:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def make_scene(workload: str, seed: int):
+def make_scene(workload: str, seed: int, size: str = "full"):
     from mps_solvers_b200 import scene
+    if size == "small":
+        # a ~110k-particle tank at the same resolution, for detailed profiles
+        sc = scene.small_tank(seed=seed, interior=(80, 30, 60), fluid=(30, 20, 45), l0=0.01,
+                              dt=1e-4 if workload == "explicit" else 5e-4)
+        return sc
     if workload == "explicit":
         return scene.dam_break_explicit(seed=seed)
     return scene.dam_break_semi(seed=seed)
@@ -200,7 +205,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     method = capi.METHOD_EXPLICIT if args.workload == "explicit" else capi.METHOD_SEMI_IMPLICIT
     arith = capi.ARITH_EXACT if args.arith == "exact" else capi.ARITH_FAST
     tmpd = tempfile.mkdtemp(prefix=f"mpsb_{rank}_")
-    pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank))
+    pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
     n = len(pos0)
     sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1)
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
@@ -278,7 +283,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if method == capi.METHOD_EXPLICIT else "f32+f64",
         "data": "synthetic",
-        "config": {"workload": workload_name(args.workload), "particles": n,
+        "config": {"workload": workload_name(args.workload) if args.size == "full" else
+                   f"{args.workload} small profiling tank", "particles": n,
                    "fluid": int(n - nb2 - nb1), "arith": args.arith,
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -322,6 +328,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="explicit", choices=["explicit", "semi"])
     ap.add_argument("--arith", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--size", default="full", choices=["full", "small"],
+                    help="small: a ~110k-particle tank of the same kernels (profiling)")
     ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -71,39 +71,48 @@ __global__ void __launch_bounds__(SORT_THREADS) k_radix_upsweep(const uint32_t* 
     for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) hist[d * tiles + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of `total` counters by one block.
+// Exclusive scan of `total` counters by one block: chunks of 4096 entries,
+// each thread loading 4 consecutive counters (coalesced), a block scan of
+// the thread sums, and a running carry between chunks.
 __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, uint32_t total) {
     __shared__ uint32_t warp_sums[32];
-    const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
-    const uint32_t b0 = threadIdx.x * per;
-    const uint32_t b1 = min(total, b0 + per);
-    uint32_t s = 0;
-    for (uint32_t k = b0; k < b1; k++) s += a[k];
-    // block exclusive scan of s
+    __shared__ uint32_t carry;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t v = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    if (lane == 31) warp_sums[warp] = v;
+    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    if (warp == 0) {
-        uint32_t w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0u;
+    for (uint32_t c0 = 0; c0 < total; c0 += 4096) {
+        const uint32_t b0 = c0 + 4 * threadIdx.x;
+        uint32_t v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = (b0 + u < total) ? a[b0 + u] : 0u;
+        const uint32_t s = v[0] + v[1] + v[2] + v[3];
+        uint32_t x = s;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
+            const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
         }
-        warp_sums[lane] = w;  // inclusive over warps
-    }
-    __syncthreads();
-    uint32_t run = v - s + (warp > 0 ? warp_sums[warp - 1] : 0u);
-    for (uint32_t k = b0; k < b1; k++) {
-        uint32_t t = a[k];
-        a[k] = run;
-        run += t;
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += t;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        uint32_t run = carry + (x - s) + (warp > 0 ? warp_sums[warp - 1] : 0u);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (b0 + u < total) a[b0 + u] = run;
+            run += v[u];
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = run;
+        __syncthreads();
     }
 }
 

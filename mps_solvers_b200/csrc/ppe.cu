@@ -86,8 +86,17 @@ __device__ bool grid_reduce(const double (&v)[K], double* part, double* result, 
             const int lane = threadIdx.x;
 #pragma unroll
             for (int k = 0; k < K; k++) {
+                // up to 8 partials per lane loaded before adding (latency)
+                double v8[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const unsigned b = lane + 32u * u;
+                    v8[u] = b < gridDim.x ? __ldcg(part + b * PPE_PARTS + k) : 0.0;
+                }
                 double t = 0.0;
-                for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(part + b * PPE_PARTS + k);
+#pragma unroll
+                for (int u = 0; u < 8; u++) t += v8[u];
+                for (unsigned b = lane + 256u; b < gridDim.x; b += 32) t += __ldcg(part + b * PPE_PARTS + k);
                 t = warp_sum_d(t);
                 if (lane == 0) result[k] = t;
             }
@@ -249,13 +258,13 @@ struct SolveArgs {
 };
 
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
-    // Rows are the ordered list of non-Dirichlet rows; slices of 32 of them
-    // are dealt to warps round-robin (one thread per row inside a slice),
-    // and each block owns an equal contiguous range of the list for the
-    // row-wise vector updates.
+    // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them
+    // are dealt to warps round-robin (4 lanes per row inside a slice); the
+    // row-wise vector updates take one thread per row.
     const uint32_t R = *S.nrows;
-    const uint32_t nslices = (R + 31) / 32;
+    const uint32_t nslices = (R + SELL_C - 1) / SELL_C;
     const uint32_t lane = threadIdx.x & 31;
+    const uint32_t rsub = lane & 7, q = lane >> 3;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t* __restrict__ rowlist = S.rowlist;
@@ -268,14 +277,16 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         // ---- true residual r64 = b - A x64 (FP64), inner start: z = M^-1 r, p = 0
         double acc[3] = {0.0, 0.0, 0.0};  // |r64|^2, |b|^2, r.z
         for (uint32_t sl = gw; sl < nslices; sl += nw) {
-            const uint32_t k = sl * 32 + lane;
+            const uint32_t k = sl * SELL_C + rsub;
             const uint32_t base = __ldg(S.off + sl);
-            const uint32_t W = (__ldg(S.off + sl + 1) - base) >> 5;
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
             const uint32_t* cols = S.scols + base + lane;
             const float* vals = S.svals + base + lane;
             double s = 0.0;
-            for (uint32_t e = 0; e < W; e++) s += (double)__ldg(vals + 32 * e) * S.x64[__ldg(cols + 32 * e)];
-            if (k < R) {
+            for (uint32_t t = 0; t < T; t++) s += (double)__ldg(vals + 32 * t) * S.x64[__ldg(cols + 32 * t)];
+            s += __shfl_xor_sync(0xffffffffu, s, 8);
+            s += __shfl_xor_sync(0xffffffffu, s, 16);
+            if (q == 0 && k < R) {
                 const uint32_t i = __ldg(rowlist + k);
                 const double bi = S.b64[i];
                 const double ri = bi - (S.diag64[i] * S.x64[i] + s);
@@ -309,20 +320,20 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             // ---- q = A p_new with p_new = z + beta p (fused), p.q
             double pq[1] = {0.0};
             for (uint32_t sl = gw; sl < nslices; sl += nw) {
-                const uint32_t k = sl * 32 + lane;
+                const uint32_t k = sl * SELL_C + rsub;
                 const uint32_t base = __ldg(S.off + sl);
-                const uint32_t W = (__ldg(S.off + sl + 1) - base) >> 5;
+                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
                 const uint32_t* cols = S.scols + base + lane;
                 const float* vals = S.svals + base + lane;
                 float s0 = 0.f, s1 = 0.f;
-                uint32_t e = 0;
-                for (; e + 8 <= W; e += 8) {
+                uint32_t t = 0;
+                for (; t + 8 <= T; t += 8) {
                     uint32_t j[8];
                     float w[8];
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
-                        j[u] = __ldg(cols + 32 * (e + u));
-                        w[u] = __ldg(vals + 32 * (e + u));
+                        j[u] = __ldg(cols + 32 * (t + u));
+                        w[u] = __ldg(vals + 32 * (t + u));
                     }
 #pragma unroll
                     for (int u = 0; u < 8; u += 2) {
@@ -330,14 +341,17 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                         s1 = fmaf(w[u + 1], fmaf(beta, pcur[j[u + 1]], S.z[j[u + 1]]), s1);
                     }
                 }
-                for (; e < W; e++) {
-                    const uint32_t jj = __ldg(cols + 32 * e);
-                    s0 = fmaf(__ldg(vals + 32 * e), fmaf(beta, pcur[jj], S.z[jj]), s0);
+                for (; t < T; t++) {
+                    const uint32_t jj = __ldg(cols + 32 * t);
+                    s0 = fmaf(__ldg(vals + 32 * t), fmaf(beta, pcur[jj], S.z[jj]), s0);
                 }
-                if (k < R) {
+                float s = s0 + s1;
+                s += __shfl_xor_sync(0xffffffffu, s, 8);
+                s += __shfl_xor_sync(0xffffffffu, s, 16);
+                if (q == 0 && k < R) {
                     const uint32_t i = __ldg(rowlist + k);
                     const float pn = fmaf(beta, pcur[i], S.z[i]);
-                    const float qi = fmaf(S.diag32[i], pn, s0 + s1);
+                    const float qi = fmaf(S.diag32[i], pn, s);
                     pnew[i] = pn;
                     S.q[i] = qi;
                     pq[0] += (double)pn * (double)qi;
@@ -436,24 +450,27 @@ __global__ void __launch_bounds__(256) k_rows_scatter(const uint32_t* __restrict
     if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) *nrows = run;
 }
 
-// ---------------------------------------------------------------- SELL-32
-// Sliced ELL: slice s holds rows rowlist[32s .. 32s+31], width W_s = the
-// longest of them, entries column-major (entry k of lane l at
-// sell_off[s] + 32k + l), padded with the row's own index and weight 0.
+// ---------------------------------------------------------------- SELL-8
+// Sliced ELL: slice s holds rows rowlist[8s .. 8s+7], width W_s = the
+// longest of them rounded up to a multiple of 4, entries column-major
+// (entry e of row r at sell_off[s] + 8e + r), padded with the row's own index
+// and weight 0.  A warp takes one slice with 4 lanes per row: lane L = 8q + r
+// reads entries e = 4t + q, i.e. address 32t + L, so every load is one
+// coalesced 128-byte line.
 __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__ rlen,
                                                     const uint32_t* __restrict__ rowlist,
-                                                    const uint32_t* __restrict__ nrows, uint32_t* __restrict__ width32) {
+                                                    const uint32_t* __restrict__ nrows, uint32_t* __restrict__ width,
+                                                    uint32_t maxslices) {
     const uint32_t R = *nrows;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
-    const uint32_t nslices = (R + 31) / 32;
-    const uint32_t slice = k >> 5;
-    if (slice >= nslices) {
-        if ((k & 31) == 0) width32[slice] = 0u;
-        return;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;  // slice
+    if (s > maxslices) return;
+    uint32_t m = 0;
+    const uint32_t k0 = s * SELL_C;
+    for (uint32_t r = 0; r < SELL_C; r++) {
+        const uint32_t k = k0 + r;
+        if (k < R) m = max(m, rlen[rowlist[k]]);
     }
-    const uint32_t len = k < R ? rlen[rowlist[k]] : 0u;
-    const uint32_t m = __reduce_max_sync(0xffffffffu, len);
-    if ((k & 31) == 0) width32[slice] = 32u * m;
+    width[s] = SELL_C * ((m + 3u) & ~3u);
 }
 
 __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm, const float* __restrict__ vals_rm,
@@ -461,11 +478,11 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
                                                    const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
                                                    uint32_t* __restrict__ scols, float* __restrict__ svals) {
     const uint32_t R = *nrows;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t slice = k >> 5, lane = k & 31;
-    if (slice >= (R + 31) / 32) return;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
+    const uint32_t slice = k / SELL_C, r = k % SELL_C;
+    if (slice >= (R + SELL_C - 1) / SELL_C) return;
     const uint32_t base = off[slice];
-    const uint32_t W = (off[slice + 1] - base) >> 5;
+    const uint32_t W = (off[slice + 1] - base) / SELL_C;
     const bool has = k < R;
     const uint32_t i = has ? rowlist[k] : 0u;
     const uint32_t len = has ? rlen[i] : 0u;
@@ -473,8 +490,8 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
     const float* rv = vals_rm + (size_t)i * PPE_W;
     for (uint32_t e = 0; e < W; e++) {
         const bool real = e < len;
-        scols[base + 32u * e + lane] = real ? rc[e] : i;
-        svals[base + 32u * e + lane] = real ? rv[e] : 0.f;
+        scols[base + SELL_C * e + r] = real ? rc[e] : i;
+        svals[base + SELL_C * e + r] = real ? rv[e] : 0.f;
     }
 }
 
@@ -601,9 +618,9 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.p[0], (size_t)cap * sizeof(float));
     ok &= al((void**)&w.p[1], (size_t)cap * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
-    ok &= al((void**)&w.sell_off, ((size_t)cap / 32 + 4) * sizeof(uint32_t));
-    ok &= al((void**)&w.sell_cols, ((size_t)cap + 32) * PPE_W * sizeof(uint32_t));
-    ok &= al((void**)&w.sell_vals, ((size_t)cap + 32) * PPE_W * sizeof(float));
+    ok &= al((void**)&w.sell_off, ((size_t)cap / SELL_C + 4) * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_cols, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_vals, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(float));
     ok &= al((void**)&w.tilecnt, ((size_t)cap / 2048 + 2) * sizeof(uint32_t));
     ok &= al((void**)&w.nrows, sizeof(uint32_t));
     if (!ok) {
@@ -619,7 +636,7 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
         *err = "device cannot run the cooperative PPE solver";
         return MPS_ERR_CUDA;
     }
-    if (per_sm > 2) per_sm = 2;
+    if (per_sm > 1) per_sm = 1;
     w.blocks = sms * per_sm;
     ok &= al((void**)&w.part, (size_t)w.blocks * PPE_PARTS * sizeof(double));
     ok &= al((void**)&w.result, PPE_PARTS * sizeof(double));
@@ -688,12 +705,12 @@ int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t
     k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
     launch_scan_exclusive(w.tilecnt, ntiles, st);
     k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
-    // SELL-32 layout of the non-Dirichlet rows
-    const uint32_t maxslices = (cap + 31) / 32;
-    k_sell_width<<<blocks_for((maxslices + 1) * 32u, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off);
+    // SELL-8 layout of the non-Dirichlet rows
+    const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
+    k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
     launch_scan_exclusive(w.sell_off, maxslices + 1, st);
-    k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.vals, w.rlen, w.rowlist, w.nrows,
-                                                                  w.sell_off, w.sell_cols, w.sell_vals);
+    k_sell_pack<<<blocks_for(maxslices * SELL_C, 256), 256, 0, st>>>(w.cols, w.vals, w.rlen, w.rowlist, w.nrows,
+                                                                     w.sell_off, w.sell_cols, w.sell_vals);
     void* args[] = {&S};
     w.launch_err = cudaLaunchCooperativeKernel((const void*)k_ppe_solve, w.blocks, PPE_THREADS, args, 0, st);
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);

@@ -22,8 +22,9 @@ namespace mpsb {
 
 constexpr uint32_t PPE_W = 352;        // stride: > the 256 lattice neighbours within 4 l0
 constexpr uint32_t PPE_DIRICHLET = 0xffffffffu;
-constexpr int PPE_THREADS = 512;
+constexpr int PPE_THREADS = 1024;
 constexpr int PPE_PARTS = 4;           // FP64 partial sums per block
+constexpr uint32_t SELL_C = 8;         // rows per sliced-ELL slice
 
 struct PpeWork {
     bool ready = false;
