@@ -216,6 +216,26 @@ mps_status mps_cell_sort_dev(const float* pos4_dev, uint32_t n, const mps_grid* 
                              uint32_t* perm_dev, uint32_t* cell_of_dev, uint32_t* start_dev,
                              uint32_t* end_dev, uint32_t* n_in_grid_dev, void* stream);
 
+/* ---- allocation-free variant of mps_cell_sort_dev -------------------------
+ * No counterpart in the reference (the reference allocates and frees device
+ * memory around every kernel call).  Same arguments, results and errors as
+ * mps_cell_sort_dev, but it calls no cudaMalloc/cudaFree: its scratch is one
+ * fixed device array of 10.25 MiB inside the library.  For callers that may
+ * not allocate device memory themselves or through a library: hosts whose
+ * pool allocator owns all device memory, and latency-critical loops where
+ * the device-wide synchronisation of cudaMalloc/cudaFree is not acceptable.
+ * Limits: n <= MPS_NOALLOC_MAX_PARTICLES and ncells <= MPS_NOALLOC_MAX_CELLS,
+ * else MPS_ERR_CAPACITY.  All calls on a device share the array, so calls
+ * whose GPU work overlaps race and must be serialised.  The first call on a
+ * device (with it current) looks the array's address up; make it before any
+ * stream capture.  The array stays allocated on every device that loaded the
+ * library until the process exits. */
+#define MPS_NOALLOC_MAX_PARTICLES 524288u
+#define MPS_NOALLOC_MAX_CELLS 524288u
+mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t n, const mps_grid* g,
+                                     uint32_t* perm_dev, uint32_t* cell_of_dev, uint32_t* start_dev,
+                                     uint32_t* end_dev, uint32_t* n_in_grid_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,9 @@ PRECOND_DIAGONAL, PRECOND_LEARNED = 0, 1
 ORDER_SORTED, ORDER_BY_ID = 0, 1
 PHASE = dict(update_dt=0, visc=1, divide_cell=2, collision=3, cal_n=4, pres_expl=5, dash=6, ppe=7)
 
+NOALLOC_MAX_PARTICLES = 524288
+NOALLOC_MAX_CELLS = 524288
+
 STATUS = {0: "MPS_OK", 1: "MPS_ERR_IO", 2: "MPS_ERR_CELLS_TOO_THIN", 3: "MPS_ERR_DT_TOO_SMALL",
           4: "MPS_ERR_PARTICLE_OUT", 5: "MPS_ERR_CG_NOT_CONVERGED", 6: "MPS_ERR_DEVICE_TIMEOUT",
           7: "MPS_ERR_CUDA", 8: "MPS_ERR_NAN", 9: "MPS_ERR_INVALID", 10: "MPS_ERR_CAPACITY"}
@@ -33,7 +36,7 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_destroy", "mps_step", "mps_step_async", "mps_run", "mps_get_counts", "mps_get_state", "mps_set_state",
            "mps_get_cell_tables", "mps_get_grid", "mps_get_scalars", "mps_get_normal_ids",
            "mps_phase", "mps_get_stream", "mps_write_case", "mps_last_error", "mps_cell_sort_dev",
-           "mps_profile_steps", "mps_stage_name")
+           "mps_profile_steps", "mps_stage_name", "mps_cell_sort_dev_noalloc")
 
 
 class mps_options(C.Structure):
@@ -109,6 +112,9 @@ def lib():
             "mps_cell_sort_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(mps_grid), C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p]),
+            "mps_cell_sort_dev_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(mps_grid),
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
