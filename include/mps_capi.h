@@ -110,7 +110,8 @@ typedef struct {
     double cg_relres;    /* final FP64 |b - Ax| / |b| of the last step          */
     int status;          /* sticky device error word mapped to mps_status      */
     float ms;            /* device time of the call (CUDA events on the stream) */
-    uint32_t reserved[4];
+    uint32_t cg_outer;   /* FP64 true-residual passes of the last PPE solve    */
+    uint32_t reserved[3];
 } mps_step_stats;
 
 typedef struct mps_handle mps_handle;
@@ -173,7 +174,7 @@ mps_status mps_get_cell_tables(mps_handle* h, uint32_t* cell_of, uint32_t* start
 mps_status mps_get_grid(mps_handle* h, mps_grid* g);
 /* n0, lambda, dt, time, c_lap = 2d/(n0 lambda), rho c^2, alpha, cg iterations,
  * cg relative residual, step, status, number of cells, kernels launched by
- * one step, and 3 spare slots. */
+ * one step, FP64 residual passes of the last PPE solve, and 2 spare slots. */
 mps_status mps_get_scalars(mps_handle* h, double out16[16]);
 /* i_normal as GEO.dat indices: for each particle (by GEO index) the GEO index
  * of its wall particle (itself when it has none), np0 entries. */
@@ -190,8 +191,9 @@ mps_status mps_phase(mps_handle* h, int phase);
  * with CUDA events between stages; stage_ms[k] (k < max_stages) receives the
  * summed milliseconds of stage k, *nstages the number of stages, and
  * mps_stage_name(k) its name (update_dt, visc, collision, pnd, pressure,
- * dash, step_end, cell_keys, radix_sort, cell_table, gather).  The steps
- * advance the simulation like mps_step. */
+ * dash, step_end, cell_keys, radix_sort, cell_table, gather, ppe_solve;
+ * pressure is the dummy copy of the explicit method or the PPE assembly of
+ * the semi-implicit one).  The steps advance the simulation like mps_step. */
 mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int max_stages, int* nstages);
 const char* mps_stage_name(int k);
 

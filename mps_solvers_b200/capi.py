@@ -55,7 +55,8 @@ class mps_params(C.Structure):
 class mps_step_stats(C.Structure):
     _fields_ = [("np", C.c_uint32), ("nexcl", C.c_uint32), ("step", C.c_int), ("time", C.c_float),
                 ("dt", C.c_float), ("cg_iters", C.c_int), ("cg_relres", C.c_double),
-                ("status", C.c_int), ("ms", C.c_float), ("reserved", C.c_uint32 * 4)]
+                ("status", C.c_int), ("ms", C.c_float), ("cg_outer", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
 
 
 class mps_grid(C.Structure):
@@ -264,7 +265,7 @@ class Simulation:
         o = (C.c_double * 16)()
         self._check(lib().mps_get_scalars(self.h, o))
         names = ("nzero", "lambda", "dt", "time", "c_lap", "one_over_alpha", "alpha", "cg_iters",
-                 "cg_relres", "step", "status", "ncells", "launches_per_step")
+                 "cg_relres", "step", "status", "ncells", "launches_per_step", "cg_outer")
         return dict(zip(names, list(o)))
 
     def normal_ids(self) -> np.ndarray:

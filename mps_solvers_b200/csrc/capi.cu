@@ -123,9 +123,10 @@ static StageArgs stage_args(mps_handle* h) {
 
 // Stage tags of mps_profile_steps (names in kStageNames).
 enum { ST_UPDATE_DT = 0, ST_VISC, ST_COLLISION, ST_PND, ST_PRESSURE, ST_DASH, ST_STEP_END, ST_KEYS, ST_SORT,
-       ST_CELLS, ST_GATHER, ST_COUNT };
-static const char* kStageNames[ST_COUNT] = {"update_dt", "visc", "collision", "pnd", "pressure", "dash",
-                                            "step_end", "cell_keys", "radix_sort", "cell_table", "gather"};
+       ST_CELLS, ST_GATHER, ST_PPE_SOLVE, ST_COUNT };
+static const char* kStageNames[ST_COUNT] = {"update_dt", "visc",       "collision",  "pnd",
+                                            "pressure",  "dash",       "step_end",   "cell_keys",
+                                            "radix_sort", "cell_table", "gather",     "ppe_solve"};
 
 static void mark(mps_handle* h, int tag) {
     if (!h->prof_on) return;
@@ -183,7 +184,9 @@ static void enqueue_step(mps_handle* h) {
     } else {
         launch_pnd(stage_args(h), 0, 0, cap, st);
         mark(h, ST_PRESSURE);
-        h->launches += 1 + ppe_enqueue(h->ppe, stage_args(h), h->opt, cap, st);
+        h->launches += 1 + ppe_enqueue_setup(h->ppe, stage_args(h), h->opt, cap, st);
+        mark(h, ST_PPE_SOLVE);
+        h->launches += ppe_enqueue_solve(h->ppe, stage_args(h), h->opt, cap, st);
         if (h->ppe.launch_err != cudaSuccess) h->launch_err = h->ppe.launch_err;
     }
     mark(h, ST_DASH);
@@ -543,6 +546,7 @@ extern "C" mps_status mps_step(mps_handle* h, int nsteps, mps_step_stats* stats)
         stats->dt = sc.dt;
         stats->cg_iters = sc.cg_iters;
         stats->cg_relres = sc.cg_relres;
+        stats->cg_outer = (uint32_t)sc.cg_outer;
         stats->status = (int)s;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
@@ -578,7 +582,8 @@ extern "C" mps_status mps_phase(mps_handle* h, int phase) {
         case 6: launch_dash(stage_args(h), cap, st); h->pending_apply = APPLY_ADD_VEL; break;
         case 7:
             if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) return MPS_ERR_INVALID;
-            ppe_enqueue(h->ppe, stage_args(h), h->opt, cap, st);
+            ppe_enqueue_setup(h->ppe, stage_args(h), h->opt, cap, st);
+            ppe_enqueue_solve(h->ppe, stage_args(h), h->opt, cap, st);
             break;
         default: return MPS_ERR_INVALID;
     }
@@ -693,6 +698,7 @@ extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
     o[10] = (double)st;
     o[11] = h->g.ncells;
     o[12] = h->launches;
+    o[13] = s.cg_outer;
     return MPS_OK;
 }
 

@@ -40,7 +40,9 @@ struct Scalars {
     double cg_relres;
     uint32_t n_fluid;      // entries of the fluid list built by the last rebuild
     uint32_t n_solid;      // entries of the fluid + wall list
-    double pad[3];
+    int cg_outer;          // FP64 true-residual passes of the last PPE solve
+    int pad_i;
+    double pad[2];
 };
 
 enum : uint32_t {

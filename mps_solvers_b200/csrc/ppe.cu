@@ -133,7 +133,6 @@ __device__ bool grid_reduce(const double (&v)[K], double* part, double* result, 
 struct AsmArgs {
     StageArgs a;
     uint32_t* cols;
-    float* vals;
     uint32_t* rlen;
     double* diag64;
     float* diag32;
@@ -176,7 +175,6 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const float re = a.P.rlap, thr = a.P.rlap_thr;
     const double bthr = A.beta * A.n0;
     uint32_t* cols = A.cols + (size_t)i * PPE_W;
-    float* vals = A.vals + (size_t)i * PPE_W;
     uint32_t count = 0;
     double diag = 0.0;
     const uint32_t c = a.cur.cell[i];
@@ -203,10 +201,7 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
             const uint32_t m = __ballot_sync(0xffffffffu, app);
             if (app) {
                 const uint32_t k = count + __popc(m & lt);
-                if (k < PPE_W) {
-                    cols[k] = j;
-                    vals[k] = w;
-                }
+                if (k < PPE_W) cols[k] = j;
             }
             count += __popc(m);
         }
@@ -230,7 +225,6 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
 // ---------------------------------------------------------------- solve
 struct SolveArgs {
     const uint32_t* cols;
-    const float* vals;
     const uint32_t* rlen;
     const double* diag64;
     const float* diag32;
@@ -249,7 +243,8 @@ struct SolveArgs {
     const uint32_t* nrows;
     const uint32_t* off;
     const uint32_t* scols;
-    const float* svals;
+    const float4* pos;
+    float rlap, rlap_thr;
     Scalars* sc;
     double tol;
     int max_iter;
@@ -257,6 +252,18 @@ struct SolveArgs {
     int max_outer;
 };
 
+// The weight of a stored neighbour, recomputed from the positions with the
+// function the assembly used for the diagonal (so the operator is the same
+// matrix in every product); a padding entry (j == i) weighs 0.
+template <bool EX>
+__device__ __forceinline__ float stencil_weight(const SolveArgs& S, const float4& pi, uint32_t i, uint32_t j) {
+    const float4 pj = __ldg(S.pos + j);
+    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+    return (j != i && rr < S.rlap_thr) ? weight_rr<EX>(S.rlap, rr) : 0.f;
+}
+
+template <bool EX>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them
     // are dealt to warps round-robin (4 lanes per row inside a slice); the
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t* __restrict__ rowlist = S.rowlist;
-    int total = 0;
+    int total = 0, outers = 0;
     double relres = 0.0;
     bool converged = false;
     float* pcur = S.p0;
@@ -281,9 +288,13 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             const uint32_t base = __ldg(S.off + sl);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
             const uint32_t* cols = S.scols + base + lane;
-            const float* vals = S.svals + base + lane;
+            const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
+            const float4 pi = __ldg(S.pos + ii);
             double s = 0.0;
-            for (uint32_t t = 0; t < T; t++) s += (double)__ldg(vals + 32 * t) * S.x64[__ldg(cols + 32 * t)];
+            for (uint32_t t = 0; t < T; t++) {
+                const uint32_t j = __ldg(cols + 32 * t);
+                s += (double)stencil_weight<EX>(S, pi, ii, j) * S.x64[j];
+            }
             s += __shfl_xor_sync(0xffffffffu, s, 8);
             s += __shfl_xor_sync(0xffffffffu, s, 16);
             if (q == 0 && k < R) {
@@ -302,6 +313,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         }
         double tot[3];
         if (!grid_reduce<3>(acc, S.part, S.result, S.bar, S.sc, tot)) return;
+        outers++;
         const double rr64 = tot[0], bb = tot[1];
         relres = bb > 0.0 ? sqrt(rr64 / bb) : 0.0;
         if (relres <= S.tol) {
@@ -324,26 +336,26 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const uint32_t base = __ldg(S.off + sl);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
                 const uint32_t* cols = S.scols + base + lane;
-                const float* vals = S.svals + base + lane;
+                const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
+                const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
                 uint32_t t = 0;
-                for (; t + 8 <= T; t += 8) {
-                    uint32_t j[8];
-                    float w[8];
+                for (; t + 4 <= T; t += 4) {
+                    uint32_t j[4];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        j[u] = __ldg(cols + 32 * (t + u));
-                        w[u] = __ldg(vals + 32 * (t + u));
-                    }
+                    for (int u = 0; u < 4; u++) j[u] = __ldg(cols + 32 * (t + u));
+                    float w[4];
 #pragma unroll
-                    for (int u = 0; u < 8; u += 2) {
+                    for (int u = 0; u < 4; u++) w[u] = stencil_weight<EX>(S, pi, ii, j[u]);
+#pragma unroll
+                    for (int u = 0; u < 4; u += 2) {
                         s0 = fmaf(w[u], fmaf(beta, pcur[j[u]], S.z[j[u]]), s0);
                         s1 = fmaf(w[u + 1], fmaf(beta, pcur[j[u + 1]], S.z[j[u + 1]]), s1);
                     }
                 }
                 for (; t < T; t++) {
                     const uint32_t jj = __ldg(cols + 32 * t);
-                    s0 = fmaf(__ldg(vals + 32 * t), fmaf(beta, pcur[jj], S.z[jj]), s0);
+                    s0 = fmaf(stencil_weight<EX>(S, pi, ii, jj), fmaf(beta, pcur[jj], S.z[jj]), s0);
                 }
                 float s = s0 + s1;
                 s += __shfl_xor_sync(0xffffffffu, s, 8);
@@ -389,6 +401,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S.sc->cg_iters = total;
+        S.sc->cg_outer = outers;
         S.sc->cg_relres = relres;
         if (!converged) atomicOr(&S.sc->err, ERR_CG_NOT_CONVERGED);
     }
@@ -473,10 +486,10 @@ __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__
     width[s] = SELL_C * ((m + 3u) & ~3u);
 }
 
-__global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm, const float* __restrict__ vals_rm,
+__global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm,
                                                    const uint32_t* __restrict__ rlen, const uint32_t* __restrict__ rowlist,
                                                    const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
-                                                   uint32_t* __restrict__ scols, float* __restrict__ svals) {
+                                                   uint32_t* __restrict__ scols) {
     const uint32_t R = *nrows;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
     const uint32_t slice = k / SELL_C, r = k % SELL_C;
@@ -487,11 +500,9 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
     const uint32_t i = has ? rowlist[k] : 0u;
     const uint32_t len = has ? rlen[i] : 0u;
     const uint32_t* rc = cols_rm + (size_t)i * PPE_W;
-    const float* rv = vals_rm + (size_t)i * PPE_W;
     for (uint32_t e = 0; e < W; e++) {
         const bool real = e < len;
         scols[base + SELL_C * e + r] = real ? rc[e] : i;
-        svals[base + SELL_C * e + r] = real ? rv[e] : 0.f;
     }
 }
 
@@ -605,7 +616,6 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     };
     bool ok = true;
     ok &= al((void**)&w.cols, (size_t)cap * PPE_W * sizeof(uint32_t));
-    ok &= al((void**)&w.vals, (size_t)cap * PPE_W * sizeof(float));
     ok &= al((void**)&w.rlen, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.diag64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.diag32, (size_t)cap * sizeof(float));
@@ -620,7 +630,6 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.sell_off, ((size_t)cap / SELL_C + 4) * sizeof(uint32_t));
     ok &= al((void**)&w.sell_cols, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(uint32_t));
-    ok &= al((void**)&w.sell_vals, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(float));
     ok &= al((void**)&w.tilecnt, ((size_t)cap / 2048 + 2) * sizeof(uint32_t));
     ok &= al((void**)&w.nrows, sizeof(uint32_t));
     if (!ok) {
@@ -631,7 +640,10 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppe_solve, PPE_THREADS, 0);
+    int per_sm2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppe_solve<true>, PPE_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_ppe_solve<false>, PPE_THREADS, 0);
+    per_sm = per_sm < per_sm2 ? per_sm : per_sm2;
     if (!coop || per_sm < 1) {
         *err = "device cannot run the cooperative PPE solver";
         return MPS_ERR_CUDA;
@@ -649,11 +661,11 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     return MPS_OK;
 }
 
-int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
+int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
+    (void)opt;
     AsmArgs A;
     A.a = a;
     A.cols = w.cols;
-    A.vals = w.vals;
     A.rlen = w.rlen;
     A.diag64 = w.diag64;
     A.diag32 = w.diag32;
@@ -673,10 +685,22 @@ int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t
     const uint32_t warps_blocks = blocks_for(cap * 32u, 256);
     if (a.exact) k_ppe_assemble<true><<<warps_blocks, 256, 0, st>>>(A);
     else k_ppe_assemble<false><<<warps_blocks, 256, 0, st>>>(A);
+    const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
+    k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
+    launch_scan_exclusive(w.tilecnt, ntiles, st);
+    k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
+    // SELL-8 layout of the non-Dirichlet rows
+    const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
+    k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
+    launch_scan_exclusive(w.sell_off, maxslices + 1, st);
+    k_sell_pack<<<blocks_for(maxslices * SELL_C, 256), 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows,
+                                                                     w.sell_off, w.sell_cols);
+    return 7;
+}
 
+int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
     SolveArgs S;
     S.cols = w.cols;
-    S.vals = w.vals;
     S.rlen = w.rlen;
     S.diag64 = w.diag64;
     S.diag32 = w.diag32;
@@ -695,32 +719,25 @@ int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t
     S.nrows = w.nrows;
     S.off = w.sell_off;
     S.scols = w.sell_cols;
-    S.svals = w.sell_vals;
+    S.pos = a.cur.pos;
+    S.rlap = a.P.rlap;
+    S.rlap_thr = a.P.rlap_thr;
     S.sc = a.sc;
     S.tol = opt.cg_tol;
     S.max_iter = opt.cg_max_iter;
     S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
     S.max_outer = 40;
-    const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
-    k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
-    launch_scan_exclusive(w.tilecnt, ntiles, st);
-    k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
-    // SELL-8 layout of the non-Dirichlet rows
-    const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
-    k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
-    launch_scan_exclusive(w.sell_off, maxslices + 1, st);
-    k_sell_pack<<<blocks_for(maxslices * SELL_C, 256), 256, 0, st>>>(w.cols, w.vals, w.rlen, w.rowlist, w.nrows,
-                                                                     w.sell_off, w.sell_cols, w.sell_vals);
     void* args[] = {&S};
-    w.launch_err = cudaLaunchCooperativeKernel((const void*)k_ppe_solve, w.blocks, PPE_THREADS, args, 0, st);
+    w.launch_err = cudaLaunchCooperativeKernel(a.exact ? (const void*)k_ppe_solve<true> : (const void*)k_ppe_solve<false>,
+                                               w.blocks, PPE_THREADS, args, 0, st);
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
-    return 9;
+    return 2;
 }
 
 void ppe_free(PpeWork& w) {
-    void* ps[] = {w.cols, w.vals, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
+    void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar, w.gvals,
-                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_vals};
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols};
     for (void* p : ps)
         if (p) cudaFree(p);
     w = PpeWork();

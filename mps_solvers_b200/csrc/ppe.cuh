@@ -8,8 +8,10 @@
 // Dirichlet rows (n_i < beta n0 or type 2) are identity rows with b = 0, so
 // their solution is 0 and they are left out of the solve.  Then p = max(x, 0).
 //
-// Storage: row-major with a fixed stride of PPE_W entries per particle
-// (column index + float weight), the diagonal in double.
+// Storage: the neighbour stencil of each row (column indices, in sliced-ELL
+// order) and the diagonal in double; the off-diagonal weights are recomputed
+// from the float positions in every matrix product with the same function
+// the assembly used (matrix-free in the weights).
 #pragma once
 #include <cstdint>
 #include <string>
@@ -31,7 +33,6 @@ struct PpeWork {
     uint32_t cap = 0;
     int blocks = 0;                    // co-resident blocks of the persistent solver
     uint32_t* cols = nullptr;          // cap * PPE_W
-    float* vals = nullptr;             // cap * PPE_W
     uint32_t* rlen = nullptr;          // off-diagonal count, PPE_DIRICHLET for Dirichlet rows
     double* diag64 = nullptr;
     float* diag32 = nullptr;
@@ -46,7 +47,6 @@ struct PpeWork {
     uint32_t* nrows = nullptr;
     uint32_t* sell_off = nullptr;      // slice offsets (exclusive scan of 32 * width)
     uint32_t* sell_cols = nullptr;
-    float* sell_vals = nullptr;
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
     // preconditioner (learned factor G); unused for the diagonal one
     float* gvals = nullptr;
@@ -56,8 +56,10 @@ struct PpeWork {
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
               std::string* err);
-// returns the number of kernels enqueued
-int ppe_enqueue(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
+// assembly, row list and sliced-ELL layout; returns the kernels enqueued
+int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
+// the persistent solve and p = max(x, 0); returns the kernels enqueued
+int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);
 
 // FP64 particle number density of every particle (initialisation of the
