@@ -210,7 +210,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tmpd = tempfile.mkdtemp(prefix=f"mpsb_{rank}_")
     pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
     n = len(pos0)
-    sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1)
+    precond = capi.PRECOND_LEARNED if args.precond == "learned" else capi.PRECOND_DIAGONAL
+    sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
+                          precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+    if method == capi.METHOD_SEMI_IMPLICIT and precond == capi.PRECOND_LEARNED:
+        from mps_solvers_b200 import precond_weights
+        sim.set_precond_params(precond_weights.load())
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
@@ -261,6 +266,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     launches = int(scal["launches_per_step"])
     prof_iters, prof_outer = int(scal["cg_iters"]), int(scal["cg_outer"])
     sim.close()
+    compare = None
+    if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare:
+        compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)))
 
     # max over ranks
     tot = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
@@ -294,6 +302,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "data": "synthetic",
         "config": {"workload": workload_name(args.workload) if args.size == "full" else
                    f"{args.workload} small profiling tank", "particles": n,
+                   "precond": args.precond if method == capi.METHOD_SEMI_IMPLICIT else None,
                    "fluid": int(n - nb2 - nb1), "arith": args.arith,
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -308,11 +317,40 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
+        "ppe_compare": compare,
         "final": {"np": stats.np, "step": stats.step, "time": stats.time, "dt": stats.dt,
                   "cg_iters": stats.cg_iters, "cg_outer": stats.cg_outer,
                   "cg_relres": stats.cg_relres},
     }
     return line
+
+
+def ppe_compare(case_dir: str, arith: int, device: int, warm: int, steps: int):
+    """PPE solve milliseconds and PCG iterations per step (FP64 true residual
+    to 1e-8) with diagonal scaling and with the trained learned factor, each
+    on a fresh copy of the scene after `warm` steps."""
+    from mps_solvers_b200 import capi, precond_weights
+    out = {"tolerance": 1e-8, "steps": steps, "warmup": warm,
+           "weights": os.path.relpath(precond_weights.PATH, ROOT)}
+    for name, pc in (("diagonal", capi.PRECOND_DIAGONAL), ("learned", capi.PRECOND_LEARNED)):
+        with capi.Simulation(case_dir, method=capi.METHOD_SEMI_IMPLICIT, arith=arith, device=device,
+                             precond=pc) as s:
+            if pc == capi.PRECOND_LEARNED:
+                s.set_precond_params(precond_weights.load())
+            s.step(warm)
+            iters, worst = 0, 0.0
+            for _ in range(steps):
+                st = s.step(1)
+                iters += st.cg_iters
+                worst = max(worst, st.cg_relres)
+            prof = s.profile(steps)
+            out[name] = {"ppe_solve_ms": prof["ppe_solve"] / steps,
+                         "ppe_total_ms": (prof["ppe_solve"] + prof.get("pressure", 0.0)) / steps,
+                         "cg_iters": iters / steps, "max_relres": worst,
+                         "step_ms": sum(prof.values()) / steps}
+    out["iters_ratio"] = out["learned"]["cg_iters"] / out["diagonal"]["cg_iters"]
+    out["ppe_solve_ratio"] = out["learned"]["ppe_solve_ms"] / out["diagonal"]["ppe_solve_ms"]
+    return out
 
 
 def _traffic_from_profiles(kernel: str, workload: str):
@@ -348,6 +386,10 @@ def main():
                     help="small: a ~110k-particle tank of the same kernels (profiling)")
     ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precond", default="diagonal", choices=["diagonal", "learned"],
+                    help="PPE preconditioner of the semi-implicit timed run")
+    ap.add_argument("--no-ppe-compare", action="store_true",
+                    help="skip the diagonal-vs-learned PPE comparison (semi-implicit)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -197,6 +197,35 @@ mps_status mps_phase(mps_handle* h, int phase);
 mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int max_stages, int* nstages);
 const char* mps_stage_name(int k);
 
+/* ---- learned PPE preconditioner (no counterpart in the reference) --------
+ * M^-1 = D^-1/2 G^T G D^-1/2 with G lower triangular on each row's r0
+ * neighbours, its entries produced by a two-round message-passing network
+ * (hidden 64, GELU, BF16 weights, FP32 accumulation); selected with
+ * options.precond = MPS_PRECOND_LEARNED (semi-implicit method).  The
+ * parameter vector has mps_precond_num_params() floats. */
+uint32_t mps_precond_num_params(void);
+mps_status mps_precond_get_params(mps_handle* h, float* w, uint32_t n);
+/* Load parameters (also enables the network on a handle created with the
+ * diagonal preconditioner, for training). */
+mps_status mps_precond_set_params(mps_handle* h, const float* w, uint32_t n);
+/* On the PPE system of the last step: the training loss
+ * L = log(z^T M z / n) - (2/n) sum_i log G_ii, M = G Ahat G^T,
+ * Ahat = D^-1/2 (-A) D^-1/2, n the number of unknowns and z a Rademacher
+ * vector drawn from seed and the particle ids -- the logarithm of Kaporin's
+ * condition number of M up to a constant of the system, with Hutchinson's
+ * estimate of the trace -- and its gradient with respect to the FP32
+ * parameters (n floats). */
+mps_status mps_precond_loss_grad(mps_handle* h, uint64_t seed, double* loss, float* grad);
+/* iters Adam steps (learning rate lr, probe seeds seed, seed+1, ...) on the
+ * PPE system of the last step; loss of the first and last step. */
+mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint64_t seed, double* loss_first,
+                             double* loss_last);
+/* The state the last PPE system was assembled from (np entries each):
+ * x y z type-bits per particle, n, GEO index, 1 for a solved (non-Dirichlet)
+ * row, the diagonal of A. */
+mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
+                            double* diag, uint32_t* count);
+
 /* The handle's cudaStream_t, for callers that time or order work around it. */
 mps_status mps_get_stream(mps_handle* h, void** stream);
 /* Write the reference's text output for the current state:

@@ -36,7 +36,9 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_destroy", "mps_step", "mps_step_async", "mps_run", "mps_get_counts", "mps_get_state", "mps_set_state",
            "mps_get_cell_tables", "mps_get_grid", "mps_get_scalars", "mps_get_normal_ids",
            "mps_phase", "mps_get_stream", "mps_write_case", "mps_last_error", "mps_cell_sort_dev",
-           "mps_profile_steps", "mps_stage_name", "mps_cell_sort_dev_noalloc")
+           "mps_profile_steps", "mps_stage_name", "mps_cell_sort_dev_noalloc",
+           "mps_precond_num_params", "mps_precond_get_params", "mps_precond_set_params",
+           "mps_precond_loss_grad", "mps_precond_train", "mps_ppe_snapshot")
 
 
 class mps_options(C.Structure):
@@ -110,6 +112,13 @@ def lib():
             "mps_profile_steps": (C.c_int, [H, C.c_int, C.POINTER(C.c_double), C.c_int,
                                             C.POINTER(C.c_int)]),
             "mps_stage_name": (C.c_char_p, [C.c_int]),
+            "mps_precond_num_params": (C.c_uint32, []),
+            "mps_precond_get_params": (C.c_int, [H, Fp, C.c_uint32]),
+            "mps_precond_set_params": (C.c_int, [H, Fp, C.c_uint32]),
+            "mps_precond_loss_grad": (C.c_int, [H, C.c_uint64, C.POINTER(C.c_double), Fp]),
+            "mps_precond_train": (C.c_int, [H, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]),
+            "mps_ppe_snapshot": (C.c_int, [H, Fp, Fp, U, U, C.POINTER(C.c_double), U]),
             "mps_cell_sort_dev": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(mps_grid), C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p]),
@@ -279,6 +288,41 @@ class Simulation:
         ns = C.c_int()
         self._check(lib().mps_profile_steps(self.h, nsteps, buf, 32, C.byref(ns)))
         return {lib().mps_stage_name(k).decode(): buf[k] for k in range(ns.value)}
+
+    # ---- learned PPE preconditioner
+    def precond_params(self) -> np.ndarray:
+        n = lib().mps_precond_num_params()
+        w = np.empty(n, np.float32)
+        self._check(lib().mps_precond_get_params(self.h, _p(w), n))
+        return w
+
+    def set_precond_params(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(lib().mps_precond_set_params(self.h, _p(w), len(w)))
+
+    def precond_loss_grad(self, seed: int):
+        n = lib().mps_precond_num_params()
+        g = np.empty(n, np.float32)
+        loss = C.c_double()
+        self._check(lib().mps_precond_loss_grad(self.h, seed, C.byref(loss), _p(g)))
+        return loss.value, g
+
+    def precond_train(self, iters: int, lr: float, seed: int):
+        a, b = C.c_double(), C.c_double()
+        self._check(lib().mps_precond_train(self.h, iters, lr, seed, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def ppe_snapshot(self) -> Dict[str, np.ndarray]:
+        n = self.counts()["np"]
+        out = dict(pos4=np.empty((n, 4), np.float32), n=np.empty(n, np.float32),
+                   id=np.empty(n, np.uint32), is_row=np.empty(n, np.uint32),
+                   diag=np.empty(n, np.float64))
+        cnt = C.c_uint32()
+        self._check(lib().mps_ppe_snapshot(self.h, _p(out["pos4"]), _p(out["n"]),
+                                           _p(out["id"], C.c_uint32), _p(out["is_row"], C.c_uint32),
+                                           out["diag"].ctypes.data_as(C.POINTER(C.c_double)),
+                                           C.byref(cnt)))
+        return out
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -412,6 +412,10 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
         int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
+        if (h->opt.precond == MPS_PRECOND_LEARNED) {
+            e = ppe_enable_learned(h->ppe, &h->err);
+            if (e != MPS_OK) return (mps_status)e;
+        }
     }
     Scalars s;
     return read_status(h, &s);
@@ -699,6 +703,132 @@ extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
     o[11] = h->g.ncells;
     o[12] = h->launches;
     o[13] = s.cg_outer;
+    return MPS_OK;
+}
+
+// ---------------------------------------------------------------- learned preconditioner
+extern "C" uint32_t mps_precond_num_params(void) { return (uint32_t)LP_NPARAM; }
+
+static mps_status need_semi(mps_handle* h) {
+    if (!h) return MPS_ERR_INVALID;
+    if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) {
+        h->err = "the learned preconditioner belongs to the semi-implicit method";
+        return MPS_ERR_INVALID;
+    }
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_precond_get_params(mps_handle* h, float* w, uint32_t n) {
+    mps_status s = need_semi(h);
+    if (s != MPS_OK) return s;
+    if (!w || n != (uint32_t)LP_NPARAM) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    if (!h->ppe.lp.ready) {
+        lp_init_params(w, 1234);
+        return MPS_OK;
+    }
+    CK(cudaMemcpyAsync(w, h->ppe.lp.w32, n * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_precond_set_params(mps_handle* h, const float* w, uint32_t n) {
+    mps_status s = need_semi(h);
+    if (s != MPS_OK) return s;
+    if (!w || n != (uint32_t)LP_NPARAM) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    int e = ppe_enable_learned(h->ppe, &h->err);
+    if (e != MPS_OK) return (mps_status)e;
+    lp_upload_params(h->ppe.lp, w, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    return MPS_OK;
+}
+
+static mps_status need_snapshot(mps_handle* h) {
+    mps_status s = need_semi(h);
+    if (s != MPS_OK) return s;
+    if (!h->ppe.lp.ready || !h->ppe.have_snapshot) {
+        h->err = "no PPE system with the learned stencil yet: enable the learned preconditioner "
+                 "(option or mps_precond_set_params) and take a step first";
+        return MPS_ERR_INVALID;
+    }
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_precond_loss_grad(mps_handle* h, uint64_t seed, double* loss, float* grad) {
+    mps_status s = need_snapshot(h);
+    if (s != MPS_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    const LpSystem L = ppe_lp_system(h->ppe, stage_args(h));
+    if (lp_loss_grad(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, seed, h->cap, h->stream) != 0)
+        return MPS_ERR_CUDA;
+    double lz[2] = {0, 0};
+    uint32_t nrows = 0;
+    CK(cudaMemcpyAsync(lz, h->ppe.lp.loss, 16, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&nrows, h->ppe.nrows, 4, cudaMemcpyDeviceToHost, h->stream));
+    if (grad) CK(cudaMemcpyAsync(grad, h->ppe.lp.grad, LP_NPARAM * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    if (loss) *loss = lp_loss_value(lz, nrows);
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint64_t seed, double* loss_first,
+                                        double* loss_last) {
+    mps_status s = need_snapshot(h);
+    if (s != MPS_OK) return s;
+    if (iters < 0) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    const LpSystem L = ppe_lp_system(h->ppe, stage_args(h));
+    double first = 0.0, last = 0.0;
+    for (int k = 0; k < iters; k++) {
+        if (lp_loss_grad(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, seed + (uint64_t)k, h->cap, h->stream) != 0)
+            return MPS_ERR_CUDA;
+        if (k == 0 || k == iters - 1) {
+            double lz[2] = {0, 0};
+            uint32_t nrows = 0;
+            CK(cudaMemcpyAsync(lz, h->ppe.lp.loss, 16, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(&nrows, h->ppe.nrows, 4, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            const double v = lp_loss_value(lz, nrows);
+            if (k == 0) first = v;
+            last = v;
+        }
+        lp_adam(h->ppe.lp, lr, h->stream);
+    }
+    // refresh G for the current system with the updated weights
+    lp_forward(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, h->cap, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    if (loss_first) *loss_first = first;
+    if (loss_last) *loss_last = last;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
+                                       double* diag, uint32_t* count) {
+    mps_status s = need_semi(h);
+    if (s != MPS_OK) return s;
+    if (!h->ppe.have_snapshot) {
+        h->err = "no PPE system assembled yet";
+        return MPS_ERR_INVALID;
+    }
+    CK(cudaSetDevice(h->dev));
+    Scalars sc;
+    if (counts(h, &sc) != MPS_OK) return MPS_ERR_CUDA;
+    const size_t np = sc.np;
+    cudaStream_t st = h->stream;
+    if (pos4) CK(cudaMemcpyAsync(pos4, h->ppe.pos_snap, np * 16, cudaMemcpyDeviceToHost, st));
+    if (n) CK(cudaMemcpyAsync(n, h->ppe.n_snap, np * 4, cudaMemcpyDeviceToHost, st));
+    if (id) CK(cudaMemcpyAsync(id, h->ppe.id_snap, np * 4, cudaMemcpyDeviceToHost, st));
+    if (diag) CK(cudaMemcpyAsync(diag, h->ppe.diag64, np * 8, cudaMemcpyDeviceToHost, st));
+    if (is_row) {
+        CK(cudaMemcpyAsync(is_row, h->ppe.rlen, np * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (is_row)
+        for (size_t k = 0; k < np; k++) is_row[k] = is_row[k] != PPE_DIRICHLET ? 1u : 0u;
+    if (count) *count = (uint32_t)np;
     return MPS_OK;
 }
 

@@ -245,6 +245,15 @@ struct SolveArgs {
     const uint32_t* scols;
     const float4* pos;
     float rlap, rlap_thr;
+    // learned preconditioner
+    const uint32_t* lo_off;   // G' rows, sliced ELL (learned.cuh)
+    const uint32_t* lo_cols;
+    const float* lo_vals;
+    const uint32_t* up_off;   // G' columns
+    const uint32_t* up_cols;
+    const float* up_vals;
+    float* y;
+    float* ralt;
     Scalars* sc;
     double tol;
     int max_iter;
@@ -263,7 +272,22 @@ __device__ __forceinline__ float stencil_weight(const SolveArgs& S, const float4
     return (j != i && rr < S.rlap_thr) ? weight_rr<EX>(S.rlap, rr) : 0.f;
 }
 
-template <bool EX>
+// Row position k of the learned factor's packed layout: sum over its
+// entries of val * x(col), x given as a functor of the column.
+template <class X>
+__device__ __forceinline__ float lp_packed_row(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cols,
+                                               const float* __restrict__ vals, uint32_t k, X x) {
+    const uint32_t base = __ldg(off + k / LP_SLICE) + k % LP_SLICE;
+    const uint32_t W = (__ldg(off + k / LP_SLICE + 1) - __ldg(off + k / LP_SLICE)) / LP_SLICE;
+    float s = 0.f;
+    for (uint32_t t = 0; t < W; t++) {
+        const uint32_t e = base + t * LP_SLICE;
+        s = fmaf(__ldg(vals + e), x(__ldg(cols + e)), s);
+    }
+    return s;
+}
+
+template <bool EX, int PREC>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them
     // are dealt to warps round-robin (4 lanes per row inside a slice); the
@@ -302,13 +326,15 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const double bi = S.b64[i];
                 const double ri = bi - (S.diag64[i] * S.x64[i] + s);
                 const float rf = (float)ri;
-                const float zf = rf * S.inv_diag[i];
                 S.r[i] = rf;
-                S.z[i] = zf;
                 pcur[i] = 0.f;
                 acc[0] += ri * ri;
                 acc[1] += bi * bi;
-                acc[2] += (double)rf * (double)zf;
+                if (PREC == 0) {
+                    const float zf = rf * S.inv_diag[i];
+                    S.z[i] = zf;
+                    acc[2] += (double)rf * (double)zf;
+                }
             }
         }
         double tot[3];
@@ -321,6 +347,27 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             break;
         }
         if (total >= S.max_iter) break;
+        if (PREC == 1) {
+            // z = D^-1/2 G^T G D^-1/2 r: y = G D^-1/2 r, then z from y
+            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                const uint32_t i = __ldg(rowlist + kk);
+                const float* r = S.r;
+                S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r](uint32_t j) { return r[j]; });
+            }
+            double dummy[1] = {0.0}, td[1];
+            if (!grid_reduce<1>(dummy, S.part, S.result, S.bar, S.sc, td)) return;
+            double rzp[1] = {0.0};
+            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                const uint32_t i = __ldg(rowlist + kk);
+                const float* y = S.y;
+                const float zi = lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                S.z[i] = zi;
+                rzp[0] += (double)S.r[i] * (double)zi;
+            }
+            double tz[1];
+            if (!grid_reduce<1>(rzp, S.part, S.result, S.bar, S.sc, tz)) return;
+            tot[2] = tz[0];
+        }
         // inner target |r| <= eta |r64|
         double eta = 0.3 * S.tol / relres;
         if (eta < 1e-4) eta = 1e-4;
@@ -375,19 +422,55 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             const float alpha_f = (float)alpha;
             // ---- x64 += alpha p, r -= alpha q, z = M^-1 r, r.z, r.r
             double acc2[2] = {0.0, 0.0};
-            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
-                const uint32_t i = __ldg(rowlist + kk);
-                const float pn = pnew[i];
-                S.x64[i] += alpha * (double)pn;
-                const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
-                const float zi = ri * S.inv_diag[i];
-                S.r[i] = ri;
-                S.z[i] = zi;
-                acc2[0] += (double)ri * (double)zi;
-                acc2[1] += (double)ri * (double)ri;
-            }
             double tot2[2];
-            if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
+            if (PREC == 0) {
+                for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                    const uint32_t i = __ldg(rowlist + kk);
+                    const float pn = pnew[i];
+                    S.x64[i] += alpha * (double)pn;
+                    const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
+                    const float zi = ri * S.inv_diag[i];
+                    S.r[i] = ri;
+                    S.z[i] = zi;
+                    acc2[0] += (double)ri * (double)zi;
+                    acc2[1] += (double)ri * (double)ri;
+                }
+                if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
+            } else {
+                // new residual into the second buffer; y = G D^-1/2 r_new with
+                // the neighbours' r_new recomputed from r and q
+                float* rnew = S.ralt;
+                for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                    const uint32_t i = __ldg(rowlist + kk);
+                    const float pn = pnew[i];
+                    S.x64[i] += alpha * (double)pn;
+                    const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
+                    rnew[i] = ri;
+                    const float* r = S.r;
+                    const float* q = S.q;
+                    S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk,
+                                           [r, q, alpha_f](uint32_t j) { return fmaf(-alpha_f, q[j], r[j]); });
+                    acc2[1] += (double)ri * (double)ri;
+                }
+                double rrp[1] = {acc2[1]}, trr[1];
+                if (!grid_reduce<1>(rrp, S.part, S.result, S.bar, S.sc, trr)) return;
+                double rzp[1] = {0.0};
+                for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
+                    const uint32_t i = __ldg(rowlist + kk);
+                    const float* y = S.y;
+                    const float zi =
+                        lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                    S.z[i] = zi;
+                    rzp[0] += (double)rnew[i] * (double)zi;
+                }
+                double trz[1];
+                if (!grid_reduce<1>(rzp, S.part, S.result, S.bar, S.sc, trz)) return;
+                tot2[0] = trz[0];
+                tot2[1] = trr[0];
+                // swap the residual buffers
+                S.ralt = S.r;
+                S.r = rnew;
+            }
             total++;
             beta = (float)(tot2[0] / rz);
             rz = tot2[0];
@@ -628,6 +711,11 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.p[0], (size_t)cap * sizeof(float));
     ok &= al((void**)&w.p[1], (size_t)cap * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
+    ok &= al((void**)&w.y, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.ralt, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.pos_snap, (size_t)cap * sizeof(float4));
+    ok &= al((void**)&w.n_snap, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.id_snap, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.sell_off, ((size_t)cap / SELL_C + 4) * sizeof(uint32_t));
     ok &= al((void**)&w.sell_cols, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(uint32_t));
     ok &= al((void**)&w.tilecnt, ((size_t)cap / 2048 + 2) * sizeof(uint32_t));
@@ -640,10 +728,15 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    int per_sm2 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppe_solve<true>, PPE_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_ppe_solve<false>, PPE_THREADS, 0);
-    per_sm = per_sm < per_sm2 ? per_sm : per_sm2;
+    {
+        int o[4] = {0, 0, 0, 0};
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], k_ppe_solve<true, 0>, PPE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], k_ppe_solve<false, 0>, PPE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], k_ppe_solve<true, 1>, PPE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], k_ppe_solve<false, 1>, PPE_THREADS, 0);
+        per_sm = o[0];
+        for (int q = 1; q < 4; q++) per_sm = o[q] < per_sm ? o[q] : per_sm;
+    }
     if (!coop || per_sm < 1) {
         *err = "device cannot run the cooperative PPE solver";
         return MPS_ERR_CUDA;
@@ -695,7 +788,42 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     launch_scan_exclusive(w.sell_off, maxslices + 1, st);
     k_sell_pack<<<blocks_for(maxslices * SELL_C, 256), 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows,
                                                                      w.sell_off, w.sell_cols);
-    return 7;
+    // the state this system was assembled from
+    cudaMemcpyAsync(w.pos_snap, a.cur.pos, (size_t)cap * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(w.id_snap, a.cur.id, (size_t)cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    w.have_snapshot = true;
+    int launched = 7;
+    if (w.lp.ready) {
+        const LpSystem L = ppe_lp_system(w, a);
+        lp_build_stencil(w.lp, L, cap, st);
+        lp_forward(w.lp, L, a.exact, cap, st);
+        launched += 10;
+    }
+    return launched;
+}
+
+LpSystem ppe_lp_system(const PpeWork& w, const StageArgs& a) {
+    LpSystem L;
+    L.pos = w.pos_snap;
+    L.n = w.n_snap;
+    L.id = w.id_snap;
+    L.rlen = w.rlen;
+    L.diag64 = w.diag64;
+    L.rowlist = w.rowlist;
+    L.nrows = w.nrows;
+    L.acols = w.cols;
+    L.cell = a.cur.cell;
+    L.cell_start = a.cell_start;
+    L.g = a.g;
+    L.P = a.P;
+    L.sc = a.sc;
+    return L;
+}
+
+int ppe_enable_learned(PpeWork& w, std::string* err) {
+    if (w.lp.ready) return MPS_OK;
+    return lp_setup(w.lp, w.cap, err);
 }
 
 int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
@@ -722,22 +850,34 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.pos = a.cur.pos;
     S.rlap = a.P.rlap;
     S.rlap_thr = a.P.rlap_thr;
+    S.lo_off = w.lp.lo_off;
+    S.lo_cols = w.lp.lo_cols;
+    S.lo_vals = w.lp.lo_vals;
+    S.up_off = w.lp.up_off;
+    S.up_cols = w.lp.up_cols;
+    S.up_vals = w.lp.up_vals;
+    S.y = w.y;
+    S.ralt = w.ralt;
     S.sc = a.sc;
     S.tol = opt.cg_tol;
     S.max_iter = opt.cg_max_iter;
     S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
     S.max_outer = 40;
     void* args[] = {&S};
-    w.launch_err = cudaLaunchCooperativeKernel(a.exact ? (const void*)k_ppe_solve<true> : (const void*)k_ppe_solve<false>,
-                                               w.blocks, PPE_THREADS, args, 0, st);
+    const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+    const void* fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1> : (const void*)k_ppe_solve<true, 0>)
+                             : (learned ? (const void*)k_ppe_solve<false, 1> : (const void*)k_ppe_solve<false, 0>);
+    w.launch_err = cudaLaunchCooperativeKernel(fn, w.blocks, PPE_THREADS, args, 0, st);
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
     return 2;
 }
 
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
-                  w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar, w.gvals,
-                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols};
+                  w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar,
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.y, w.ralt, w.pos_snap, w.n_snap,
+                  w.id_snap};
+    lp_free(w.lp);
     for (void* p : ps)
         if (p) cudaFree(p);
     w = PpeWork();

@@ -18,11 +18,12 @@
 #include <cuda_runtime.h>
 
 #include "../../include/mps_capi.h"
+#include "learned.cuh"
 #include "physics.cuh"
 
 namespace mpsb {
 
-constexpr uint32_t PPE_W = 352;        // stride: > the 256 lattice neighbours within 4 l0
+constexpr uint32_t PPE_W = 512;        // stride: 2x the 256 lattice neighbours within 4 l0
 constexpr uint32_t PPE_DIRICHLET = 0xffffffffu;
 constexpr int PPE_THREADS = 1024;
 constexpr int PPE_PARTS = 4;           // FP64 partial sums per block
@@ -48,16 +49,27 @@ struct PpeWork {
     uint32_t* sell_off = nullptr;      // slice offsets (exclusive scan of 32 * width)
     uint32_t* sell_cols = nullptr;
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
-    // preconditioner (learned factor G); unused for the diagonal one
-    float* gvals = nullptr;
+    // learned preconditioner (set up on first use)
+    LearnedWork lp;
+    float* y = nullptr;                // G D^-1/2 r
+    float* ralt = nullptr;             // second residual buffer
+    // state at the last assembly (the system the network and its training see)
+    float4* pos_snap = nullptr;
+    float* n_snap = nullptr;
+    uint32_t* id_snap = nullptr;
+    bool have_snapshot = false;
     double n0_64 = 0.0, lambda64 = 0.0, alpha64 = 0.0;
     cudaError_t launch_err = cudaSuccess;  // of the last cooperative launch
 };
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
               std::string* err);
-// assembly, row list and sliced-ELL layout; returns the kernels enqueued
+// assembly, row list and sliced-ELL layout (and, with the learned
+// preconditioner, its stencil and network forward); returns the kernels enqueued
 int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
+// the system the network works on, from the last assembly
+LpSystem ppe_lp_system(const PpeWork& w, const StageArgs& a);
+int ppe_enable_learned(PpeWork& w, std::string* err);
 // the persistent solve and p = max(x, 0); returns the kernels enqueued
 int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);

@@ -1,0 +1,120 @@
+"""Learned PPE preconditioner: GPU gradients against the float64 CPU oracle,
+SPD safety of the learned PCG, and what training gains over diagonal
+scaling."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import load_golden, write_golden_case
+
+pytestmark = pytest.mark.gpu
+
+
+def random_params(capi, seed, om_scale=0.05):
+    import precond_oracle as po
+    rng = np.random.default_rng(seed)
+    w = np.zeros(capi.lib().mps_precond_num_params(), np.float32)
+    k = 0
+    for name, shape in po.LAYOUT:
+        n = int(np.prod(shape))
+        fan = shape[-1] if len(shape) == 2 else 64
+        scale = {"om": om_scale, "dl": 0.05, "bd": 0.3}.get(name, 1.0 / np.sqrt(fan))
+        w[k:k + n] = rng.uniform(-scale, scale, n)
+        k += n
+    w[-1] += 0.5413  # softplus(bd) ~ 1
+    return po.to_bf16(w)
+
+
+def sim_and_system(capi, d, w, steps=3):
+    import precond_oracle as po
+    s = capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, precond=capi.PRECOND_LEARNED)
+    s.set_precond_params(w)
+    s.step(steps)
+    snap = s.ppe_snapshot()
+    sc = s.scalars()
+    # input.dat holds label/value line pairs: DP is the 4th value, R0 and
+    # RLAP (multiples of DP) the 5th and 6th; the solver forms them in float32
+    val = open(os.path.join(d, "input.dat")).read().split("\n")[1::2]
+    dp = np.float32(float(val[3]))
+    r0 = np.float32(np.float32(float(val[4])) * dp)
+    rlap = np.float32(np.float32(float(val[5])) * dp)
+    system = po.System(snap, r0, rlap, float(np.float32(1.0 / sc["nzero"])))
+    return s, system
+
+
+def test_gradients_match_cpu_oracle(capi, tmp_path):
+    import precond_oracle as po
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    w = random_params(capi, 0)
+    s, system = sim_and_system(capi, d, w)
+    with s:
+        loss_gpu, grad = s.precond_loss_grad(seed=7)
+    loss_cpu = system.loss(w, 7)
+    assert abs(loss_gpu - loss_cpu) <= 1e-5 + 1e-4 * abs(loss_cpu), (loss_gpu, loss_cpu)
+    rng = np.random.default_rng(1)
+    # directional derivatives along random directions
+    for _ in range(3):
+        v = rng.standard_normal(len(w))
+        v /= np.linalg.norm(v)
+        fd = po.directional_fd(system, w, v, 7, h=1e-3)
+        an = float(grad.astype(np.float64) @ v)
+        assert abs(fd - an) <= 2e-3 * max(abs(fd), 1e-6) + 1e-7, (fd, an)
+    # single parameters with the largest gradients
+    idx = np.argsort(-np.abs(grad))[:12]
+    for k in idx:
+        v = np.zeros(len(w)); v[k] = 1.0
+        fd = po.directional_fd(system, w, v, 7, h=1e-3)
+        assert abs(fd - grad[k]) <= 5e-3 * max(abs(fd), 1e-6) + 1e-7, (int(k), fd, grad[k])
+
+
+def test_learned_pcg_is_spd_safe(capi, tmp_path):
+    """With untrained random network weights M^-1 = D^-1/2 G^T G D^-1/2 is
+    still SPD, so the learned PCG reaches the FP64 tolerance and its pressure
+    agrees with the diagonally scaled CG's to the accuracy of the solves."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    press = {}
+    for name, pc in (("diag", capi.PRECOND_DIAGONAL), ("learned", capi.PRECOND_LEARNED)):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, precond=pc) as s:
+            if pc == capi.PRECOND_LEARNED:
+                s.set_precond_params(random_params(capi, 3))
+            st = s.step(1)
+            assert st.cg_relres <= 1e-8 and st.status == 0
+            press[name] = s.state(capi.ORDER_BY_ID)["press"].astype(np.float64)
+    scale = np.abs(press["diag"]).max()
+    assert np.abs(press["learned"] - press["diag"]).max() <= 1e-4 * scale
+
+
+def test_training_lowers_the_loss(capi, tmp_path):
+    """Adam on one system lowers the loss measured with a fixed probe."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, precond=capi.PRECOND_LEARNED) as s:
+        s.step(4)
+        before, _ = s.precond_loss_grad(seed=99)
+        s.precond_train(200, 2e-3, 1000)
+        after, _ = s.precond_loss_grad(seed=99)
+        assert after < before - 1e-4, (before, after)
+
+
+def test_trained_network_reduces_cg_iterations(capi, tmp_path):
+    """The committed trained weights against plain diagonal scaling on a
+    held-out seed: same FP64 tolerance, fewer PCG iterations."""
+    from mps_solvers_b200 import precond_weights, scene
+    w = precond_weights.load()
+    d = str(tmp_path / "c")
+    scene.write_case(d, scene.dam_break_semi(seed=11))
+    it = {}
+    for name, pc in (("diag", capi.PRECOND_DIAGONAL), ("learned", capi.PRECOND_LEARNED)):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, precond=pc, arith=capi.ARITH_FAST) as s:
+            if pc == capi.PRECOND_LEARNED:
+                s.set_precond_params(w)
+            tot = 0
+            for _ in range(10):
+                st = s.step(1)
+                assert st.cg_relres <= 1e-8
+                tot += st.cg_iters
+            it[name] = tot
+    assert it["learned"] < it["diag"], it
