@@ -267,6 +267,41 @@ mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t n, const mp
                                      uint32_t* perm_dev, uint32_t* cell_of_dev, uint32_t* start_dev,
                                      uint32_t* end_dev, uint32_t* n_in_grid_dev, void* stream);
 
+/* ---- batches of scenes and the tank-acceleration body force ----
+ * No counterpart in the reference, which runs one scene per process
+ * (MPS_CAL_expl_v1.0/main.cpp:13-24).  A batch steps up to 256 scenes (each
+ * its own input.dat / GEO.dat, grid, constants, dt and time) as one particle
+ * set: every stage is one launch over all scenes, and the semi-implicit PPE
+ * of all scenes is one persistent launch in which each scene runs its own
+ * PCG to options.cg_tol.  Each scene evolves as it would in its own handle.
+ * Particle ids of scene s are id_base(s) + its GEO.dat index;
+ * mps_get_state(..., MPS_ORDER_BY_ID) returns all scenes in that order. */
+typedef struct mps_scene_spec {
+    const char* input_dat;
+    const char* geo_dat;
+    /* tank acceleration a(t) = accel_amp sin(2 pi accel_freq t) along x; the
+     * viscosity stage's body force becomes g - a(t) (0: plain gravity) */
+    float accel_amp;   /* m/s^2 */
+    float accel_freq;  /* Hz */
+    uint32_t reserved[4];
+} mps_scene_spec;
+
+typedef struct mps_scene_info {
+    uint32_t id_base, np0, nb2, nb1;
+    float time, dt, nzero, pad;
+    int cg_iters, cg_outer;  /* the scene's last PPE solve */
+    double cg_relres;
+    uint32_t reserved[4];
+} mps_scene_info;
+
+mps_status mps_batch_create(const mps_scene_spec* scenes, uint32_t nscenes, const mps_options* opt,
+                            mps_handle** out);
+/* nsteps steps of every scene (the same as mps_step on a batch handle) */
+mps_status mps_batch_step(mps_handle* h, int nsteps, mps_step_stats* stats);
+mps_status mps_batch_scene_info(mps_handle* h, uint32_t scene, mps_scene_info* info);
+/* Set the tank acceleration of a scene (scene 0 of a single-scene handle). */
+mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float accel_amp, float accel_freq);
+
 #ifdef __cplusplus
 }
 #endif

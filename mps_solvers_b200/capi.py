@@ -38,7 +38,8 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_phase", "mps_get_stream", "mps_write_case", "mps_last_error", "mps_cell_sort_dev",
            "mps_profile_steps", "mps_stage_name", "mps_cell_sort_dev_noalloc",
            "mps_precond_num_params", "mps_precond_get_params", "mps_precond_set_params",
-           "mps_precond_loss_grad", "mps_precond_train", "mps_ppe_snapshot")
+           "mps_precond_loss_grad", "mps_precond_train", "mps_ppe_snapshot",
+           "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force")
 
 
 class mps_options(C.Structure):
@@ -65,6 +66,18 @@ class mps_grid(C.Structure):
     _fields_ = [("left", C.c_float), ("back", C.c_float), ("bottom", C.c_float),
                 ("cell_size", C.c_float), ("cdx", C.c_uint32), ("cdy", C.c_uint32),
                 ("cdz", C.c_uint32), ("ncells", C.c_uint32), ("dim", C.c_int)]
+
+
+class mps_scene_spec(C.Structure):
+    _fields_ = [("input_dat", C.c_char_p), ("geo_dat", C.c_char_p), ("accel_amp", C.c_float),
+                ("accel_freq", C.c_float), ("reserved", C.c_uint32 * 4)]
+
+
+class mps_scene_info(C.Structure):
+    _fields_ = [("id_base", C.c_uint32), ("np0", C.c_uint32), ("nb2", C.c_uint32), ("nb1", C.c_uint32),
+                ("time", C.c_float), ("dt", C.c_float), ("nzero", C.c_float), ("pad", C.c_float),
+                ("cg_iters", C.c_int), ("cg_outer", C.c_int), ("cg_relres", C.c_double),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class MPSError(RuntimeError):
@@ -125,6 +138,11 @@ def lib():
             "mps_cell_sort_dev_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(mps_grid),
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_void_p]),
+            "mps_batch_create": (C.c_int, [C.POINTER(mps_scene_spec), C.c_uint32, C.POINTER(mps_options),
+                                           C.POINTER(H)]),
+            "mps_batch_step": (C.c_int, [H, C.c_int, C.POINTER(mps_step_stats)]),
+            "mps_batch_scene_info": (C.c_int, [H, C.c_uint32, C.POINTER(mps_scene_info)]),
+            "mps_set_body_force": (C.c_int, [H, C.c_uint32, C.c_float, C.c_float]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
@@ -184,6 +202,36 @@ class Simulation:
             msg = L.mps_last_error(h).decode() if h else ""
             self.close()
             raise MPSError(st, msg)
+        return self
+
+    @classmethod
+    def batch(cls, case_dirs, accel=None, options: Optional[mps_options] = None, **opt) -> "Simulation":
+        """A batch handle over the scenes in `case_dirs` (each with input.dat
+        and GEO.dat); accel[s] = (amplitude m/s^2, frequency Hz) of scene s's
+        tank acceleration."""
+        self = cls.__new__(cls)
+        L = lib()
+        self.options = options if options is not None else default_options(**opt)
+        n = len(case_dirs)
+        specs = (mps_scene_spec * n)()
+        keep = []
+        for s, d in enumerate(case_dirs):
+            a = os.path.join(d, "input.dat").encode()
+            g = os.path.join(d, "GEO.dat").encode()
+            keep += [a, g]
+            specs[s].input_dat = a
+            specs[s].geo_dat = g
+            amp, freq = accel[s] if accel is not None else (0.0, 0.0)
+            specs[s].accel_amp = amp
+            specs[s].accel_freq = freq
+        h = C.c_void_p()
+        st = L.mps_batch_create(specs, n, C.byref(self.options), C.byref(h))
+        self.h = h
+        if st != 0:
+            msg = L.mps_last_error(h).decode() if h else ""
+            self.close()
+            raise MPSError(st, msg)
+        self.nscenes = n
         return self
 
     def _check(self, st: int):
@@ -323,6 +371,15 @@ class Simulation:
                                            out["diag"].ctypes.data_as(C.POINTER(C.c_double)),
                                            C.byref(cnt)))
         return out
+
+    def set_body_force(self, accel_amp: float, accel_freq: float, scene: int = 0):
+        """Tank acceleration accel_amp*sin(2*pi*accel_freq*t) along x."""
+        self._check(lib().mps_set_body_force(self.h, scene, accel_amp, accel_freq))
+
+    def scene_info(self, scene: int = 0) -> mps_scene_info:
+        info = mps_scene_info()
+        self._check(lib().mps_batch_scene_info(self.h, scene, C.byref(info)))
+        return info
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -60,6 +60,15 @@ struct mps_handle {
     cudaError_t launch_err = cudaSuccess;  // first failed launch not seen by cudaGetLastError
     std::string err;
     std::vector<void*> allocs;
+    // batch of scenes (nscenes == 0: a single scene)
+    uint32_t nscenes = 0;
+    BatchDev batch{};
+    std::vector<uint32_t> id_base;   // first particle id of each scene, then the total
+    std::vector<uint32_t> scene_nb2, scene_nb1;
+    std::vector<Phys> scene_phys;
+    std::vector<Grid> scene_grid;
+    std::vector<HostConst> scene_hc;
+    Phys* phys_dev = nullptr;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -118,6 +127,7 @@ static StageArgs stage_args(mps_handle* h) {
     a.list_solid = h->list_solid;
     a.n_solid = &h->sc->n_solid;
     a.cap_solid = h->cap_solid;
+    a.batch = h->batch;
     return a;
 }
 
@@ -148,14 +158,15 @@ static void rebuild(mps_handle* h, int apply) {
     State& src = h->S[h->cur];
     State& dst = h->S[h->cur ^ 1];
     mark(h, ST_KEYS);
-    launch_cell_keys(src.pos, src.vel, h->tmp, apply, h->g, h->sc, h->sort.keys[0], h->sort.vals[0], h->cap, st);
+    launch_cell_keys(src.pos, src.vel, h->tmp, apply, h->g, h->sc, h->sort.keys[0], h->sort.vals[0], h->cap, st,
+                     src.id, h->batch);
     mark(h, ST_SORT);
     const int r = launch_radix_sort(h->sort, &h->sc->np, h->passes, h->cap, st);
     mark(h, ST_CELLS);
     launch_cell_start(h->sort.keys[r], h->g, h->sc, h->cell_start, h->cap, st);
     mark(h, ST_GATHER);
     launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
-                  h->list_fluid, h->list_solid);
+                  h->list_fluid, h->list_solid, h->batch);
     h->launches += 3 + 3 * h->passes;
     h->cur ^= 1;
 }
@@ -197,7 +208,7 @@ static void enqueue_step(mps_handle* h) {
         launch_update_dt(stage_args(h), cap, st);
         h->launches += 1;
     }
-    launch_step_end(h->sc, st);
+    launch_step_end(h->sc, h->batch, st);
     h->launches += 5;
 }
 
@@ -229,6 +240,74 @@ extern "C" void mps_default_options(mps_options* o) {
     o->capacity = 0;
 }
 
+// constants of a scene that do not depend on n0
+static Phys base_phys(const mps_params& prm) {
+    Phys P;
+    memset(&P, 0, sizeof P);
+    P.rzero = prm.rzero;
+    P.rlap = prm.rlap;
+    P.col_dis = prm.col_dis;
+    P.col_rate = prm.col_rate;
+    P.niu = prm.niu;
+    P.rho = prm.rho;
+    P.dt_max = prm.dt_max;
+    P.dt_min = prm.dt_min;
+    P.cfl_dp = prm.cfl * prm.dp;
+    P.beta = prm.beta;
+    P.g[0] = 0.0f;
+    P.g[1] = 0.0f;
+    P.g[2] = -9.81f;
+    P.dim_f = (float)prm.dim;
+    P.rzero_thr = rr_threshold(prm.rzero);
+    P.rlap_thr = rr_threshold(prm.rlap);
+    P.col_thr = rr_threshold(prm.col_dis);
+    P.rzero2 = prm.rzero * prm.rzero;
+    return P;
+}
+
+// MPS_CPU::Initial / MPS::calOnce of MPS_CAL_v4.0 (MPS_CPU.cpp:54-122,
+// MPS.cpp:305-370): the constants from n0 and lambda in double
+static HostConst semi_constants(const mps_params& prm, double n0, double lambda) {
+    HostConst c;
+    c.nzero = (float)n0;
+    c.lambda = (float)lambda;
+    c.alpha = (float)(1.0 / ((double)prm.rho * prm.cs * prm.cs));
+    c.one_over_alpha = (float)((double)prm.rho * prm.cs * prm.cs);
+    c.one_over_rho = (float)(1.0 / (double)prm.rho);
+    c.one_over_nzero = (float)(1.0 / n0);
+    c.one_over_dim = (float)(1.0 / (double)prm.dim);
+    c.one_over_dt = (float)(1.0 / (double)prm.dt_max);
+    c.c_lap = (float)((2.0 * prm.dim) / (n0 * lambda));
+    return c;
+}
+
+static void apply_constants(Phys& P, const HostConst& c) {
+    P.nzero = c.nzero;
+    P.one_over_nzero = c.one_over_nzero;
+    P.one_over_alpha = c.one_over_alpha;
+    P.one_over_rho = c.one_over_rho;
+    P.c_lap = c.c_lap;
+    P.lambda = c.lambda;
+    P.alpha = c.alpha;
+    P.one_over_dt_fixed = c.one_over_dt;
+}
+
+static Grid device_grid(const HostGrid& hg, uint32_t base) {
+    Grid g;
+    g.left = hg.left;
+    g.back = hg.back;
+    g.bottom = hg.bottom;
+    g.cell_size = hg.cell_size;
+    g.cdx = hg.cdx;
+    g.cdy = hg.cdy;
+    g.cdz = hg.cdz;
+    g.sheet = hg.sheet;
+    g.ncells = hg.ncells;
+    g.dim = hg.dim;
+    g.base = base;
+    return g;
+}
+
 static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint32_t nb2, uint32_t nb1,
                         const float* pos3, const float* vel3, const float* press) {
     h->prm = prm;
@@ -254,6 +333,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     g.sheet = h->hg.sheet;
     g.ncells = h->hg.ncells;
     g.dim = h->hg.dim;
+    g.base = 0;
     h->passes = sort_passes(g.ncells);
     // reach (in cells) that covers sqrt(2) r0 for the dummy-to-wall search
     {
@@ -320,31 +400,14 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         sc0.np = np;
         sc0.np_new = np;
         sc0.dt = prm.dt_max;
+        sc0.g_eff[2] = -9.81f;
         CK(cudaMemcpyAsync(h->sc, &sc0, sizeof sc0, cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
 
     // constants that do not depend on n0
     Phys& P = h->P;
-    memset(&P, 0, sizeof P);
-    P.rzero = prm.rzero;
-    P.rlap = prm.rlap;
-    P.col_dis = prm.col_dis;
-    P.col_rate = prm.col_rate;
-    P.niu = prm.niu;
-    P.rho = prm.rho;
-    P.dt_max = prm.dt_max;
-    P.dt_min = prm.dt_min;
-    P.cfl_dp = prm.cfl * prm.dp;
-    P.beta = prm.beta;
-    P.g[0] = 0.0f;
-    P.g[1] = 0.0f;
-    P.g[2] = -9.81f;
-    P.dim_f = (float)prm.dim;
-    P.rzero_thr = rr_threshold(prm.rzero);
-    P.rlap_thr = rr_threshold(prm.rlap);
-    P.col_thr = rr_threshold(prm.col_dis);
-    P.rzero2 = prm.rzero * prm.rzero;
+    P = base_phys(prm);
 
     // MPS_GPU::Initial (MPS_CAL_expl_v1.0/MPS_GPU.cpp:63-115): divideCell, then calOnce.
     rebuild(h, APPLY_NONE);
@@ -369,16 +432,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         }
         h->ppe.n0_64 = hr[0];
         h->ppe.lambda64 = hr[1];
-        HostConst& c = h->hc;
-        c.nzero = (float)hr[0];
-        c.lambda = (float)hr[1];
-        c.alpha = (float)(1.0 / ((double)prm.rho * prm.cs * prm.cs));
-        c.one_over_alpha = (float)((double)prm.rho * prm.cs * prm.cs);
-        c.one_over_rho = (float)(1.0 / (double)prm.rho);
-        c.one_over_nzero = (float)(1.0 / hr[0]);
-        c.one_over_dim = (float)(1.0 / (double)prm.dim);
-        c.one_over_dt = (float)(1.0 / (double)prm.dt_max);
-        c.c_lap = (float)((2.0 * prm.dim) / (hr[0] * hr[1]));
+        h->hc = semi_constants(prm, hr[0], hr[1]);
     } else {
         StageArgs a = stage_args(h);
         launch_pnd(a, 0, 1, h->cap, h->stream);  // n of every particle
@@ -400,14 +454,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         }
         derive_constants(prm, n0, lam, &h->hc);
     }
-    P.nzero = h->hc.nzero;
-    P.one_over_nzero = h->hc.one_over_nzero;
-    P.one_over_alpha = h->hc.one_over_alpha;
-    P.one_over_rho = h->hc.one_over_rho;
-    P.c_lap = h->hc.c_lap;
-    P.lambda = h->hc.lambda;
-    P.alpha = h->hc.alpha;
-    P.one_over_dt_fixed = h->hc.one_over_dt;
+    apply_constants(P, h->hc);
 
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
         int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
@@ -457,6 +504,352 @@ extern "C" mps_status mps_create_from_arrays(const mps_params* p, uint32_t np, u
     int st = setup(h, *p, np, nb2, nb1, pos3, vel3, press);
     *out = h;
     return (mps_status)st;
+}
+
+// ---------------------------------------------------------------- batch
+// A batch is one particle set made of the scenes' particles (ids offset by
+// the earlier scenes' counts), one cell space made of each scene's own grid
+// (offset by the earlier grids' cells), and per-scene constants and step
+// scalars.  Every stage kernel runs once over all scenes; a particle reads
+// its scene's grid, constants and dt, so each scene evolves as it would
+// alone.
+static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms, const std::vector<Geo>& geos,
+                              const mps_scene_spec* specs) {
+    const uint32_t S = (uint32_t)prms.size();
+    for (uint32_t s = 1; s < S; s++)
+        if (prms[s].dim != prms[0].dim) {
+            h->err = "every scene of a batch must have the same dimension";
+            return MPS_ERR_INVALID;
+        }
+    if (h->opt.precond == MPS_PRECOND_LEARNED) {
+        h->err = "the learned preconditioner is not available for batches";
+        return MPS_ERR_INVALID;
+    }
+    h->prm = prms[0];
+    h->nscenes = S;
+    uint64_t np64 = 0;
+    h->id_base.assign(S + 1, 0);
+    h->nb2 = h->nb1 = 0;
+    uint32_t nfluid = 0;
+    for (uint32_t s = 0; s < S; s++) {
+        h->id_base[s] = (uint32_t)np64;
+        np64 += geos[s].np;
+        h->nb2 += geos[s].nb2;
+        h->nb1 += geos[s].nb1;
+        nfluid += geos[s].np - geos[s].nb2 - geos[s].nb1;
+        h->scene_nb2.push_back(geos[s].nb2);
+        h->scene_nb1.push_back(geos[s].nb1);
+    }
+    if (np64 >= 0xffffffffull) {
+        h->err = "too many particles in the batch";
+        return MPS_ERR_INVALID;
+    }
+    const uint32_t np = (uint32_t)np64;
+    h->id_base[S] = np;
+    h->np0 = np;
+    h->cap = h->opt.capacity > np ? h->opt.capacity : np;
+    CK(cudaSetDevice(h->opt.device));
+    h->dev = h->opt.device;
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    // per-scene grids in one cell space
+    uint64_t cells = 0;
+    int reach = 1;
+    for (uint32_t s = 0; s < S; s++) {
+        HostGrid hg;
+        int st = make_grid(prms[s], geos[s].pos.data(), geos[s].np, &hg, &h->err);
+        if (st != MPS_OK) {
+            h->err = "scene " + std::to_string(s) + ": " + h->err;
+            return (mps_status)st;
+        }
+        if (s == 0) h->hg = hg;
+        h->scene_grid.push_back(device_grid(hg, (uint32_t)cells));
+        cells += hg.ncells;
+        const double need = std::sqrt(2.0) * (double)prms[s].rzero;
+        const int r = (int)std::ceil(need / (double)hg.cell_size - 1e-12);
+        reach = r > reach ? r : reach;
+    }
+    if (cells >= 0xffffffffull) {
+        h->err = "too many cells in the batch";
+        return MPS_ERR_INVALID;
+    }
+    h->g = h->scene_grid[0];
+    h->g.ncells = (uint32_t)cells;  // the whole cell space (cell table and sort)
+    h->g.base = 0;
+    h->passes = sort_passes(h->g.ncells);
+    h->normal_reach = reach;
+
+    const uint32_t cap = h->cap;
+    for (int b = 0; b < 2; b++) {
+        State& st = h->S[b];
+        CK(dalloc(h, &st.pos, cap));
+        CK(dalloc(h, &st.vel, cap));
+        CK(dalloc(h, &st.press, cap));
+        CK(dalloc(h, &st.n, cap));
+        CK(dalloc(h, &st.id, cap));
+        CK(dalloc(h, &st.cell, cap));
+    }
+    CK(dalloc(h, &h->tmp, cap));
+    CK(dalloc(h, &h->index_of_id, cap));
+    CK(dalloc(h, &h->normal_id_of, cap));
+    h->cap_fluid = nfluid;
+    h->cap_solid = np - h->nb2;
+    CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
+    CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
+    CK(dalloc(h, &h->cell_start, (size_t)h->g.ncells + 1));
+    h->sort.tiles = sort_tiles(cap);
+    for (int b = 0; b < 2; b++) {
+        CK(dalloc(h, &h->sort.keys[b], cap));
+        CK(dalloc(h, &h->sort.vals[b], cap));
+    }
+    CK(dalloc(h, &h->sort.hist, (size_t)SORT_RADIX * h->sort.tiles));
+    CK(dalloc(h, &h->stage.pos3, 3 * (size_t)cap));
+    CK(dalloc(h, &h->stage.vel3, 3 * (size_t)cap));
+    CK(dalloc(h, &h->stage.press, cap));
+    CK(dalloc(h, &h->stage.n, cap));
+    CK(dalloc(h, &h->stage.id, cap));
+    CK(dalloc(h, &h->stage.type, cap));
+    CK(dalloc(h, &h->sc, 1));
+    CK(dalloc(h, &h->best, 1));
+    CK(dalloc(h, &h->lambda_dev, 1));
+    // scene tables
+    uint32_t* sid = nullptr;
+    Grid* grid_dev = nullptr;
+    CK(dalloc(h, &sid, np));
+    CK(dalloc(h, &grid_dev, S));
+    CK(dalloc(h, &h->phys_dev, S));
+    CK(dalloc(h, &h->batch.dt, S));
+    CK(dalloc(h, &h->batch.time, S));
+    CK(dalloc(h, &h->batch.g_eff, S));
+    CK(dalloc(h, &h->batch.vmax2_bits, S));
+    h->batch.n = S;
+    h->batch.sid_of_id = sid;
+    h->batch.grid = grid_dev;
+    h->batch.phys = h->phys_dev;
+    h->batch.ncells = h->g.ncells;
+    for (uint32_t s = 0; s < S; s++) {
+        Phys P = base_phys(prms[s]);
+        P.body_amp = (double)specs[s].accel_amp;
+        P.body_omega = 2.0 * M_PI * (double)specs[s].accel_freq;
+        h->scene_phys.push_back(P);
+    }
+    {
+        std::vector<float4> p4(np), v4(np);
+        std::vector<uint32_t> ids(np), sids(np);
+        std::vector<float> pr(np, 0.f), dts(S), times(S, 0.f);
+        std::vector<float4> ge(S, make_float4(0.f, 0.f, -9.81f, 0.f));
+        for (uint32_t s = 0; s < S; s++) {
+            const Geo& g = geos[s];
+            for (uint32_t k = 0; k < g.np; k++) {
+                const uint32_t i = h->id_base[s] + k;
+                const uint32_t t = k < g.nb2 ? T_DUMMY : (k < g.nb2 + g.nb1 ? T_WALL : T_FLUID);
+                float w;
+                memcpy(&w, &t, 4);
+                p4[i] = make_float4(g.pos[3 * k], g.pos[3 * k + 1], g.pos[3 * k + 2], w);
+                v4[i] = make_float4(g.vel[3 * k], g.vel[3 * k + 1], g.vel[3 * k + 2], 0.f);
+                pr[i] = g.press[k];
+                ids[i] = i;
+                sids[i] = s;
+            }
+            dts[s] = prms[s].dt_max;
+        }
+        State& st0 = h->S[0];
+        CK(cudaMemcpyAsync(st0.pos, p4.data(), np * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(st0.vel, v4.data(), np * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(st0.press, pr.data(), np * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(st0.id, ids.data(), np * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(sid, sids.data(), np * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(grid_dev, h->scene_grid.data(), S * sizeof(Grid), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->phys_dev, h->scene_phys.data(), S * sizeof(Phys), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->batch.dt, dts.data(), S * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->batch.time, times.data(), S * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->batch.g_eff, ge.data(), S * sizeof(float4), cudaMemcpyHostToDevice, h->stream));
+        Scalars sc0;
+        memset(&sc0, 0, sizeof sc0);
+        sc0.np = np;
+        sc0.np_new = np;
+        sc0.dt = prms[0].dt_max;
+        sc0.g_eff[2] = -9.81f;
+        CK(cudaMemcpyAsync(h->sc, &sc0, sizeof sc0, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->P = h->scene_phys[0];
+
+    // initial rebuild, then each scene's n0 and lambda from its own particles
+    rebuild(h, APPLY_NONE);
+    std::vector<uint32_t> lo(S), hi(S);
+    for (uint32_t s = 0; s < S; s++) {
+        const Grid& g = h->scene_grid[s];
+        CK(cudaMemcpyAsync(&lo[s], h->cell_start + g.base, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&hi[s], h->cell_start + g.base + g.ncells, 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<PpeScene> ppe_scenes(S);
+    StageArgs a = stage_args(h);
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        double* n64 = nullptr;
+        double* res = nullptr;
+        CK(dalloc(h, &n64, cap));
+        CK(dalloc(h, &res, 2 * (size_t)S));
+        launch_pnd64(a, n64, cap, h->stream);
+        for (uint32_t s = 0; s < S; s++) launch_n0_lambda64(a, n64, res + 2 * s, h->stream, lo[s], hi[s]);
+        std::vector<double> hr(2 * (size_t)S);
+        CK(cudaMemcpyAsync(hr.data(), res, hr.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaGetLastError());
+        for (uint32_t s = 0; s < S; s++) {
+            const double n0 = hr[2 * s], lam = hr[2 * s + 1];
+            if (!(n0 > 0.0)) {
+                h->err = "scene " + std::to_string(s) + ": n0 is not positive";
+                return MPS_ERR_INVALID;
+            }
+            const mps_params& q = prms[s];
+            const HostConst c = semi_constants(q, n0, lam);
+            h->scene_hc.push_back(c);
+            apply_constants(h->scene_phys[s], c);
+            const double rho = (double)q.rho, dim = (double)q.dim;
+            const double alpha = 1.0 / (rho * (double)q.cs * (double)q.cs);
+            const double one_over_dt = 1.0 / (double)q.dt_max;
+            ppe_scenes[s].n0 = n0;
+            ppe_scenes[s].beta = (double)q.beta;
+            ppe_scenes[s].b_tmp = lam * rho * (0.5 * (1.0 / dim) * one_over_dt * one_over_dt);
+            ppe_scenes[s].rho_lambda_alpha_n0 = rho * lam * alpha * n0;
+        }
+        h->ppe.n0_64 = ppe_scenes[0].n0;
+        h->ppe.lambda64 = hr[1];
+    } else {
+        launch_pnd(a, 0, 1, cap, h->stream);
+        for (uint32_t s = 0; s < S; s++) {
+            CK(cudaMemsetAsync(h->best, 0, sizeof(unsigned long long), h->stream));
+            launch_nzero_range(h->S[h->cur].n, lo[s], hi[s], h->best, h->stream);
+            launch_lambda(a, h->best, h->lambda_dev, h->stream);
+            unsigned long long best = 0;
+            float lam = 0.f;
+            CK(cudaMemcpyAsync(&best, h->best, 8, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(&lam, h->lambda_dev, 4, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            CK(cudaGetLastError());
+            const uint32_t nbits = (uint32_t)(best >> 32);
+            float n0;
+            memcpy(&n0, &nbits, 4);
+            if (!(n0 > 0.f)) {
+                h->err = "scene " + std::to_string(s) + ": n0 is not positive";
+                return MPS_ERR_INVALID;
+            }
+            HostConst c;
+            derive_constants(prms[s], n0, lam, &c);
+            h->scene_hc.push_back(c);
+            apply_constants(h->scene_phys[s], c);
+        }
+    }
+    launch_normals(a, h->normal_reach, h->normal_id_of, cap, h->stream);
+    CK(cudaMemcpyAsync(h->phys_dev, h->scene_phys.data(), S * sizeof(Phys), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->P = h->scene_phys[0];
+    h->hc = h->scene_hc[0];
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        int e = ppe_setup(h->ppe, cap, h->g, h->P, h->prm, h->stream, &h->err);
+        if (e != MPS_OK) return (mps_status)e;
+        e = ppe_setup_batch(h->ppe, ppe_scenes.data(), S, h->stream, &h->err);
+        if (e != MPS_OK) return (mps_status)e;
+    }
+    Scalars sc;
+    return read_status(h, &sc);
+}
+
+extern "C" mps_status mps_batch_create(const mps_scene_spec* scenes, uint32_t nscenes, const mps_options* opt,
+                                       mps_handle** out) {
+    if (!out || !scenes || nscenes == 0) return MPS_ERR_INVALID;
+    *out = nullptr;
+    mps_handle* h;
+    create_common(&h, opt);
+    *out = h;
+    if (nscenes > PPE_MAX_SCENES) {
+        h->err = "a batch holds at most " + std::to_string(PPE_MAX_SCENES) + " scenes";
+        return MPS_ERR_INVALID;
+    }
+    std::vector<mps_params> prms(nscenes);
+    std::vector<Geo> geos(nscenes);
+    for (uint32_t s = 0; s < nscenes; s++) {
+        if (!scenes[s].input_dat || !scenes[s].geo_dat) return MPS_ERR_INVALID;
+        int st = read_input_dat(scenes[s].input_dat, &prms[s], &h->err);
+        if (st == MPS_OK) st = read_geo_dat(scenes[s].geo_dat, &geos[s], &h->err);
+        if (st != MPS_OK) {
+            h->err = "scene " + std::to_string(s) + ": " + h->err;
+            return (mps_status)st;
+        }
+    }
+    return setup_batch(h, prms, geos, scenes);
+}
+
+extern "C" mps_status mps_batch_step(mps_handle* h, int nsteps, mps_step_stats* stats) {
+    return mps_step(h, nsteps, stats);
+}
+
+extern "C" mps_status mps_batch_scene_info(mps_handle* h, uint32_t scene, mps_scene_info* info) {
+    if (!h || !info) return MPS_ERR_INVALID;
+    const uint32_t S = h->nscenes ? h->nscenes : 1;
+    if (scene >= S) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    Scalars sc;
+    mps_status st = read_status(h, &sc);
+    if (st == MPS_ERR_CUDA) return st;
+    memset(info, 0, sizeof *info);
+    if (!h->nscenes) {
+        info->id_base = 0;
+        info->np0 = h->np0;
+        info->nb2 = h->nb2;
+        info->nb1 = h->nb1;
+        info->time = sc.time;
+        info->dt = sc.dt;
+        info->cg_iters = sc.cg_iters;
+        info->cg_outer = sc.cg_outer;
+        info->cg_relres = sc.cg_relres;
+        info->nzero = h->hc.nzero;
+        return MPS_OK;
+    }
+    info->id_base = h->id_base[scene];
+    info->np0 = h->id_base[scene + 1] - h->id_base[scene];
+    info->nb2 = h->scene_nb2[scene];
+    info->nb1 = h->scene_nb1[scene];
+    info->nzero = h->scene_hc[scene].nzero;
+    cudaStream_t s = h->stream;
+    CK(cudaMemcpyAsync(&info->time, h->batch.time + scene, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&info->dt, h->batch.dt + scene, 4, cudaMemcpyDeviceToHost, s));
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT && h->ppe.scene_iters) {
+        CK(cudaMemcpyAsync(&info->cg_iters, h->ppe.scene_iters + scene, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&info->cg_outer, h->ppe.scene_outer + scene, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&info->cg_relres, h->ppe.scene_relres + scene, 8, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float accel_amp, float accel_freq) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    const double amp = (double)accel_amp, omega = 2.0 * M_PI * (double)accel_freq;
+    if (h->nscenes) {
+        if (scene >= h->nscenes) return MPS_ERR_INVALID;
+        h->scene_phys[scene].body_amp = amp;
+        h->scene_phys[scene].body_omega = omega;
+        CK(cudaMemcpyAsync(h->phys_dev + scene, &h->scene_phys[scene], sizeof(Phys), cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return MPS_OK;
+    }
+    if (scene != 0) return MPS_ERR_INVALID;
+    h->P.body_amp = amp;
+    h->P.body_omega = omega;
+    // the captured steps hold the old constants
+    CK(cudaStreamSynchronize(h->stream));
+    for (int b = 0; b < 2; b++)
+        if (h->graph[b]) {
+            cudaGraphExecDestroy(h->graph[b]);
+            h->graph[b] = nullptr;
+        }
+    return MPS_OK;
 }
 
 extern "C" void mps_destroy(mps_handle* h) {
@@ -711,6 +1104,10 @@ extern "C" uint32_t mps_precond_num_params(void) { return (uint32_t)LP_NPARAM; }
 
 static mps_status need_semi(mps_handle* h) {
     if (!h) return MPS_ERR_INVALID;
+    if (h->nscenes) {
+        h->err = "the learned preconditioner is not available for batches";
+        return MPS_ERR_INVALID;
+    }
     if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) {
         h->err = "the learned preconditioner belongs to the semi-implicit method";
         return MPS_ERR_INVALID;
@@ -888,6 +1285,10 @@ extern "C" mps_status mps_write_case(mps_handle* h, const char* path, int format
 // whenever time - threshold >= 0, threshold += tout; then a step.
 extern "C" mps_status mps_run(mps_handle* h, const char* out_dir) {
     if (!h) return MPS_ERR_INVALID;
+    if (h->nscenes) {
+        h->err = "mps_run drives a single scene; step a batch with mps_batch_step";
+        return MPS_ERR_INVALID;
+    }
     float threshold = 0.0f;
     int count = 0;
     for (;;) {

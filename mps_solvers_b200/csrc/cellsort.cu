@@ -10,10 +10,14 @@
 namespace mpsb {
 
 // ---------------------------------------------------------------- keys
+// In a batch each particle is binned in its own scene's grid and keyed by
+// that grid's first global cell plus its cell there; outside its grid it
+// takes the sentinel of all scenes' cells.
 __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                    const float4* __restrict__ tmp, int apply, Grid g,
                                                    Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
-                                                   uint32_t* __restrict__ vals) {
+                                                   uint32_t* __restrict__ vals, const uint32_t* __restrict__ id,
+                                                   BatchDev batch) {
     const uint32_t n = sc->np;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -23,8 +27,13 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ po
     }
     if (i >= n) return;
     float4 p = pos[i];
+    uint32_t s = 0;
+    if (batch.n) {
+        s = batch.sid_of_id[id[i]];
+        g = batch.grid[s];
+    }
     if (apply != APPLY_NONE && ptype(p) == T_FLUID) {
-        const float dt = sc->dt;
+        const float dt = batch.n ? batch.dt[s] : sc->dt;
         float4 t = tmp[i];
         // x = x + dt * tmp, in float with one rounding per operation
         p.x = __fadd_rn(p.x, __fmul_rn(dt, t.x));
@@ -34,6 +43,7 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ po
     bool nan_flag = false;
     uint32_t k = cell_of_pos(g, p.x, p.y, p.z, &nan_flag);
     if (nan_flag) atomicOr(&sc->err, ERR_NAN);
+    if (batch.n) k = k == g.ncells ? batch.ncells : g.base + k;
     keys[i] = k;
     vals[i] = i;
 }
@@ -229,8 +239,9 @@ __global__ void k_start_end(const uint32_t* __restrict__ cs, uint32_t ncells, ui
 static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 
 void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
-                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st) {
-    k_cell_keys<<<blocks_for(cap, 256), 256, 0, st>>>(pos, vel, tmp, apply, g, sc, keys, vals);
+                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st, const uint32_t* id,
+                      const BatchDev& batch) {
+    k_cell_keys<<<blocks_for(cap, 256), 256, 0, st>>>(pos, vel, tmp, apply, g, sc, keys, vals, id, batch);
 }
 
 int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st) {

@@ -39,9 +39,12 @@ enum ApplyMode : int {
 };
 
 // Launchers (all asynchronous on `st`).
-// Stage 1: cell key of every active particle (after the pending update).
+// Stage 1: cell key of every active particle (after the pending update);
+// with batch.n > 0 g is the whole cell space and each particle (by id) uses
+// its scene's grid.
 void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
-                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st);
+                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st, const uint32_t* id,
+                      const BatchDev& batch);
 // Stage 2: stable LSD radix sort of (keys[0], vals[0]) over sc->np keys;
 // returns the buffer index (0/1) that holds the result.
 int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st);

@@ -10,6 +10,7 @@ struct Grid {
     float left, back, bottom, cell_size;
     uint32_t cdx, cdy, cdz, sheet, ncells;
     int dim;
+    uint32_t base;  // first global cell id of this grid (scenes of a batch; 0 otherwise)
 };
 
 // Per-scene constants, fixed after initialisation.
@@ -23,6 +24,9 @@ struct Phys {
     float rzero_thr, rlap_thr, col_thr, rzero2;
     // PPE (semi-implicit)
     float lambda, alpha, one_over_dt_fixed;
+    // tank acceleration a(t) = body_amp sin(body_omega t) along x; the body
+    // force of the viscosity stage is g - a(t)
+    double body_amp, body_omega;
 };
 
 // Device-resident per-step scalars (one instance per handle).
@@ -42,8 +46,33 @@ struct Scalars {
     uint32_t n_solid;      // entries of the fluid + wall list
     int cg_outer;          // FP64 true-residual passes of the last PPE solve
     int pad_i;
-    double pad[2];
+    float g_eff[3];        // body force of the current step: g - a(time)
+    float pad_f;
 };
+
+// The scenes of a batch: one particle set and one cell space made of each
+// scene's own particles and cell grid, with per-scene constants and step
+// scalars.  n == 0 (the default) is a single scene, and no array is read.
+struct BatchDev {
+    uint32_t n = 0;
+    const uint32_t* sid_of_id = nullptr;  // scene of each particle id
+    const Grid* grid = nullptr;           // per scene; base = its first global cell
+    const Phys* phys = nullptr;           // per scene
+    float* dt = nullptr;                  // per scene: dt of the current step
+    float* time = nullptr;                // per scene: simulated time
+    float4* g_eff = nullptr;              // per scene: g - a(time) of the current step
+    uint32_t* vmax2_bits = nullptr;       // per scene: max |u|^2 of the running update_dt
+    uint32_t ncells = 0;                  // cells of all scenes (the sentinel key)
+};
+
+// g - a(t) with a(t) = body_amp sin(body_omega t) along x, each component
+// rounded once to float; exactly g when there is no tank acceleration.
+__device__ __forceinline__ void body_force(const Phys& P, float t, float out[3]) {
+    out[0] = P.g[0];
+    out[1] = P.g[1];
+    out[2] = P.g[2];
+    if (P.body_amp != 0.0) out[0] = (float)((double)P.g[0] - P.body_amp * sin(P.body_omega * (double)t));
+}
 
 enum : uint32_t {
     ERR_DT_TOO_SMALL = 1u,

@@ -22,7 +22,8 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
                                                 const uint32_t* __restrict__ keys_sorted,
                                                 const float4* __restrict__ tmp, int apply,
                                                 uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc,
-                                                uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid) {
+                                                uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid,
+                                                BatchDev batch) {
     const uint32_t n = sc->np, nn = sc->np_new;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t ty = T_EXCL;
@@ -30,7 +31,7 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
         const uint32_t old = perm[p];
         float4 x = src.pos[old], u = src.vel[old];
         if (apply != 0 && ptype(x) == T_FLUID) {
-            const float dt = sc->dt;
+            const float dt = batch.n ? batch.dt[batch.sid_of_id[src.id[old]]] : sc->dt;
             const float4 d = tmp[old];
             if (apply == 1) {
                 u.x = d.x; u.y = d.y; u.z = d.z;
@@ -87,9 +88,9 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
 
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
                    const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
-                   uint32_t* list_fluid, uint32_t* list_solid) {
+                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch) {
     k_gather<<<blocks_for(cap, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc,
-                                                    list_fluid, list_solid);
+                                                    list_fluid, list_solid, batch);
 }
 
 // ---------------------------------------------------------------- update_dt
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(256) k_update_dt(const float4* __restrict__ ve
             const float dt = t < P.dt_max ? t : P.dt_max;
             if (dt < P.dt_min) atomicOr(&sc->err, ERR_DT_TOO_SMALL);
             sc->dt = dt;
+            body_force(P, sc->time, sc->g_eff);
             sc->vmax2_bits = 0;
             sc->done_blocks = 0;
             __threadfence();
@@ -128,16 +130,72 @@ __global__ void __launch_bounds__(256) k_update_dt(const float4* __restrict__ ve
     }
 }
 
-void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    k_update_dt<<<blocks_for(cap, 256), 256, 0, st>>>(a.cur.vel, a.P, a.sc);
+// The same per scene of a batch: each scene's dt from its own largest |u|^2
+// and constants, and its body force at its own time.
+__global__ void __launch_bounds__(256) k_update_dt_batch(const float4* __restrict__ vel, const uint32_t* __restrict__ id,
+                                                         BatchDev b, Scalars* __restrict__ sc) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float4 u = vel[i];
+        const float vv = dot3<true>(u.x, u.y, u.z, u.x, u.y, u.z);
+        const uint32_t s = b.sid_of_id[id[i]];
+        // lanes of the same scene (consecutive particles mostly share one)
+        // combine before one atomic
+        const uint32_t peers = __match_any_sync(__activemask(), s);
+        uint32_t m = 0;
+        if (vv == vv) m = __float_as_uint(vv);
+        else atomicOr(&sc->err, ERR_NAN);
+        uint32_t best = m;
+        for (uint32_t rest = peers; rest;) {
+            const int l = __ffs(rest) - 1;
+            rest &= rest - 1u;
+            best = max(best, __shfl_sync(peers, m, l));
+        }
+        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1) && best) atomicMax(b.vmax2_bits + s, best);
+    }
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (uint32_t s = threadIdx.x; s < b.n; s += blockDim.x) {
+        const Phys P = b.phys[s];
+        const float vmax = __uint_as_float(atomicAdd(b.vmax2_bits + s, 0u));
+        const float t = __double2float_rn((double)P.cfl_dp / sqrt((double)vmax));
+        const float dt = t < P.dt_max ? t : P.dt_max;
+        if (dt < P.dt_min) atomicOr(&sc->err, ERR_DT_TOO_SMALL);
+        b.dt[s] = dt;
+        float g[3];
+        body_force(P, b.time[s], g);
+        b.g_eff[s] = make_float4(g[0], g[1], g[2], 0.f);
+        b.vmax2_bits[s] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sc->dt = b.dt[0];
+        sc->done_blocks = 0;
+        __threadfence();
+    }
 }
 
-__global__ void k_step_end(Scalars* sc) {
+void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    if (a.batch.n) k_update_dt_batch<<<blocks_for(cap, 256), 256, 0, st>>>(a.cur.vel, a.cur.id, a.batch, a.sc);
+    else k_update_dt<<<blocks_for(cap, 256), 256, 0, st>>>(a.cur.vel, a.P, a.sc);
+}
+
+__global__ void k_step_end(Scalars* sc, BatchDev b) {
     sc->time = __fadd_rn(sc->time, sc->dt);
     sc->step += 1;
+    for (uint32_t s = 0; s < b.n; s++) b.time[s] = __fadd_rn(b.time[s], b.dt[s]);
+    if (b.n) sc->time = b.time[0];
 }
 
-void launch_step_end(Scalars* sc, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(sc); }
+void launch_step_end(Scalars* sc, const BatchDev& batch, cudaStream_t st) { k_step_end<<<1, 1, 0, st>>>(sc, batch); }
 
 // ---------------------------------------------------------------- warp per particle
 // One warp per particle; lane l takes candidate j = base + l of each row
@@ -193,12 +251,13 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     const float4 pi = pos[i];
     if (ptype(pi) != T_FLUID) return;
     const float4 ui = vel[i];
-    const float re = a.P.rlap, thr = a.P.rlap_thr;
+    const Local L = local_of(a, i);
+    const Phys P = phys_of(a, L.s);
+    const float re = P.rlap, thr = P.rlap_thr;
     float ax = 0.f, ay = 0.f, az = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -234,12 +293,19 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     }
     if (!ORD) { ax = warp_tree_add(ax); ay = warp_tree_add(ay); az = warp_tree_add(az); }
     if (lane != 0) return;
-    const float dt = a.sc->dt;
-    const float lx = fmul<EX>(a.P.c_lap, ax), ly = fmul<EX>(a.P.c_lap, ay), lz = fmul<EX>(a.P.c_lap, az);
+    const float dt = dt_of(a, L.s);
+    float gx, gy, gz;
+    if (a.batch.n) {
+        const float4 ge = a.batch.g_eff[L.s];
+        gx = ge.x; gy = ge.y; gz = ge.z;
+    } else {
+        gx = a.sc->g_eff[0]; gy = a.sc->g_eff[1]; gz = a.sc->g_eff[2];
+    }
+    const float lx = fmul<EX>(P.c_lap, ax), ly = fmul<EX>(P.c_lap, ay), lz = fmul<EX>(P.c_lap, az);
     float4 t;
-    t.x = fadd<EX>(ui.x, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lx), a.P.g[0])));
-    t.y = fadd<EX>(ui.y, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, ly), a.P.g[1])));
-    t.z = fadd<EX>(ui.z, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lz), a.P.g[2])));
+    t.x = fadd<EX>(ui.x, fmul<EX>(dt, fadd<EX>(fmul<EX>(P.niu, lx), gx)));
+    t.y = fadd<EX>(ui.y, fmul<EX>(dt, fadd<EX>(fmul<EX>(P.niu, ly), gy)));
+    t.z = fadd<EX>(ui.z, fmul<EX>(dt, fadd<EX>(fmul<EX>(P.niu, lz), gz)));
     t.w = 0.f;
     a.tmp[i] = t;
 }
@@ -256,10 +322,11 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     if (ptype(pi) != T_FLUID) return;
     const float4 ui = vel[i];
     float cx = 0.f, cy = 0.f, cz = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
+    const Local L = local_of(a, i);
+    const Phys P = phys_of(a, L.s);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -268,7 +335,7 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-                if (rr < a.P.col_thr) {
+                if (rr < P.col_thr) {
                     float ds, ood;
                     if (EX) { ds = __fsqrt_rn(rr); ood = __fdiv_rn(1.0f, ds); }
                     else { ood = rsqrtf(rr); ds = rr * ood; }
@@ -277,8 +344,8 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
                     const float hy = fmul<EX>(0.5f, fsub<EX>(uj.y, ui.y));
                     const float hz = fmul<EX>(0.5f, fsub<EX>(uj.z, ui.z));
                     const float vabs = fmul<EX>(dot3<EX>(hx, hy, hz, dx, dy, dz), ood);
-                    if (ds <= a.P.col_dis && vabs <= 0.f) {
-                        const float k = fmul<EX>(fmul<EX>(a.P.col_rate, vabs), ood);
+                    if (ds <= P.col_dis && vabs <= 0.f) {
+                        const float k = fmul<EX>(fmul<EX>(P.col_rate, vabs), ood);
                         tx = fmul<EX>(k, dx);
                         ty = fmul<EX>(k, dy);
                         tz = fmul<EX>(k, dz);
@@ -308,12 +375,13 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     const float4* __restrict__ pos = a.cur.pos;
     const float4 pi = pos[i];
     if (!all_types && ptype(pi) == T_DUMMY) return;
-    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    const Local L = local_of(a, i);
+    const Phys P = phys_of(a, L.s);
+    const float re = P.rzero, thr = P.rzero_thr;
     float acc = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float w = 0.f;
@@ -331,7 +399,7 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     if (lane != 0) return;
     a.cur.n[i] = acc;
     if (eos) {
-        const float t = fmul<EX>(fmul<EX>(a.P.one_over_alpha, fsub<EX>(acc, a.P.nzero)), a.P.one_over_nzero);
+        const float t = fmul<EX>(fmul<EX>(P.one_over_alpha, fsub<EX>(acc, P.nzero)), P.one_over_nzero);
         a.cur.press[i] = t > 0.f ? t : 0.f;
     }
 }
@@ -346,13 +414,14 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const float* __restrict__ press = a.cur.press;
     const float4 pi = pos[i];
     if (ptype(pi) != T_FLUID) return;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
-    const float r02 = a.P.rzero2;
+    const Local L = local_of(a, i);
+    const Phys P = phys_of(a, L.s);
+    const int rows = link_rows(L.g);
+    const float r02 = P.rzero2;
     // p_hat: a minimum, independent of order
     float hat = press[i];
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             if (j < rg.hi) {
@@ -370,11 +439,11 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, o));
-    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    const float re = P.rzero, thr = P.rzero_thr;
     const bool skip_dummy = a.semi != 0;
     float gx = 0.f, gy = 0.f, gz = 0.f;
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -412,57 +481,16 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     }
     if (!ORD) { gx = warp_tree_add(gx); gy = warp_tree_add(gy); gz = warp_tree_add(gz); }
     if (lane != 0) return;
-    const float cg = fmul<EX>(a.P.dim_f, a.P.one_over_nzero);
-    const float kk = fmul<EX>(-a.sc->dt, a.P.one_over_rho);
+    const float cg = fmul<EX>(P.dim_f, P.one_over_nzero);
+    const float kk = fmul<EX>(-dt_of(a, L.s), P.one_over_rho);
     a.tmp[i] = make_float4(fmul<EX>(kk, fmul<EX>(cg, gx)), fmul<EX>(kk, fmul<EX>(cg, gy)),
                            fmul<EX>(kk, fmul<EX>(cg, gz)), 0.f);
 }
 
-// ---------------------------------------------------------------- viscosity (thread per particle)
+// ---------------------------------------------------------------- viscosity
 // calVisc_expl + d3_LapVel (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:344-386,
 // MPS_GPU.cpp:683-717): for a fluid particle,
 //   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
-template <bool EX>
-__global__ void __launch_bounds__(256) k_visc(StageArgs a) {
-    const uint32_t n = a.sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    const float4* __restrict__ vel = a.cur.vel;
-    const float4 pi = pos[i];
-    if (ptype(pi) != T_FLUID) return;
-    const float4 ui = vel[i];
-    const float re = a.P.rlap, thr = a.P.rlap_thr;
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
-        for (uint32_t j = rg.lo; j < rg.hi; j++) {
-            const float4 pj = __ldg(pos + j);
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            if (rr < thr && j != i) {
-                const float w = weight_rr<EX>(re, rr);
-                if (w != 0.f) {
-                    const float4 uj = __ldg(vel + j);
-                    ax = fadd<EX>(ax, fmul<EX>(w, fsub<EX>(uj.x, ui.x)));
-                    ay = fadd<EX>(ay, fmul<EX>(w, fsub<EX>(uj.y, ui.y)));
-                    az = fadd<EX>(az, fmul<EX>(w, fsub<EX>(uj.z, ui.z)));
-                }
-            }
-        }
-    }
-    const float dt = a.sc->dt;
-    const float lx = fmul<EX>(a.P.c_lap, ax), ly = fmul<EX>(a.P.c_lap, ay), lz = fmul<EX>(a.P.c_lap, az);
-    float4 t;
-    t.x = fadd<EX>(ui.x, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lx), a.P.g[0])));
-    t.y = fadd<EX>(ui.y, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, ly), a.P.g[1])));
-    t.z = fadd<EX>(ui.z, fmul<EX>(dt, fadd<EX>(fmul<EX>(a.P.niu, lz), a.P.g[2])));
-    t.w = 0.f;
-    a.tmp[i] = t;
-}
-
 void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
     const bool ord = a.exact && !a.semi;
@@ -475,46 +503,6 @@ void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // MPS_GPU::collision (MPS_CAL_expl_v1.0/MPS_GPU.cpp:892-986): for a fluid
 // particle, over neighbours of any type with ds <= col_dis that approach
 // (vabs = (0.5 du).dr / ds <= 0): crt += col_rate * vabs / ds * dr.
-template <bool EX>
-__global__ void __launch_bounds__(256) k_collision(StageArgs a) {
-    const uint32_t n = a.sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    const float4* __restrict__ vel = a.cur.vel;
-    const float4 pi = pos[i];
-    if (ptype(pi) != T_FLUID) return;
-    const float4 ui = vel[i];
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
-        for (uint32_t j = rg.lo; j < rg.hi; j++) {
-            const float4 pj = __ldg(pos + j);
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            if (rr < a.P.col_thr && j != i) {
-                float ds, ood;
-                if (EX) { ds = __fsqrt_rn(rr); ood = __fdiv_rn(1.0f, ds); }
-                else { ood = rsqrtf(rr); ds = rr * ood; }
-                const float4 uj = __ldg(vel + j);
-                const float hx = fmul<EX>(0.5f, fsub<EX>(uj.x, ui.x));
-                const float hy = fmul<EX>(0.5f, fsub<EX>(uj.y, ui.y));
-                const float hz = fmul<EX>(0.5f, fsub<EX>(uj.z, ui.z));
-                const float vabs = fmul<EX>(dot3<EX>(hx, hy, hz, dx, dy, dz), ood);
-                if (ds <= a.P.col_dis && vabs <= 0.f) {
-                    const float k = fmul<EX>(fmul<EX>(a.P.col_rate, vabs), ood);
-                    cx = fadd<EX>(cx, fmul<EX>(k, dx));
-                    cy = fadd<EX>(cy, fmul<EX>(k, dy));
-                    cz = fadd<EX>(cz, fmul<EX>(k, dz));
-                }
-            }
-        }
-    }
-    a.tmp[i] = make_float4(cx, cy, cz, 0.f);
-}
-
 void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
     const bool ord = a.exact && !a.semi;
@@ -528,34 +516,6 @@ void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // for type != 2 (all types during initialisation, MPS.cpp:433-497), and the
 // equation of state of calPres_expl (MPS_GPU_EXPL.cpp:391-415):
 //   p = max(0, rho c^2 (n - n0) / n0).
-template <bool EX>
-__global__ void __launch_bounds__(256) k_pnd(StageArgs a, int eos, int all_types) {
-    const uint32_t n = a.sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    const float4 pi = pos[i];
-    if (!all_types && ptype(pi) == T_DUMMY) return;
-    const float re = a.P.rzero, thr = a.P.rzero_thr;
-    float acc = 0.f;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
-        for (uint32_t j = rg.lo; j < rg.hi; j++) {
-            const float4 pj = __ldg(pos + j);
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            if (rr < thr && j != i) acc = fadd<EX>(acc, weight_rr<EX>(re, rr));
-        }
-    }
-    a.cur.n[i] = acc;
-    if (eos) {
-        const float t = fmul<EX>(fmul<EX>(a.P.one_over_alpha, fsub<EX>(acc, a.P.nzero)), a.P.one_over_nzero);
-        a.cur.press[i] = t > 0.f ? t : 0.f;
-    }
-}
-
 void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
     const bool use_list = a.list_solid && !all_types;
     const uint32_t* list = use_list ? a.list_solid : nullptr;
@@ -590,58 +550,6 @@ void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const 
 // (itself included), grad = d/n0 * sum_{j != i} (p_j - p_hat)/r^2 w(r; r0) dr
 // over every type (semi-implicit: type 2 excluded, MPS_CAL_v4.0/MPS_CPU.cpp:384-445),
 // tmp = -dt/rho * grad.
-template <bool EX>
-__global__ void __launch_bounds__(256) k_dash(StageArgs a) {
-    const uint32_t n = a.sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    const float* __restrict__ press = a.cur.press;
-    const float4 pi = pos[i];
-    if (ptype(pi) != T_FLUID) return;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
-    float hat = press[i];
-    const float r02 = a.P.rzero2;
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
-        for (uint32_t j = rg.lo; j < rg.hi; j++) {
-            const float4 pj = __ldg(pos + j);
-            if (ptype(pj) == T_DUMMY) continue;
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            if (rr <= r02) {
-                const float pjv = __ldg(press + j);
-                if (pjv < hat) hat = pjv;
-            }
-        }
-    }
-    const float re = a.P.rzero, thr = a.P.rzero_thr;
-    const bool skip_dummy = a.semi != 0;
-    float gx = 0.f, gy = 0.f, gz = 0.f;
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
-        for (uint32_t j = rg.lo; j < rg.hi; j++) {
-            const float4 pj = __ldg(pos + j);
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            if (rr < thr && j != i && !(skip_dummy && ptype(pj) == T_DUMMY)) {
-                const float w = weight_rr<EX>(re, rr);
-                if (w != 0.f) {
-                    const float k = fmul<EX>(fdiv<EX>(fsub<EX>(__ldg(press + j), hat), rr), w);
-                    gx = fadd<EX>(gx, fmul<EX>(k, dx));
-                    gy = fadd<EX>(gy, fmul<EX>(k, dy));
-                    gz = fadd<EX>(gz, fmul<EX>(k, dz));
-                }
-            }
-        }
-    }
-    const float cg = fmul<EX>(a.P.dim_f, a.P.one_over_nzero);
-    const float kk = fmul<EX>(-a.sc->dt, a.P.one_over_rho);
-    a.tmp[i] = make_float4(fmul<EX>(kk, fmul<EX>(cg, gx)), fmul<EX>(kk, fmul<EX>(cg, gy)),
-                           fmul<EX>(kk, fmul<EX>(cg, gz)), 0.f);
-}
-
 void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st) {
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
     const bool ord = a.exact && !a.semi;
@@ -733,24 +641,42 @@ void launch_nzero(const float* n, Scalars* sc, unsigned long long* best, uint32_
     k_nzero<<<blocks_for(cap, 256), 256, 0, st>>>(n, sc, best);
 }
 
+__global__ void __launch_bounds__(256) k_nzero_range(const float* __restrict__ n, uint32_t lo, uint32_t hi,
+                                                     unsigned long long* best) {
+    const uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = 0ull;
+    if (i < hi) v = ((unsigned long long)__float_as_uint(n[i]) << 32) | (unsigned long long)(0xffffffffu - i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    if ((threadIdx.x & 31) == 0 && v) atomicMax(best, v);
+}
+
+void launch_nzero_range(const float* n, uint32_t lo, uint32_t hi, unsigned long long* best, cudaStream_t st) {
+    if (hi > lo) k_nzero_range<<<blocks_for(hi - lo, 256), 256, 0, st>>>(n, lo, hi, best);
+}
+
 // lambda (MPS_CAL_expl_v1.0/MPS.cpp:500-515): sum over i != t of
 // r^2 w(r; r0), r = |x_i - x_t|, in index order; only the linked cells of t
 // can hold non-zero terms and they are visited in ascending index order.
 __global__ void k_lambda(StageArgs a, const unsigned long long* best, float* out) {
     const uint32_t t = 0xffffffffu - (uint32_t)(*best & 0xffffffffull);
     const float4 pt = a.cur.pos[t];
-    const uint32_t c = a.cur.cell[t];
+    const Local L = local_of(a, t);
+    const Phys P = phys_of(a, L.s);
     float lam = 0.f;
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t j = rg.lo; j < rg.hi; j++) {
             if (j == t) continue;
             const float4 pj = a.cur.pos[j];
             const float dx = __fsub_rn(pj.x, pt.x), dy = __fsub_rn(pj.y, pt.y), dz = __fsub_rn(pj.z, pt.z);
             const float rr = dot3<true>(dx, dy, dz, dx, dy, dz);
             const float r = __fsqrt_rn(rr);
-            const float w = r < a.P.rzero ? __fsub_rn(__fdiv_rn(a.P.rzero, r), 1.0f) : 0.f;
+            const float w = r < P.rzero ? __fsub_rn(__fdiv_rn(P.rzero, r), 1.0f) : 0.f;
             lam = __fadd_rn(lam, __fmul_rn(__fmul_rn(r, r), w));
         }
     }
@@ -775,10 +701,12 @@ __global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_
         normal_id_of[idi] = idi;
         return;
     }
-    float dis = __fmul_rn(__fmul_rn(2.0f, a.P.rzero), a.P.rzero);
+    const Local L = local_of(a, i);
+    const Phys P = phys_of(a, L.s);
+    float dis = __fmul_rn(__fmul_rn(2.0f, P.rzero), P.rzero);
     uint32_t best = 0xffffffffu;
-    const uint32_t c = a.cur.cell[i];
-    const Grid& g = a.g;
+    const uint32_t c = L.c;
+    const Grid& g = L.g;
     const int nz = g.dim == 3 ? reach : 0;
     for (int dz = -nz; dz <= nz; dz++) {
         for (int dy = -reach; dy <= reach; dy++) {
@@ -792,7 +720,7 @@ __global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_
                 }
             }
             if (first == 0xffffffffu) continue;
-            const uint32_t lo = a.cell_start[first], hi = a.cell_start[last + 1];
+            const uint32_t lo = L.cs[first], hi = L.cs[last + 1];
             for (uint32_t j = lo; j < hi; j++) {
                 const float4 pj = a.cur.pos[j];
                 if (ptype(pj) != T_WALL) continue;

@@ -33,12 +33,42 @@ struct StageArgs {
     const uint32_t* list_solid = nullptr;  // fluid + wall (type != 2)
     const uint32_t* n_solid = nullptr;
     uint32_t cap_solid = 0;
+    BatchDev batch;            // scenes of a batch (n == 0: one scene, g and P)
 };
+
+// Scene-local view of particle i: its scene, its grid, its cell table (the
+// global table from the grid's first cell) and its cell in that grid.
+struct Local {
+    Grid g;
+    const uint32_t* cs;
+    uint32_t c;
+    uint32_t s;
+};
+
+__device__ __forceinline__ Local local_of(const StageArgs& a, uint32_t i) {
+    Local L;
+    const uint32_t cell = a.cur.cell[i];
+    if (a.batch.n) {
+        L.s = __ldg(a.batch.sid_of_id + a.cur.id[i]);
+        L.g = a.batch.grid[L.s];
+        L.cs = a.cell_start + L.g.base;
+        L.c = cell - L.g.base;
+    } else {
+        L.s = 0;
+        L.g = a.g;
+        L.cs = a.cell_start;
+        L.c = cell;
+    }
+    return L;
+}
+
+__device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) { return a.batch.n ? a.batch.phys[s] : a.P; }
+__device__ __forceinline__ float dt_of(const StageArgs& a, uint32_t s) { return a.batch.n ? a.batch.dt[s] : a.sc->dt; }
 
 // reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
                    const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
-                   uint32_t* list_fluid, uint32_t* list_solid);
+                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch);
 
 // update_dt: max |u|^2, then dt on the device
 void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st);
@@ -49,7 +79,7 @@ void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaSt
 void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const uint32_t* index_of_id, uint32_t cap,
                         cudaStream_t st);
 void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st);
-void launch_step_end(Scalars* sc, cudaStream_t st);
+void launch_step_end(Scalars* sc, const BatchDev& batch, cudaStream_t st);
 
 // host-layout staging (x y z per particle) <-> the float4 state
 struct Staging {
@@ -70,6 +100,8 @@ void launch_pack(const State& s, const Staging& in, int mask, const Scalars* sc,
 // initialisation
 // n0 and the particle it belongs to: max n with the lowest index on ties
 void launch_nzero(const float* n, Scalars* sc, unsigned long long* best, uint32_t cap, cudaStream_t st);
+// the same over the particle range [lo, hi) (one scene of a batch)
+void launch_nzero_range(const float* n, uint32_t lo, uint32_t hi, unsigned long long* best, cudaStream_t st);
 // lambda = sum over j of r^2 w(r0) around particle `best`, in index order
 void launch_lambda(const StageArgs& a, const unsigned long long* best, float* lambda_out, cudaStream_t st);
 // nearest type-1 particle (first in index order) within sqrt(2) r0 of each

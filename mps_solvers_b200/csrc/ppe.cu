@@ -141,6 +141,7 @@ struct AsmArgs {
     double* x64;
     unsigned* bar;
     double n0, lambda, beta, b_tmp, rho_lambda_alpha_n0, dim2;
+    const PpeScene* scenes;  // per scene of a batch (these constants otherwise)
 };
 
 // One warp per particle: scan the reference's 27 linked cells for rlap
@@ -158,7 +159,16 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const float* __restrict__ nn = a.cur.n;
     const float4 pi = pos[i];
     const double ni = (double)nn[i];
-    const bool dir_i = ptype(pi) == T_DUMMY || ni < A.beta * A.n0;
+    const Local L = local_of(a, i);
+    double n0 = A.n0, beta = A.beta, b_tmp = A.b_tmp, rlan0 = A.rho_lambda_alpha_n0;
+    if (a.batch.n) {
+        const PpeScene& ps = A.scenes[L.s];
+        n0 = ps.n0;
+        beta = ps.beta;
+        b_tmp = ps.b_tmp;
+        rlan0 = ps.rho_lambda_alpha_n0;
+    }
+    const bool dir_i = ptype(pi) == T_DUMMY || ni < beta * n0;
     if (dir_i) {
         if (lane == 0) {
             A.rlen[i] = PPE_DIRICHLET;
@@ -170,18 +180,18 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
         }
         return;
     }
-    const double dt = (double)a.sc->dt;
-    const double Aii = A.rho_lambda_alpha_n0 / (A.dim2 * dt * dt);
-    const float re = a.P.rlap, thr = a.P.rlap_thr;
-    const double bthr = A.beta * A.n0;
+    const double dt = (double)dt_of(a, L.s);
+    const double Aii = rlan0 / (A.dim2 * dt * dt);
+    const Phys P = phys_of(a, L.s);
+    const float re = P.rlap, thr = P.rlap_thr;
+    const double bthr = beta * n0;
     uint32_t* cols = A.cols + (size_t)i * PPE_W;
     uint32_t count = 0;
     double diag = 0.0;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     const uint32_t lt = (1u << lane) - 1u;
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             bool app = false;
@@ -217,7 +227,7 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
         A.diag64[i] = dg;
         A.diag32[i] = (float)dg;
         A.inv_diag[i] = (float)(1.0 / dg);
-        A.b64[i] = A.b_tmp * (A.n0 - ni);
+        A.b64[i] = b_tmp * (n0 - ni);
         A.x64[i] = (double)a.cur.press[i];
     }
 }
@@ -490,6 +500,332 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     }
 }
 
+// ---------------------------------------------------------------- batched solve
+// The scenes of a batch in one persistent launch.  Each scene runs its own
+// diagonally scaled PCG (its own alpha, beta, inner stop and FP64 true
+// residual) exactly as a single scene does; the scenes share the grid
+// barriers, and a scene that has met its inner target idles until the
+// others reach theirs (or the inner cap), then every unconverged scene takes
+// its next FP64 true-residual pass.  Per-scene sums are added in shared
+// memory (a warp whose rows share one scene adds once), written per block,
+// and the last block to arrive adds the blocks in order.
+struct BatchSolveArgs {
+    const uint32_t* rowlist;
+    const uint32_t* nrows;
+    const uint32_t* row_scene;
+    const uint32_t* off;
+    const uint32_t* scols;
+    const float4* pos;
+    const Phys* phys;
+    const double* b64;
+    const double* diag64;
+    const float* diag32;
+    const float* inv_diag;
+    double* x64;
+    float *r, *z, *q, *p0, *p1;
+    double* part;
+    double* result;
+    unsigned* bar;
+    Scalars* sc;
+    int* iters;
+    int* outers;
+    double* relres;
+    uint32_t ns;
+    double tol;
+    int max_iter, inner_cap, max_outer;
+};
+
+// add v[k] of every contributing lane to acc[k * ns + s] (whole warp calls)
+template <int K>
+__device__ __forceinline__ void scene_add(double* acc, uint32_t ns, uint32_t s, bool contrib, const double (&v)[K]) {
+    const uint32_t s0 = __shfl_sync(0xffffffffu, s, 0);
+    if (__all_sync(0xffffffffu, !contrib || s == s0)) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double t = warp_sum_d(contrib ? v[k] : 0.0);
+            if ((threadIdx.x & 31) == 0) atomicAdd(acc + k * ns + s0, t);
+        }
+    } else if (contrib) {
+#pragma unroll
+        for (int k = 0; k < K; k++) atomicAdd(acc + k * ns + s, v[k]);
+    }
+}
+
+// Grid-wide per-scene sums (acc: this block's K * ns sums in shared memory,
+// replaced by the totals) fused with a grid barrier; bounded wait as in
+// grid_reduce.
+template <int K>
+__device__ bool grid_reduce_scenes(double* acc, uint32_t ns, double* part, double* result, unsigned* bar, Scalars* sc) {
+    __syncthreads();
+    const uint32_t m = K * ns;
+    for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) part[(size_t)blockIdx.x * m + t] = acc[t];
+    __threadfence();
+    __shared__ int last, ok;
+    __shared__ unsigned gen0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned* gen = bar + 1;
+        gen0 = *gen;
+        __threadfence();
+        last = atomicAdd(bar, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) {
+            double v = 0.0;
+            for (uint32_t b = 0; b < gridDim.x; b++) v += __ldcg(part + (size_t)b * m + t);
+            result[t] = v;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        unsigned long long it = 0;
+        while (*gen == gen0) {
+            if (++it > (1ull << 24)) {
+                atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) acc[t] = __ldcg(result + t);
+    const bool good = ok != 0;
+    __syncthreads();
+    return good;
+}
+
+template <bool EX>
+__device__ __forceinline__ float batch_weight(const float4* __restrict__ pos, float rlap, float thr, const float4& pi,
+                                              uint32_t i, uint32_t j) {
+    const float4 pj = __ldg(pos + j);
+    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+    return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
+}
+
+template <bool EX>
+__global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs S) {
+    __shared__ double acc[3 * PPE_MAX_SCENES];
+    __shared__ double rz[PPE_MAX_SCENES], stop[PPE_MAX_SCENES], alpha[PPE_MAX_SCENES], rel[PPE_MAX_SCENES];
+    __shared__ float beta[PPE_MAX_SCENES];
+    __shared__ int its[PPE_MAX_SCENES], outs[PPE_MAX_SCENES];
+    __shared__ unsigned char active[PPE_MAX_SCENES], done[PPE_MAX_SCENES];
+    __shared__ int n_open, n_active;
+    const uint32_t ns = S.ns;
+    const uint32_t R = *S.nrows;
+    const uint32_t nslices = (R + SELL_C - 1) / SELL_C;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t rsub = lane & 7, q = lane >> 3;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t* __restrict__ rowlist = S.rowlist;
+    for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
+        done[s] = 0;
+        active[s] = 0;
+        its[s] = 0;
+        outs[s] = 0;
+        rel[s] = 0.0;
+    }
+    int total = 0;
+    float* pcur = S.p0;
+    float* pnew = S.p1;
+    for (int outer = 0; outer < S.max_outer; outer++) {
+        for (uint32_t t = threadIdx.x; t < 3 * ns; t += blockDim.x) acc[t] = 0.0;
+        __syncthreads();
+        // ---- FP64 true residual of the unconverged scenes' rows
+        for (uint32_t sl = gw; sl < nslices; sl += nw) {
+            const uint32_t k = sl * SELL_C + rsub;
+            const bool has = k < R;
+            const uint32_t ii = has ? __ldg(rowlist + k) : 0u;
+            const uint32_t s = has ? __ldg(S.row_scene + k) : 0u;
+            const bool work = has && !done[s];
+            if (!__any_sync(0xffffffffu, work)) continue;
+            const uint32_t base = __ldg(S.off + sl);
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
+            const uint32_t* cols = S.scols + base + lane;
+            const float4 pi = __ldg(S.pos + ii);
+            const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
+            double sum = 0.0;
+            if (work)
+                for (uint32_t t = 0; t < T; t++) {
+                    const uint32_t j = __ldg(cols + 32 * t);
+                    sum += (double)batch_weight<EX>(S.pos, rl, thr, pi, ii, j) * S.x64[j];
+                }
+            sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+            const bool contrib = q == 0 && work;
+            double v[3] = {0.0, 0.0, 0.0};
+            if (contrib) {
+                const double bi = S.b64[ii];
+                const double ri = bi - (S.diag64[ii] * S.x64[ii] + sum);
+                const float rf = (float)ri;
+                const float zf = rf * S.inv_diag[ii];
+                S.r[ii] = rf;
+                S.z[ii] = zf;
+                pcur[ii] = 0.f;
+                v[0] = ri * ri;
+                v[1] = bi * bi;
+                v[2] = (double)rf * (double)zf;
+            }
+            scene_add<3>(acc, ns, s, contrib, v);
+        }
+        if (!grid_reduce_scenes<3>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+        for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
+            if (done[s]) continue;
+            const double rr64 = acc[s], bb = acc[ns + s];
+            const double relres = bb > 0.0 ? sqrt(rr64 / bb) : 0.0;
+            rel[s] = relres;
+            outs[s]++;
+            if (relres <= S.tol) {
+                done[s] = 1;
+                active[s] = 0;
+            } else {
+                double eta = 0.3 * S.tol / relres;
+                if (eta < 1e-4) eta = 1e-4;
+                if (eta > 0.5) eta = 0.5;
+                active[s] = 1;
+                rz[s] = acc[2 * ns + s];
+                stop[s] = eta * eta * rr64;
+                beta[s] = 0.f;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int c = 0;
+            for (uint32_t s = 0; s < ns; s++) c += done[s] ? 0 : 1;
+            n_open = c;
+        }
+        __syncthreads();
+        if (n_open == 0 || total >= S.max_iter) break;
+        for (int it = 0; it < S.inner_cap && total < S.max_iter; it++) {
+            for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[t] = 0.0;
+            __syncthreads();
+            // ---- q = A p_new with p_new = z + beta p (fused), p.q per scene
+            for (uint32_t sl = gw; sl < nslices; sl += nw) {
+                const uint32_t k = sl * SELL_C + rsub;
+                const bool has = k < R;
+                const uint32_t ii = has ? __ldg(rowlist + k) : 0u;
+                const uint32_t s = has ? __ldg(S.row_scene + k) : 0u;
+                const bool work = has && active[s];
+                if (!__any_sync(0xffffffffu, work)) continue;
+                const uint32_t base = __ldg(S.off + sl);
+                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
+                const uint32_t* cols = S.scols + base + lane;
+                const float4 pi = __ldg(S.pos + ii);
+                const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
+                const float bs = beta[s];
+                float sum = 0.f;
+                if (work)
+                    for (uint32_t t = 0; t < T; t++) {
+                        const uint32_t j = __ldg(cols + 32 * t);
+                        sum = fmaf(batch_weight<EX>(S.pos, rl, thr, pi, ii, j), fmaf(bs, pcur[j], S.z[j]), sum);
+                    }
+                sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+                const bool contrib = q == 0 && work;
+                double v[1] = {0.0};
+                if (contrib) {
+                    const float pn = fmaf(bs, pcur[ii], S.z[ii]);
+                    const float qi = fmaf(S.diag32[ii], pn, sum);
+                    pnew[ii] = pn;
+                    S.q[ii] = qi;
+                    v[0] = (double)pn * (double)qi;
+                }
+                scene_add<1>(acc, ns, s, contrib, v);
+            }
+            if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+            for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x)
+                if (active[s]) alpha[s] = rz[s] / acc[s];
+            __syncthreads();
+            for (uint32_t t = threadIdx.x; t < 2 * ns; t += blockDim.x) acc[t] = 0.0;
+            __syncthreads();
+            // ---- x64 += alpha p, r -= alpha q, z = D^-1 r; r.z and r.r per scene
+            for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
+                const uint32_t kk = k0 + lane;
+                const bool has = kk < R;
+                const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
+                const bool contrib = has && active[s];
+                double v[2] = {0.0, 0.0};
+                if (contrib) {
+                    const uint32_t i = __ldg(rowlist + kk);
+                    const double al = alpha[s];
+                    const float pn = pnew[i];
+                    S.x64[i] += al * (double)pn;
+                    const float ri = fmaf(-(float)al, S.q[i], S.r[i]);
+                    const float zi = ri * S.inv_diag[i];
+                    S.r[i] = ri;
+                    S.z[i] = zi;
+                    v[0] = (double)ri * (double)zi;
+                    v[1] = (double)ri * (double)ri;
+                }
+                scene_add<2>(acc, ns, s, contrib, v);
+            }
+            if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+            for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
+                if (!active[s]) continue;
+                beta[s] = (float)(acc[s] / rz[s]);
+                rz[s] = acc[s];
+                its[s]++;
+                if (acc[ns + s] <= stop[s]) active[s] = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int c = 0;
+                for (uint32_t s = 0; s < ns; s++) c += active[s] ? 1 : 0;
+                n_active = c;
+            }
+            __syncthreads();
+            total++;
+            float* t = pcur;
+            pcur = pnew;
+            pnew = t;
+            if (n_active == 0) break;
+        }
+    }
+    if (blockIdx.x == 0) {
+        for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
+            S.iters[s] = its[s];
+            S.outers[s] = outs[s];
+            S.relres[s] = rel[s];
+            if (!done[s]) atomicOr(&S.sc->err, ERR_CG_NOT_CONVERGED);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int mi = 0, mo = 0;
+            double mr = 0.0;
+            for (uint32_t s = 0; s < ns; s++) {
+                mi = its[s] > mi ? its[s] : mi;
+                mo = outs[s] > mo ? outs[s] : mo;
+                mr = rel[s] > mr ? rel[s] : mr;
+            }
+            S.sc->cg_iters = mi;
+            S.sc->cg_outer = mo;
+            S.sc->cg_relres = mr;
+        }
+    }
+}
+
+// scene of every row (batch)
+__global__ void __launch_bounds__(256) k_row_scene(const uint32_t* __restrict__ rowlist, const uint32_t* __restrict__ nrows,
+                                                   const uint32_t* __restrict__ id, const uint32_t* __restrict__ sid_of_id,
+                                                   uint32_t* __restrict__ row_scene, uint32_t cap) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nrows || k >= cap) return;
+    row_scene[k] = sid_of_id[id[rowlist[k]]];
+}
+
 // ---------------------------------------------------------------- row list
 // Ordered list of the non-Dirichlet rows: the solver splits it into equal
 // contiguous slices per block (Dirichlet and dummy rows cluster in space, so
@@ -611,12 +947,12 @@ __global__ void __launch_bounds__(256) k_pnd64(StageArgs a, double* __restrict__
     if (i >= n) return;
     const float4* __restrict__ pos = a.cur.pos;
     const float4 pi = pos[i];
-    const double re = (double)a.P.rzero;
+    const Local L = local_of(a, i);
+    const double re = (double)phys_of(a, L.s).rzero;
     double acc = 0.0;
-    const uint32_t c = a.cur.cell[i];
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t j = rg.lo; j < rg.hi; j++) {
             if (j == i) continue;
             const float4 pj = __ldg(pos + j);
@@ -637,13 +973,14 @@ void launch_pnd64(const StageArgs& a, double* n64, uint32_t cap, cudaStream_t st
 // runs before the first sort, MPS_CAL_v4.0/MPS.cpp:316-333): the largest n64,
 // smallest id on ties; then lambda = sum r^2 w(r; r0) / n0 around it
 // (MPS.cpp:335-348).  One block.
-__global__ void __launch_bounds__(1024) k_n0_lambda64(StageArgs a, const double* __restrict__ n64, double* out) {
+__global__ void __launch_bounds__(1024) k_n0_lambda64(StageArgs a, const double* __restrict__ n64, double* out,
+                                                     uint32_t lo, uint32_t hi) {
     __shared__ double sn[1024];
     __shared__ uint32_t sid[1024], sidx[1024];
-    const uint32_t np = a.sc->np;
+    const uint32_t np = hi < a.sc->np ? hi : a.sc->np;
     double bn = -1.0;
     uint32_t bid = 0xffffffffu, bix = 0xffffffffu;
-    for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) {
+    for (uint32_t i = lo + threadIdx.x; i < np; i += blockDim.x) {
         const double v = n64[i];
         const uint32_t id = a.cur.id[i];
         if (v > bn || (v == bn && id < bid)) { bn = v; bid = id; bix = i; }
@@ -665,12 +1002,12 @@ __global__ void __launch_bounds__(1024) k_n0_lambda64(StageArgs a, const double*
     const double n0 = sn[0];
     if (t == 0xffffffffu || !(n0 > 0.0)) { out[0] = 0.0; out[1] = 0.0; return; }
     const float4 pt = a.cur.pos[t];
-    const double re = (double)a.P.rzero;
+    const Local L = local_of(a, t);
+    const double re = (double)phys_of(a, L.s).rzero;
     double lam = 0.0;
-    const uint32_t c = a.cur.cell[t];
-    const int rows = link_rows(a.g);
+    const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(a.g, a.cell_start, c, row);
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
         for (uint32_t j = rg.lo; j < rg.hi; j++) {
             if (j == t) continue;
             const float4 pj = a.cur.pos[j];
@@ -683,8 +1020,9 @@ __global__ void __launch_bounds__(1024) k_n0_lambda64(StageArgs a, const double*
     out[1] = lam / n0;
 }
 
-void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st) {
-    k_n0_lambda64<<<1, 1024, 0, st>>>(a, n64, out);
+void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st, uint32_t lo,
+                        uint32_t hi) {
+    k_n0_lambda64<<<1, 1024, 0, st>>>(a, n64, out, lo, hi);
 }
 
 // ---------------------------------------------------------------- host side
@@ -729,13 +1067,15 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     {
-        int o[4] = {0, 0, 0, 0};
+        int o[6] = {0, 0, 0, 0, 0, 0};
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], k_ppe_solve<true, 0>, PPE_THREADS, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], k_ppe_solve<false, 0>, PPE_THREADS, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], k_ppe_solve<true, 1>, PPE_THREADS, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], k_ppe_solve<false, 1>, PPE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[4], k_ppe_solve_batch<true>, PPE_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[5], k_ppe_solve_batch<false>, PPE_THREADS, 0);
         per_sm = o[0];
-        for (int q = 1; q < 4; q++) per_sm = o[q] < per_sm ? o[q] : per_sm;
+        for (int q = 1; q < 6; q++) per_sm = o[q] < per_sm ? o[q] : per_sm;
     }
     if (!coop || per_sm < 1) {
         *err = "device cannot run the cooperative PPE solver";
@@ -775,6 +1115,7 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     A.b_tmp = w.lambda64 * rho * (0.5 * (1.0 / dim) * one_over_dt * one_over_dt);
     A.rho_lambda_alpha_n0 = rho * w.lambda64 * alpha * w.n0_64;
     A.dim2 = 2.0 * dim;
+    A.scenes = w.scenes;
     const uint32_t warps_blocks = blocks_for(cap * 32u, 256);
     if (a.exact) k_ppe_assemble<true><<<warps_blocks, 256, 0, st>>>(A);
     else k_ppe_assemble<false><<<warps_blocks, 256, 0, st>>>(A);
@@ -782,6 +1123,12 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
     launch_scan_exclusive(w.tilecnt, ntiles, st);
     k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
+    int launched = 7;
+    if (a.batch.n) {
+        k_row_scene<<<blocks_for(cap, 256), 256, 0, st>>>(w.rowlist, w.nrows, a.cur.id, a.batch.sid_of_id, w.row_scene,
+                                                          cap);
+        launched++;
+    }
     // SELL-8 layout of the non-Dirichlet rows
     const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
     k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
@@ -793,7 +1140,6 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.id_snap, a.cur.id, (size_t)cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
     w.have_snapshot = true;
-    int launched = 7;
     if (w.lp.ready) {
         const LpSystem L = ppe_lp_system(w, a);
         lp_build_stencil(w.lp, L, cap, st);
@@ -863,6 +1209,43 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.max_iter = opt.cg_max_iter;
     S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
     S.max_outer = 40;
+    if (a.batch.n) {
+        BatchSolveArgs B;
+        B.rowlist = w.rowlist;
+        B.nrows = w.nrows;
+        B.row_scene = w.row_scene;
+        B.off = w.sell_off;
+        B.scols = w.sell_cols;
+        B.pos = a.cur.pos;
+        B.phys = a.batch.phys;
+        B.b64 = w.b64;
+        B.diag64 = w.diag64;
+        B.diag32 = w.diag32;
+        B.inv_diag = w.inv_diag;
+        B.x64 = w.x64;
+        B.r = w.r;
+        B.z = w.z;
+        B.q = w.q;
+        B.p0 = w.p[0];
+        B.p1 = w.p[1];
+        B.part = w.bpart;
+        B.result = w.bresult;
+        B.bar = w.bar;
+        B.sc = a.sc;
+        B.iters = w.scene_iters;
+        B.outers = w.scene_outer;
+        B.relres = w.scene_relres;
+        B.ns = w.nscenes;
+        B.tol = S.tol;
+        B.max_iter = S.max_iter;
+        B.inner_cap = S.inner_cap;
+        B.max_outer = S.max_outer;
+        void* bargs[] = {&B};
+        const void* bfn = a.exact ? (const void*)k_ppe_solve_batch<true> : (const void*)k_ppe_solve_batch<false>;
+        w.launch_err = cudaLaunchCooperativeKernel(bfn, w.blocks, PPE_THREADS, bargs, 0, st);
+        k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
+        return 2;
+    }
     void* args[] = {&S};
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
     const void* fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1> : (const void*)k_ppe_solve<true, 0>)
@@ -872,11 +1255,42 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     return 2;
 }
 
+int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaStream_t st, std::string* err) {
+    if (nscenes == 0 || nscenes > PPE_MAX_SCENES) {
+        *err = "a batch holds 1 to " + std::to_string(PPE_MAX_SCENES) + " scenes";
+        return MPS_ERR_INVALID;
+    }
+    w.nscenes = nscenes;
+    bool ok = true;
+    auto al = [&](void** p, size_t bytes) {
+        if (cudaMalloc(p, bytes + 64) != cudaSuccess) { ok = false; return; }
+        cudaMemsetAsync(*p, 0, bytes + 64, st);
+    };
+    al((void**)&w.scenes, nscenes * sizeof(PpeScene));
+    al((void**)&w.row_scene, (size_t)w.cap * sizeof(uint32_t));
+    al((void**)&w.bpart, (size_t)w.blocks * 3 * nscenes * sizeof(double));
+    al((void**)&w.bresult, 3 * nscenes * sizeof(double));
+    al((void**)&w.scene_iters, nscenes * sizeof(int));
+    al((void**)&w.scene_outer, nscenes * sizeof(int));
+    al((void**)&w.scene_relres, nscenes * sizeof(double));
+    if (!ok) {
+        *err = "cudaMalloc failed for the batch PPE tables";
+        return MPS_ERR_CUDA;
+    }
+    if (cudaMemcpyAsync(w.scenes, scenes, nscenes * sizeof(PpeScene), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        *err = "upload of the batch PPE constants failed";
+        return MPS_ERR_CUDA;
+    }
+    return MPS_OK;
+}
+
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar,
                   w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.y, w.ralt, w.pos_snap, w.n_snap,
-                  w.id_snap};
+                  w.id_snap, w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
+                  w.scene_relres};
     lp_free(w.lp);
     for (void* p : ps)
         if (p) cudaFree(p);

@@ -28,6 +28,12 @@ constexpr uint32_t PPE_DIRICHLET = 0xffffffffu;
 constexpr int PPE_THREADS = 1024;
 constexpr int PPE_PARTS = 4;           // FP64 partial sums per block
 constexpr uint32_t SELL_C = 8;         // rows per sliced-ELL slice
+constexpr uint32_t PPE_MAX_SCENES = 256;  // scenes of a batch the solver holds in shared memory
+
+// PPE constants of one scene of a batch (MPS_CAL_v4.0/MPS_CPU.cpp:619-650)
+struct PpeScene {
+    double n0, beta, b_tmp, rho_lambda_alpha_n0;
+};
 
 struct PpeWork {
     bool ready = false;
@@ -60,10 +66,21 @@ struct PpeWork {
     bool have_snapshot = false;
     double n0_64 = 0.0, lambda64 = 0.0, alpha64 = 0.0;
     cudaError_t launch_err = cudaSuccess;  // of the last cooperative launch
+    // batch: per-scene constants, scene of each row, per-scene results
+    uint32_t nscenes = 0;
+    PpeScene* scenes = nullptr;
+    uint32_t* row_scene = nullptr;
+    double* bpart = nullptr;           // blocks * 3 * nscenes
+    double* bresult = nullptr;         // 3 * nscenes
+    int* scene_iters = nullptr;
+    int* scene_outer = nullptr;
+    double* scene_relres = nullptr;
 };
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
               std::string* err);
+// the per-scene tables of a batch (after ppe_setup)
+int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaStream_t st, std::string* err);
 // assembly, row list and sliced-ELL layout (and, with the learned
 // preconditioner, its stencil and network forward); returns the kernels enqueued
 int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
@@ -77,7 +94,8 @@ void ppe_free(PpeWork& w);
 // FP64 particle number density of every particle (initialisation of the
 // semi-implicit method: n0 and lambda in double, MPS_CAL_v4.0/MPS.cpp:305-361)
 void launch_pnd64(const StageArgs& a, double* n64, uint32_t cap, cudaStream_t st);
-// out[0] = n0, out[1] = lambda (double)
-void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st);
+// out[0] = n0, out[1] = lambda (double), over the particles [lo, hi) (all: 0, ~0u)
+void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cudaStream_t st, uint32_t lo = 0,
+                        uint32_t hi = 0xffffffffu);
 
 }  // namespace mpsb

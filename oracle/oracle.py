@@ -53,6 +53,7 @@ def lib():
             getattr(L, f"orc_step_{s}").argtypes = [C.c_void_p]
             getattr(L, f"orc_step_{s}").restype = C.c_int
             getattr(L, f"orc_set_cg_{s}").argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+            getattr(L, f"orc_set_body_force_{s}").argtypes = [C.c_void_p, C.c_double, C.c_double]
             getattr(L, f"orc_counts_{s}").argtypes = [C.c_void_p] + [U] * 5
             getattr(L, f"orc_scalars_{s}").argtypes = [C.c_void_p, C.POINTER(C.c_double)]
             getattr(L, f"orc_get_state_{s}").argtypes = [C.c_void_p, U, U, P, P, P, P]
@@ -104,6 +105,12 @@ class Oracle:
 
     def set_cg(self, relative: bool, tol: float = 1e-8, max_iter: int = 0):
         self._f("set_cg")(self.h, int(relative), tol, max_iter)
+
+    def set_body_force(self, amp: float, freq: float):
+        """Tank acceleration amp*sin(2*pi*freq*t) along x (amp and freq are
+        taken as float32 values, as the GPU API takes them)."""
+        self._f("set_body_force")(self.h, C.c_double(float(np.float32(amp))),
+                                  C.c_double(float(np.float32(freq))))
 
     def step(self, n: int = 1) -> int:
         st = 0
