@@ -123,7 +123,26 @@ def make_scene(workload: str, seed: int, size: str = "full"):
     return scene.dam_break_semi(seed=seed)
 
 
+def write_batch(d: str, seed: int):
+    """The batched workload's 64 scenes as case directories under d;
+    returns (dirs, accel, particles per scene)."""
+    from mps_solvers_b200 import scene
+    dirs, accel, counts = [], [], []
+    for k, (sc, amp, freq) in enumerate(scene.batch_scenes(64, seed)):
+        sd = os.path.join(d, f"scene{k:02d}")
+        pos, _, _ = scene.write_case(sd, sc)
+        dirs.append(sd)
+        accel.append((amp, freq))
+        counts.append(len(pos))
+    return dirs, accel, counts
+
+
 def workload_name(workload: str) -> str:
+    if workload == "batch":
+        return ("batched semi-implicit dam breaks: 64 tanks at l0=0.01 m, fluid counts log-uniform "
+                "in [5k, 60k] (7,421,757 particles, 1,804,829 fluid), tank acceleration "
+                "A sin(2 pi f t) x with A in [0, 2] m/s^2, f in [0.5, 2] Hz, one launch per stage "
+                "and one persistent PPE launch for all scenes, each scene's PCG to 1e-8")
     if workload == "explicit":
         return ("explicit EOS dam break: 70,912 particles (8,000 fluid), l0=0.02 m, "
                 "r0=2.1 l0, rlap=4.0 l0, c0=20 m/s, dt=1e-4 s")
@@ -175,7 +194,13 @@ def run_reference_arm(args, rank: int, world: int):
         return None
     from mps_solvers_b200 import scene
     with tempfile.TemporaryDirectory() as d:
-        pos, nb2, nb1 = scene.write_case(d, make_scene(args.workload, 0))
+        if args.workload == "batch":
+            # the smallest scene of the batch stands for the batch (the CPU
+            # step cost is proportional to the particles)
+            sc = min(scene.batch_scenes(64, 0), key=lambda t: len(scene.build(t[0])[0]))[0]
+            pos, nb2, nb1 = scene.write_case(d, sc)
+        else:
+            pos, nb2, nb1 = scene.write_case(d, make_scene(args.workload, 0))
         n = len(pos)
         # each "step" of this arm is the bounded CPU sample
         sample = args.ref_sample if args.ref_sample else (100 if args.workload == "explicit" else 1)
@@ -191,7 +216,9 @@ def run_reference_arm(args, rank: int, world: int):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.workload == "explicit" else "f64",
-        "data": "synthetic", "config": {"workload": workload_name(args.workload), "particles": n},
+        "data": "synthetic", "config": {"workload": workload_name(args.workload), "particles": n,
+                                        "sample_scene": "smallest scene of the batch" if
+                                        args.workload == "batch" else None},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -205,21 +232,32 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    method = capi.METHOD_EXPLICIT if args.workload == "explicit" else capi.METHOD_SEMI_IMPLICIT
+    method = capi.METHOD_EXPLICIT if args.workload == "explicit" else capi.METHOD_SEMI_IMPLICIT  # batch: semi
     arith = capi.ARITH_EXACT if args.arith == "exact" else capi.ARITH_FAST
     tmpd = tempfile.mkdtemp(prefix=f"mpsb_{rank}_")
-    pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
-    n = len(pos0)
     precond = capi.PRECOND_LEARNED if args.precond == "learned" else capi.PRECOND_DIAGONAL
-    sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
-                          precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+    batch_counts = None
+    if args.workload == "batch":
+        dirs, accel, batch_counts = write_batch(tmpd, rank)
+        n = int(sum(batch_counts))
+        sim = capi.Simulation.batch(dirs, accel=accel, method=method, arith=arith, device=local_rank,
+                                    use_graph=1)
+        nb2 = sum(sim.scene_info(s).nb2 for s in range(len(dirs)))
+        nb1 = sum(sim.scene_info(s).nb1 for s in range(len(dirs)))
+    else:
+        pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
+        n = len(pos0)
+        sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
+                              precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
     if method == capi.METHOD_SEMI_IMPLICIT and precond == capi.PRECOND_LEARNED:
         from mps_solvers_b200 import precond_weights
         sim.set_precond_params(precond_weights.load())
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    # launch shapes picked by the library's autotuner on this scene, then
     # warm-up (also captures the step graphs)
+    tune = sim.autotune(2)
     for _ in range(args.warmup):
         sim.step_async(1)
     sim.step(0)
@@ -265,9 +303,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     scal = sim.scalars()
     launches = int(scal["launches_per_step"])
     prof_iters, prof_outer = int(scal["cg_iters"]), int(scal["cg_outer"])
+    # PPE work of the last solve: every scene's particles x its own iterations
+    if batch_counts is not None:
+        infos = [sim.scene_info(s) for s in range(len(batch_counts))]
+        ppe_work = sum(c * (60 * i.cg_iters + 40 * i.cg_outer) for c, i in zip(batch_counts, infos))
+        scene_iters = [i.cg_iters for i in infos]
+    else:
+        ppe_work = n * (60 * prof_iters + 40 * prof_outer)
+        scene_iters = None
     sim.close()
     compare = None
-    if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare:
+    if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare and batch_counts is None:
         compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)))
 
     # max over ranks
@@ -288,8 +334,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dom_ms = kern[dom] / prof_steps
     if dom == "ppe_solve":
         # fixed accounting model: 60 B per particle per CG iteration, 40 B per
-        # FP64 defect-correction pass (the last solve's counts)
-        alg_bytes = n * (60 * prof_iters + 40 * prof_outer)
+        # FP64 defect-correction pass (the last solve's counts, per scene)
+        alg_bytes = ppe_work
     else:
         alg_bytes = STAGE_BYTES[dom] * n
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
@@ -317,7 +363,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
+        "autotune": tune,
         "ppe_compare": compare,
+        "batch": None if scene_iters is None else {
+            "scenes": len(scene_iters), "particles_min": int(min(batch_counts)),
+            "particles_max": int(max(batch_counts)), "cg_iters_min": int(min(scene_iters)),
+            "cg_iters_max": int(max(scene_iters))},
         "final": {"np": stats.np, "step": stats.step, "time": stats.time, "dt": stats.dt,
                   "cg_iters": stats.cg_iters, "cg_outer": stats.cg_outer,
                   "cg_relres": stats.cg_relres},
@@ -376,9 +427,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="semi", choices=["explicit", "semi"],
+    ap.add_argument("--workload", default="semi", choices=["explicit", "semi", "batch"],
                     help="semi (default): the 310,912-particle semi-implicit dam break the "
-                         "metric is quoted on; explicit: the 70,912-particle EOS dam break")
+                         "metric is quoted on; explicit: the 70,912-particle EOS dam break; "
+                         "batch: 64 semi-implicit tanks of 5k-60k fluid particles with tank "
+                         "acceleration, stepped as one batch")
     ap.add_argument("--arith", default=None, choices=["exact", "fast"],
                     help="default: exact for the explicit workload (bit-identical to the "
                          "reference), fast for the semi-implicit one")
@@ -395,6 +448,8 @@ def main():
         args.warmup = 3
     if args.arith is None:
         args.arith = "exact" if args.workload == "explicit" else "fast"
+    if args.workload == "batch" and args.size != "full":
+        ap.error("the batch workload has one size")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -417,9 +472,15 @@ def main():
     if line is not None and world == 1 and not args.no_cpu_baseline:
         from mps_solvers_b200 import scene
         with tempfile.TemporaryDirectory() as d:
-            pos, _, _ = scene.write_case(d, make_scene(args.workload, 0))
+            if args.workload == "batch":
+                sc = min(scene.batch_scenes(64, 0), key=lambda t: len(scene.build(t[0])[0]))[0]
+            else:
+                sc = make_scene(args.workload, 0)
+            pos, _, _ = scene.write_case(d, sc)
             sample = 300 if args.workload == "explicit" else 2
             line["cpu_baseline"] = cpu_baseline(args.workload, d, len(pos), sample)
+            if args.workload == "batch":
+                line["cpu_baseline"]["sample"] += " (the batch's smallest scene)"
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

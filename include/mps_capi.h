@@ -174,7 +174,8 @@ mps_status mps_get_cell_tables(mps_handle* h, uint32_t* cell_of, uint32_t* start
 mps_status mps_get_grid(mps_handle* h, mps_grid* g);
 /* n0, lambda, dt, time, c_lap = 2d/(n0 lambda), rho c^2, alpha, cg iterations,
  * cg relative residual, step, status, number of cells, kernels launched by
- * one step, FP64 residual passes of the last PPE solve, and 2 spare slots. */
+ * one step, FP64 residual passes of the last PPE solve, 1 when steps replay
+ * a captured CUDA graph (0: direct launches), and 1 spare slot. */
 mps_status mps_get_scalars(mps_handle* h, double out16[16]);
 /* i_normal as GEO.dat indices: for each particle (by GEO index) the GEO index
  * of its wall particle (itself when it has none), np0 entries. */
@@ -301,6 +302,22 @@ mps_status mps_batch_step(mps_handle* h, int nsteps, mps_step_stats* stats);
 mps_status mps_batch_scene_info(mps_handle* h, uint32_t scene, mps_scene_info* info);
 /* Set the tank acceleration of a scene (scene 0 of a single-scene handle). */
 mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float accel_amp, float accel_freq);
+
+/* ---- autotuner ----
+ * No counterpart in the reference.  Times, on the handle's own scene with
+ * CUDA events over `steps` steps per candidate, the block size of the
+ * particle-stage kernels (64, 128, 256 threads) and the shape of the
+ * persistent PPE grid (1024, 512 or 256 threads per block at 1024 threads
+ * per SM; semi-implicit only), and keeps the fastest of each.  The scene
+ * advances by the steps taken (call it during warm-up). */
+typedef struct mps_tune_report {
+    int stage_threads;         /* chosen */
+    int ppe_threads;           /* chosen */
+    float stage_ms[3];         /* visc + collision + pnd + dash per step at 64, 128, 256 */
+    float ppe_ms_per_iter[3];  /* PPE solve ms per PCG iteration at 1024, 512, 256 (-1: not held) */
+    uint32_t reserved[4];
+} mps_tune_report;
+mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* report);
 
 #ifdef __cplusplus
 }

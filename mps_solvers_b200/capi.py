@@ -39,7 +39,8 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_profile_steps", "mps_stage_name", "mps_cell_sort_dev_noalloc",
            "mps_precond_num_params", "mps_precond_get_params", "mps_precond_set_params",
            "mps_precond_loss_grad", "mps_precond_train", "mps_ppe_snapshot",
-           "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force")
+           "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force",
+           "mps_autotune")
 
 
 class mps_options(C.Structure):
@@ -78,6 +79,11 @@ class mps_scene_info(C.Structure):
                 ("time", C.c_float), ("dt", C.c_float), ("nzero", C.c_float), ("pad", C.c_float),
                 ("cg_iters", C.c_int), ("cg_outer", C.c_int), ("cg_relres", C.c_double),
                 ("reserved", C.c_uint32 * 4)]
+
+
+class mps_tune_report(C.Structure):
+    _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("stage_ms", C.c_float * 3),
+                ("ppe_ms_per_iter", C.c_float * 3), ("reserved", C.c_uint32 * 4)]
 
 
 class MPSError(RuntimeError):
@@ -143,6 +149,7 @@ def lib():
             "mps_batch_step": (C.c_int, [H, C.c_int, C.POINTER(mps_step_stats)]),
             "mps_batch_scene_info": (C.c_int, [H, C.c_uint32, C.POINTER(mps_scene_info)]),
             "mps_set_body_force": (C.c_int, [H, C.c_uint32, C.c_float, C.c_float]),
+            "mps_autotune": (C.c_int, [H, C.c_int, C.POINTER(mps_tune_report)]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
@@ -322,7 +329,7 @@ class Simulation:
         o = (C.c_double * 16)()
         self._check(lib().mps_get_scalars(self.h, o))
         names = ("nzero", "lambda", "dt", "time", "c_lap", "one_over_alpha", "alpha", "cg_iters",
-                 "cg_relres", "step", "status", "ncells", "launches_per_step", "cg_outer")
+                 "cg_relres", "step", "status", "ncells", "launches_per_step", "cg_outer", "graph")
         return dict(zip(names, list(o)))
 
     def normal_ids(self) -> np.ndarray:
@@ -380,6 +387,13 @@ class Simulation:
         info = mps_scene_info()
         self._check(lib().mps_batch_scene_info(self.h, scene, C.byref(info)))
         return info
+
+    def autotune(self, steps: int = 3) -> Dict[str, object]:
+        """Pick the stage block size and the PPE grid shape by timing them."""
+        r = mps_tune_report()
+        self._check(lib().mps_autotune(self.h, steps, C.byref(r)))
+        return {"stage_threads": r.stage_threads, "ppe_threads": r.ppe_threads,
+                "stage_ms": list(r.stage_ms), "ppe_ms_per_iter": list(r.ppe_ms_per_iter)}
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -69,7 +69,12 @@ struct mps_handle {
     std::vector<Grid> scene_grid;
     std::vector<HostConst> scene_hc;
     Phys* phys_dev = nullptr;
+    bool graph_off = false;          // stream capture refused: direct launches
+    std::string graph_note;
+    int stage_threads = 256;         // block size of the particle-stage kernels (autotuned)
 };
+
+static void drop_graphs(mps_handle* h);
 
 // ---------------------------------------------------------------- helpers
 static const char* kStatusNames[] = {"ok",
@@ -128,6 +133,7 @@ static StageArgs stage_args(mps_handle* h) {
     a.n_solid = &h->sc->n_solid;
     a.cap_solid = h->cap_solid;
     a.batch = h->batch;
+    a.threads = h->stage_threads;
     return a;
 }
 
@@ -844,11 +850,7 @@ extern "C" mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float ac
     h->P.body_omega = omega;
     // the captured steps hold the old constants
     CK(cudaStreamSynchronize(h->stream));
-    for (int b = 0; b < 2; b++)
-        if (h->graph[b]) {
-            cudaGraphExecDestroy(h->graph[b]);
-            h->graph[b] = nullptr;
-        }
+    drop_graphs(h);
     return MPS_OK;
 }
 
@@ -897,14 +899,30 @@ static mps_status capture_graph(mps_handle* h, int parity) {
     return MPS_OK;
 }
 
+static void drop_graphs(mps_handle* h) {
+    for (int b = 0; b < 2; b++)
+        if (h->graph[b]) {
+            cudaGraphExecDestroy(h->graph[b]);
+            h->graph[b] = nullptr;
+        }
+}
+
 static mps_status step_async(mps_handle* h, int nsteps) {
     CK(cudaSetDevice(h->dev));
     for (int k = 0; k < nsteps; k++) {
-        if (h->opt.use_graph && h->opt.method == MPS_METHOD_EXPLICIT) {
+        if (h->opt.use_graph && !h->graph_off) {
             const int p = h->cur;
             if (!h->graph[p]) {
                 mps_status s = capture_graph(h, p);
-                if (s != MPS_OK) return s;
+                if (s != MPS_OK) {
+                    // a capture the driver refuses falls back to direct
+                    // launches; the reason stays readable
+                    cudaGetLastError();
+                    h->graph_off = true;
+                    h->graph_note = h->err;
+                    enqueue_step(h);
+                    continue;
+                }
             }
             CK(cudaGraphLaunch(h->graph[p], h->stream));
             h->cur ^= 1;
@@ -1096,6 +1114,7 @@ extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
     o[11] = h->g.ncells;
     o[12] = h->launches;
     o[13] = s.cg_outer;
+    o[14] = (h->opt.use_graph && !h->graph_off) ? 1.0 : 0.0;
     return MPS_OK;
 }
 
@@ -1134,10 +1153,12 @@ extern "C" mps_status mps_precond_set_params(mps_handle* h, const float* w, uint
     if (s != MPS_OK) return s;
     if (!w || n != (uint32_t)LP_NPARAM) return MPS_ERR_INVALID;
     CK(cudaSetDevice(h->dev));
+    const bool was_ready = h->ppe.lp.ready;
     int e = ppe_enable_learned(h->ppe, &h->err);
     if (e != MPS_OK) return (mps_status)e;
     lp_upload_params(h->ppe.lp, w, h->stream);
     CK(cudaStreamSynchronize(h->stream));
+    if (!was_ready) drop_graphs(h);  // the step now also runs the network
     return MPS_OK;
 }
 
@@ -1253,6 +1274,71 @@ extern "C" mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage
         }
     }
     return read_status(h, nullptr);
+}
+
+// Autotuner: the block size of the particle-stage kernels (64, 128, 256)
+// and the shape of the persistent PPE grid (1024, 512 or 256 threads per
+// block, 1024 threads per SM), each timed with CUDA events over `steps`
+// steps of the handle's own scene; the fastest is kept.  The scene advances
+// by the steps taken.
+extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* rep) {
+    if (!h || steps < 1) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    mps_tune_report r;
+    memset(&r, 0, sizeof r);
+    std::vector<double> ms(32);
+    int nst = 0;
+    const int stage_cand[3] = {64, 128, 256};
+    double best = 1e300;
+    int best_t = h->stage_threads;
+    for (int c = 0; c < 3; c++) {
+        h->stage_threads = stage_cand[c];
+        drop_graphs(h);
+        mps_status st = mps_profile_steps(h, steps, ms.data(), 32, &nst);
+        if (st != MPS_OK) return st;
+        const double t = (ms[ST_VISC] + ms[ST_COLLISION] + ms[ST_PND] + ms[ST_DASH]) / steps;
+        r.stage_ms[c] = (float)t;
+        if (t < best) {
+            best = t;
+            best_t = stage_cand[c];
+        }
+    }
+    h->stage_threads = best_t;
+    r.stage_threads = best_t;
+    r.ppe_threads = h->ppe.threads;
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        const int ppe_cand[3] = {1024, 512, 256};
+        best = 1e300;
+        int best_p = h->ppe.threads;
+        for (int c = 0; c < 3; c++) {
+            if (ppe_set_threads(h->ppe, ppe_cand[c]) != MPS_OK) {
+                r.ppe_ms_per_iter[c] = -1.f;  // the device cannot hold this shape
+                continue;
+            }
+            drop_graphs(h);
+            double tot = 0.0;
+            long iters = 0;
+            for (int k = 0; k < steps; k++) {
+                mps_status st = mps_profile_steps(h, 1, ms.data(), 32, &nst);
+                if (st != MPS_OK) return st;
+                Scalars sc;
+                if (read_status(h, &sc) == MPS_ERR_CUDA) return MPS_ERR_CUDA;
+                tot += ms[ST_PPE_SOLVE];
+                iters += sc.cg_iters > 0 ? sc.cg_iters : 1;
+            }
+            const double t = tot / (double)iters;
+            r.ppe_ms_per_iter[c] = (float)t;
+            if (t < best) {
+                best = t;
+                best_p = ppe_cand[c];
+            }
+        }
+        ppe_set_threads(h->ppe, best_p);
+        r.ppe_threads = best_p;
+    }
+    drop_graphs(h);
+    if (rep) *rep = r;
+    return MPS_OK;
 }
 
 extern "C" mps_status mps_get_normal_ids(mps_handle* h, uint32_t* normal_id) {

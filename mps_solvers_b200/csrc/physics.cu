@@ -240,7 +240,7 @@ __device__ __forceinline__ float warp_tree_add(float v) {
     return v;
 }
 
-template <bool EX, bool ORD>
+template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __restrict__ list,
                                                 const uint32_t* __restrict__ list_n) {
     const WarpTask tk = warp_task(a, list, list_n);
@@ -251,8 +251,8 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     const float4 pi = pos[i];
     if (ptype(pi) != T_FLUID) return;
     const float4 ui = vel[i];
-    const Local L = local_of(a, i);
-    const Phys P = phys_of(a, L.s);
+    const Local L = local_of<BT>(a, i);
+    const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rlap, thr = P.rlap_thr;
     float ax = 0.f, ay = 0.f, az = 0.f;
     const int rows = link_rows(L.g);
@@ -293,9 +293,9 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     }
     if (!ORD) { ax = warp_tree_add(ax); ay = warp_tree_add(ay); az = warp_tree_add(az); }
     if (lane != 0) return;
-    const float dt = dt_of(a, L.s);
+    const float dt = dt_of<BT>(a, L.s);
     float gx, gy, gz;
-    if (a.batch.n) {
+    if (BT) {
         const float4 ge = a.batch.g_eff[L.s];
         gx = ge.x; gy = ge.y; gz = ge.z;
     } else {
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     a.tmp[i] = t;
 }
 
-template <bool EX, bool ORD>
+template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t* __restrict__ list,
                                                      const uint32_t* __restrict__ list_n) {
     const WarpTask tk = warp_task(a, list, list_n);
@@ -322,8 +322,8 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     if (ptype(pi) != T_FLUID) return;
     const float4 ui = vel[i];
     float cx = 0.f, cy = 0.f, cz = 0.f;
-    const Local L = local_of(a, i);
-    const Phys P = phys_of(a, L.s);
+    const Local L = local_of<BT>(a, i);
+    const Phys P = phys_of<BT>(a, L.s);
     const int rows = link_rows(L.g);
     for (int row = 0; row < rows; row++) {
         const RowRange rg = link_row(L.g, L.cs, L.c, row);
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     if (lane == 0) a.tmp[i] = make_float4(cx, cy, cz, 0.f);
 }
 
-template <bool EX, bool ORD>
+template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_types, const uint32_t* __restrict__ list,
                                                const uint32_t* __restrict__ list_n) {
     const WarpTask tk = warp_task(a, list, list_n);
@@ -375,8 +375,8 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     const float4* __restrict__ pos = a.cur.pos;
     const float4 pi = pos[i];
     if (!all_types && ptype(pi) == T_DUMMY) return;
-    const Local L = local_of(a, i);
-    const Phys P = phys_of(a, L.s);
+    const Local L = local_of<BT>(a, i);
+    const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rzero, thr = P.rzero_thr;
     float acc = 0.f;
     const int rows = link_rows(L.g);
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     }
 }
 
-template <bool EX, bool ORD>
+template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __restrict__ list,
                                                 const uint32_t* __restrict__ list_n) {
     const WarpTask tk = warp_task(a, list, list_n);
@@ -414,8 +414,8 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const float* __restrict__ press = a.cur.press;
     const float4 pi = pos[i];
     if (ptype(pi) != T_FLUID) return;
-    const Local L = local_of(a, i);
-    const Phys P = phys_of(a, L.s);
+    const Local L = local_of<BT>(a, i);
+    const Phys P = phys_of<BT>(a, L.s);
     const int rows = link_rows(L.g);
     const float r02 = P.rzero2;
     // p_hat: a minimum, independent of order
@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     if (!ORD) { gx = warp_tree_add(gx); gy = warp_tree_add(gy); gz = warp_tree_add(gz); }
     if (lane != 0) return;
     const float cg = fmul<EX>(P.dim_f, P.one_over_nzero);
-    const float kk = fmul<EX>(-dt_of(a, L.s), P.one_over_rho);
+    const float kk = fmul<EX>(-dt_of<BT>(a, L.s), P.one_over_rho);
     a.tmp[i] = make_float4(fmul<EX>(kk, fmul<EX>(cg, gx)), fmul<EX>(kk, fmul<EX>(cg, gy)),
                            fmul<EX>(kk, fmul<EX>(cg, gz)), 0.f);
 }
@@ -492,11 +492,17 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
 // MPS_GPU.cpp:683-717): for a fluid particle,
 //   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
 void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
-    if (a.exact && ord) k_visc_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else if (a.exact) k_visc_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else k_visc_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    if (a.batch.n) {
+        if (a.exact && ord) k_visc_w<true, true, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_visc_w<true, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_visc_w<false, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    } else {
+        if (a.exact && ord) k_visc_w<true, true, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_visc_w<true, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_visc_w<false, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    }
 }
 
 // ---------------------------------------------------------------- collision
@@ -504,11 +510,17 @@ void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // particle, over neighbours of any type with ds <= col_dis that approach
 // (vabs = (0.5 du).dr / ds <= 0): crt += col_rate * vabs / ds * dr.
 void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
-    if (a.exact && ord) k_collision_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else if (a.exact) k_collision_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else k_collision_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    if (a.batch.n) {
+        if (a.exact && ord) k_collision_w<true, true, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_collision_w<true, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_collision_w<false, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    } else {
+        if (a.exact && ord) k_collision_w<true, true, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_collision_w<true, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_collision_w<false, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    }
 }
 
 // ---------------------------------------------------------------- PND (+EOS)
@@ -519,11 +531,17 @@ void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
     const bool use_list = a.list_solid && !all_types;
     const uint32_t* list = use_list ? a.list_solid : nullptr;
-    const uint32_t nb = blocks_for((use_list ? a.cap_solid : cap) * 32u, 256);
+    const uint32_t nb = blocks_for((use_list ? a.cap_solid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
-    if (a.exact && ord) k_pnd_w<true, true><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
-    else if (a.exact) k_pnd_w<true, false><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
-    else k_pnd_w<false, false><<<nb, 256, 0, st>>>(a, eos, all_types, list, a.n_solid);
+    if (a.batch.n) {
+        if (a.exact && ord) k_pnd_w<true, true, true><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+        else if (a.exact) k_pnd_w<true, false, true><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+        else k_pnd_w<false, false, true><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+    } else {
+        if (a.exact && ord) k_pnd_w<true, true, false><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+        else if (a.exact) k_pnd_w<true, false, false><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+        else k_pnd_w<false, false, false><<<nb, a.threads, 0, st>>>(a, eos, all_types, list, a.n_solid);
+    }
 }
 
 // calPres_expl second loop (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:417-426): a
@@ -551,11 +569,17 @@ void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const 
 // over every type (semi-implicit: type 2 excluded, MPS_CAL_v4.0/MPS_CPU.cpp:384-445),
 // tmp = -dt/rho * grad.
 void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, 256);
+    const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
-    if (a.exact && ord) k_dash_w<true, true><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else if (a.exact) k_dash_w<true, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
-    else k_dash_w<false, false><<<nb, 256, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    if (a.batch.n) {
+        if (a.exact && ord) k_dash_w<true, true, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_dash_w<true, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_dash_w<false, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    } else {
+        if (a.exact && ord) k_dash_w<true, true, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.exact) k_dash_w<true, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else k_dash_w<false, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+    }
 }
 
 // ---------------------------------------------------------------- staging

@@ -34,6 +34,7 @@ struct StageArgs {
     const uint32_t* n_solid = nullptr;
     uint32_t cap_solid = 0;
     BatchDev batch;            // scenes of a batch (n == 0: one scene, g and P)
+    int threads = 256;         // block size of the particle-stage kernels (autotuned: 64, 128, 256)
 };
 
 // Scene-local view of particle i: its scene, its grid, its cell table (the
@@ -45,10 +46,13 @@ struct Local {
     uint32_t s;
 };
 
+// BT: the launch belongs to a batch (a.batch.n > 0), decided on the host so
+// that a single scene's kernels carry no batch code.
+template <bool BT>
 __device__ __forceinline__ Local local_of(const StageArgs& a, uint32_t i) {
     Local L;
     const uint32_t cell = a.cur.cell[i];
-    if (a.batch.n) {
+    if (BT) {
         L.s = __ldg(a.batch.sid_of_id + a.cur.id[i]);
         L.g = a.batch.grid[L.s];
         L.cs = a.cell_start + L.g.base;
@@ -62,8 +66,23 @@ __device__ __forceinline__ Local local_of(const StageArgs& a, uint32_t i) {
     return L;
 }
 
-__device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) { return a.batch.n ? a.batch.phys[s] : a.P; }
-__device__ __forceinline__ float dt_of(const StageArgs& a, uint32_t s) { return a.batch.n ? a.batch.dt[s] : a.sc->dt; }
+template <bool BT>
+__device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) {
+    if (BT) return a.batch.phys[s];
+    return a.P;
+}
+template <bool BT>
+__device__ __forceinline__ float dt_of(const StageArgs& a, uint32_t s) {
+    return BT ? a.batch.dt[s] : a.sc->dt;
+}
+
+// the same, decided per launch on the device (set-up kernels)
+__device__ __forceinline__ Local local_of(const StageArgs& a, uint32_t i) {
+    return a.batch.n ? local_of<true>(a, i) : local_of<false>(a, i);
+}
+__device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) {
+    return a.batch.n ? phys_of<true>(a, s) : phys_of<false>(a, s);
+}
 
 // reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,

@@ -147,7 +147,7 @@ struct AsmArgs {
 // One warp per particle: scan the reference's 27 linked cells for rlap
 // neighbours of type != 2, accumulate the diagonal, append the non-Dirichlet
 // ones in ascending index order (MPS_CAL_v4.0/MPS_CPU.cpp:651-698).
-template <bool EX>
+template <bool EX, bool BT>
 __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const StageArgs& a = A.a;
     const uint32_t n = a.sc->np;
@@ -159,9 +159,9 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const float* __restrict__ nn = a.cur.n;
     const float4 pi = pos[i];
     const double ni = (double)nn[i];
-    const Local L = local_of(a, i);
+    const Local L = local_of<BT>(a, i);
     double n0 = A.n0, beta = A.beta, b_tmp = A.b_tmp, rlan0 = A.rho_lambda_alpha_n0;
-    if (a.batch.n) {
+    if (BT) {
         const PpeScene& ps = A.scenes[L.s];
         n0 = ps.n0;
         beta = ps.beta;
@@ -180,9 +180,9 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
         }
         return;
     }
-    const double dt = (double)dt_of(a, L.s);
+    const double dt = (double)dt_of<BT>(a, L.s);
     const double Aii = rlan0 / (A.dim2 * dt * dt);
-    const Phys P = phys_of(a, L.s);
+    const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rlap, thr = P.rlap_thr;
     const double bthr = beta * n0;
     uint32_t* cols = A.cols + (size_t)i * PPE_W;
@@ -1082,8 +1082,11 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
         return MPS_ERR_CUDA;
     }
     if (per_sm > 1) per_sm = 1;
+    w.sms = sms;
+    w.threads = PPE_THREADS;
     w.blocks = sms * per_sm;
-    ok &= al((void**)&w.part, (size_t)w.blocks * PPE_PARTS * sizeof(double));
+    // partials sized for the smallest block shape (4 blocks per SM)
+    ok &= al((void**)&w.part, (size_t)sms * 4 * PPE_PARTS * sizeof(double));
     ok &= al((void**)&w.result, PPE_PARTS * sizeof(double));
     ok &= al((void**)&w.bar, 2 * sizeof(unsigned));
     if (!ok) {
@@ -1092,6 +1095,22 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     }
     w.ready = true;
     return MPS_OK;
+}
+
+// A cooperative launch through the launch-attribute form, which stream
+// capture records as a cooperative graph kernel node.
+static cudaError_t launch_cooperative(const void* fn, int blocks, int threads, void** args, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
@@ -1117,8 +1136,13 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     A.dim2 = 2.0 * dim;
     A.scenes = w.scenes;
     const uint32_t warps_blocks = blocks_for(cap * 32u, 256);
-    if (a.exact) k_ppe_assemble<true><<<warps_blocks, 256, 0, st>>>(A);
-    else k_ppe_assemble<false><<<warps_blocks, 256, 0, st>>>(A);
+    if (a.batch.n) {
+        if (a.exact) k_ppe_assemble<true, true><<<warps_blocks, 256, 0, st>>>(A);
+        else k_ppe_assemble<false, true><<<warps_blocks, 256, 0, st>>>(A);
+    } else {
+        if (a.exact) k_ppe_assemble<true, false><<<warps_blocks, 256, 0, st>>>(A);
+        else k_ppe_assemble<false, false><<<warps_blocks, 256, 0, st>>>(A);
+    }
     const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
     k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
     launch_scan_exclusive(w.tilecnt, ntiles, st);
@@ -1242,7 +1266,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.max_outer = S.max_outer;
         void* bargs[] = {&B};
         const void* bfn = a.exact ? (const void*)k_ppe_solve_batch<true> : (const void*)k_ppe_solve_batch<false>;
-        w.launch_err = cudaLaunchCooperativeKernel(bfn, w.blocks, PPE_THREADS, bargs, 0, st);
+        w.launch_err = launch_cooperative(bfn, w.blocks, w.threads, bargs, st);
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
@@ -1250,9 +1274,25 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
     const void* fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1> : (const void*)k_ppe_solve<true, 0>)
                              : (learned ? (const void*)k_ppe_solve<false, 1> : (const void*)k_ppe_solve<false, 0>);
-    w.launch_err = cudaLaunchCooperativeKernel(fn, w.blocks, PPE_THREADS, args, 0, st);
+    w.launch_err = launch_cooperative(fn, w.blocks, w.threads, args, st);
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
     return 2;
+}
+
+int ppe_set_threads(PpeWork& w, int threads) {
+    if (threads != 256 && threads != 512 && threads != 1024) return MPS_ERR_INVALID;
+    const int per_sm = PPE_THREADS / threads;
+    const void* fns[] = {(const void*)k_ppe_solve<true, 0>, (const void*)k_ppe_solve<false, 0>,
+                         (const void*)k_ppe_solve<true, 1>, (const void*)k_ppe_solve<false, 1>,
+                         (const void*)k_ppe_solve_batch<true>, (const void*)k_ppe_solve_batch<false>};
+    for (const void* f : fns) {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, threads, 0) != cudaSuccess || o < per_sm)
+            return MPS_ERR_INVALID;
+    }
+    w.threads = threads;
+    w.blocks = w.sms * per_sm;
+    return MPS_OK;
 }
 
 int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaStream_t st, std::string* err) {
@@ -1268,7 +1308,7 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
     };
     al((void**)&w.scenes, nscenes * sizeof(PpeScene));
     al((void**)&w.row_scene, (size_t)w.cap * sizeof(uint32_t));
-    al((void**)&w.bpart, (size_t)w.blocks * 3 * nscenes * sizeof(double));
+    al((void**)&w.bpart, (size_t)w.sms * 4 * 3 * nscenes * sizeof(double));
     al((void**)&w.bresult, 3 * nscenes * sizeof(double));
     al((void**)&w.scene_iters, nscenes * sizeof(int));
     al((void**)&w.scene_outer, nscenes * sizeof(int));

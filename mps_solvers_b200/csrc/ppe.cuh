@@ -39,6 +39,8 @@ struct PpeWork {
     bool ready = false;
     uint32_t cap = 0;
     int blocks = 0;                    // co-resident blocks of the persistent solver
+    int threads = PPE_THREADS;         // its block size (1024 / threads blocks per SM)
+    int sms = 0;
     uint32_t* cols = nullptr;          // cap * PPE_W
     uint32_t* rlen = nullptr;          // off-diagonal count, PPE_DIRICHLET for Dirichlet rows
     double* diag64 = nullptr;
@@ -90,6 +92,9 @@ int ppe_enable_learned(PpeWork& w, std::string* err);
 // the persistent solve and p = max(x, 0); returns the kernels enqueued
 int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);
+// the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
+// either way); MPS_ERR_INVALID when the device cannot hold that shape
+int ppe_set_threads(PpeWork& w, int threads);
 
 // FP64 particle number density of every particle (initialisation of the
 // semi-implicit method: n0 and lambda in double, MPS_CAL_v4.0/MPS.cpp:305-361)

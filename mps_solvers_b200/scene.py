@@ -232,6 +232,29 @@ def dam_break_semi(seed: int = 0, steps: int = 1000) -> Scene:
                  params=p)
 
 
+def batch_scenes(n: int = 64, seed: int = 0):
+    """Batched workload: n dam-break tanks at l0 = 0.01 m whose fluid counts
+    are log-uniform in [5,000, 60,000].  Per tank (from a generator seeded by
+    `seed`): fluid depth 10-20 sites, column height/width 1-2, tank interior
+    3x the column width, the column's depth, 1.2x its height plus 2 sites;
+    tank acceleration amplitude uniform in [0, 2] m/s^2 and frequency in
+    [0.5, 2] Hz.  Returns [(Scene, accel_amp, accel_freq)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nf = float(np.exp(rng.uniform(np.log(5000.0), np.log(60000.0))))
+        ny = int(rng.integers(10, 21))
+        aspect = float(rng.uniform(1.0, 2.0))
+        nx = max(4, int(round(np.sqrt(nf / (ny * aspect)))))
+        nz = max(4, int(round(nf / (ny * nx))))
+        interior = (3 * nx, ny, int(np.ceil(1.2 * nz)) + 2)
+        p = Params(dim=3, dp=0.01, r0=2.1, rlap=4.0, cs=20.0, dt_max=5e-4, tt=1.0, max_dis=0.01)
+        sc = Scene(l0=0.01, interior=interior, fluid=[Box(0, 0, 0, nx, ny, nz)], seed=seed * 1000 + k,
+                   params=p)
+        out.append((sc, float(rng.uniform(0.0, 2.0)), float(rng.uniform(0.5, 2.0))))
+    return out
+
+
 def small_tank(seed: int = 0, interior=(14, 6, 12), fluid=(5, 4, 8), l0: float = 0.02,
                rlap: float = 4.0, dt: float = 1e-4, cs: float = 20.0) -> Scene:
     """A few-thousand-particle tank for parity tests."""

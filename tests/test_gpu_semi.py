@@ -105,3 +105,18 @@ def test_full_size_semi_dam_break(capi, oracle_mod, tmp_path):
             assert st.cg_relres <= 1e-8 and st.status == 0
         a = s.state()
         assert np.isfinite(a["press"]).all() and a["press"].min() >= 0.0
+
+
+def test_semi_graph_replay_equals_direct_launches(capi, tmp_path):
+    """The semi-implicit step (with its cooperative PPE launch) replays as a
+    captured CUDA graph, with the same results as direct launches."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    out = []
+    for use_graph in (1, 0):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, use_graph=use_graph) as s:
+            s.step(6)
+            assert s.scalars()["graph"] == use_graph
+            out.append(s.state())
+    for f in ("pos", "vel", "press"):
+        assert np.array_equal(out[0][f], out[1][f]), f
