@@ -120,7 +120,13 @@ def make_scene(workload: str, seed: int, size: str = "full"):
         return sc
     if workload == "explicit":
         return scene.dam_break_explicit(seed=seed)
+    if workload == "large":
+        return scene.large_obstacle(seed=seed)
     return scene.dam_break_semi(seed=seed)
+
+
+SURFACE_SHAPE = (256, 64, 128)   # vertices along x (length), y (depth), z (height)
+SURFACE_EVERY = 20
 
 
 def write_batch(d: str, seed: int):
@@ -138,6 +144,11 @@ def write_batch(d: str, seed: int):
 
 
 def workload_name(workload: str) -> str:
+    if workload == "large":
+        return ("semi-implicit dam break with a box obstacle: 2,004,000 fluid particles, l0=0.005 m, "
+                "2.4 x 0.6 x 1.2 m tank, 0.15 x 0.15 x 0.3 m obstacle at x=1.0 m, dt=2.5e-4 s, PPE "
+                "diagonally scaled CG to 1e-8, marching-cubes surface on a 256 x 64 x 128 vertex "
+                "grid every 20 steps inside the timed region")
     if workload == "batch":
         return ("batched semi-implicit dam breaks: 64 tanks at l0=0.01 m, fluid counts log-uniform "
                 "in [5k, 60k] (7,421,757 particles, 1,804,829 fluid), tank acceleration "
@@ -255,6 +266,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    surface = None
+    if args.workload == "large":
+        sc_large = make_scene("large", rank)
+        origin, spacing = scene.surface_grid(sc_large, SURFACE_SHAPE)
+        sim.surface_setup(SURFACE_SHAPE, origin, spacing, 8 << 20)
+        surface = {"grid": list(SURFACE_SHAPE), "every": SURFACE_EVERY}
     # launch shapes picked by the library's autotuner on this scene, then
     # warm-up (also captures the step graphs)
     tune = sim.autotune(2)
@@ -275,12 +292,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 flush.fill_(float(k))  # write > L2 between timed steps
                 ev[k][0].record(stream)
                 sim.step_async(1)
+                if surface is not None and (k + 1) % SURFACE_EVERY == 0:
+                    sim.surface_extract(wait=False)
                 ev[k][1].record(stream)
         stream.synchronize()
     stats = sim.step(0)
     torch.cuda.synchronize(dev)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     clocks = clk.summary()
+    if surface is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            sim.surface_extract(wait=False)
+            e1.record(stream)
+        stream.synchronize()
+        surface["ms_per_extraction"] = e0.elapsed_time(e1)
+        surface["triangles"] = sim.surface_extract()
+        surface["extractions_timed"] = args.steps // SURFACE_EVERY
 
     # e2e: host buffers through the C ABI
     pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
@@ -364,6 +393,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "autotune": tune,
+        "surface": surface,
         "ppe_compare": compare,
         "batch": None if scene_iters is None else {
             "scenes": len(scene_iters), "particles_min": int(min(batch_counts)),
@@ -427,11 +457,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="semi", choices=["explicit", "semi", "batch"],
+    ap.add_argument("--workload", default="semi", choices=["explicit", "semi", "batch", "large"],
                     help="semi (default): the 310,912-particle semi-implicit dam break the "
                          "metric is quoted on; explicit: the 70,912-particle EOS dam break; "
                          "batch: 64 semi-implicit tanks of 5k-60k fluid particles with tank "
-                         "acceleration, stepped as one batch")
+                         "acceleration, stepped as one batch; large: the 3.7M-particle obstacle "
+                         "scene (2M fluid) with a marching-cubes surface every 20 steps")
     ap.add_argument("--arith", default=None, choices=["exact", "fast"],
                     help="default: exact for the explicit workload (bit-identical to the "
                          "reference), fast for the semi-implicit one")
@@ -477,7 +508,7 @@ def main():
             else:
                 sc = make_scene(args.workload, 0)
             pos, _, _ = scene.write_case(d, sc)
-            sample = 300 if args.workload == "explicit" else 2
+            sample = 300 if args.workload == "explicit" else (1 if args.workload == "large" else 2)
             line["cpu_baseline"] = cpu_baseline(args.workload, d, len(pos), sample)
             if args.workload == "batch":
                 line["cpu_baseline"]["sample"] += " (the batch's smallest scene)"

@@ -303,6 +303,37 @@ mps_status mps_batch_scene_info(mps_handle* h, uint32_t scene, mps_scene_info* i
 /* Set the tank acceleration of a scene (scene 0 of a single-scene handle). */
 mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float accel_amp, float accel_freq);
 
+/* ---- free surface by marching cubes ----
+ * The reference's iso-surface (MPS_CAL_expl_gl_v3.1: MPS_GPU::calVertex_n,
+ * calTriangle, calNorm) as a headless triangle buffer.  Vertex value n_v =
+ * sum over fluid particles of the cubic spline w(|x_j - v|; r0); iso = 0.8 x
+ * the largest particle sum of w over its neighbours, taken at
+ * mps_surface_setup (call it on the initial state to match the reference).
+ * Triangles: 9 floats each (three vertices), normals likewise (the
+ * normalised -grad n), counter-clockwise seen from the low-n side.
+ * Single-scene handles only. */
+typedef struct mps_surface_grid {
+    uint32_t nx, ny, nz, pad;  /* vertices per axis */
+    float origin[3];           /* first vertex */
+    float spacing[3];
+    uint32_t reserved[4];
+} mps_surface_grid;
+mps_status mps_surface_setup(mps_handle* h, const mps_surface_grid* grid, uint32_t max_triangles);
+/* extract on the handle's stream (asynchronous) */
+mps_status mps_surface_extract_async(mps_handle* h);
+/* extract and wait; ntri = triangles found; MPS_ERR_CAPACITY when they
+ * exceed max_triangles (the buffer then holds the first max_triangles) */
+mps_status mps_surface_extract(mps_handle* h, uint32_t* ntri);
+mps_status mps_surface_get(mps_handle* h, float* pos9, float* nrm9, uint32_t max_triangles, uint32_t* ntri);
+/* vertex values (nx*ny*nz, x fastest) and the iso level */
+mps_status mps_surface_vertex_values(mps_handle* h, float* values, float* iso);
+/* the last extracted surface as a binary STL file */
+mps_status mps_surface_write_stl(mps_handle* h, const char* path);
+/* The marching-cubes case table the library generates (host only):
+ * ntri[case] triangles, tri[16 * case + 3 * t + k] = cube edge of vertex k of
+ * triangle t; bit k of case = corner k inside. */
+mps_status mps_surface_case_table(uint8_t ntri[256], int8_t tri[256 * 16]);
+
 /* ---- autotuner ----
  * No counterpart in the reference.  Times, on the handle's own scene with
  * CUDA events over `steps` steps per candidate, the block size of the

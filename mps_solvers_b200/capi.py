@@ -40,7 +40,9 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_precond_num_params", "mps_precond_get_params", "mps_precond_set_params",
            "mps_precond_loss_grad", "mps_precond_train", "mps_ppe_snapshot",
            "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force",
-           "mps_autotune")
+           "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
+           "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
+           "mps_surface_case_table")
 
 
 class mps_options(C.Structure):
@@ -84,6 +86,11 @@ class mps_scene_info(C.Structure):
 class mps_tune_report(C.Structure):
     _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("stage_ms", C.c_float * 3),
                 ("ppe_ms_per_iter", C.c_float * 3), ("reserved", C.c_uint32 * 4)]
+
+
+class mps_surface_grid(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32), ("pad", C.c_uint32),
+                ("origin", C.c_float * 3), ("spacing", C.c_float * 3), ("reserved", C.c_uint32 * 4)]
 
 
 class MPSError(RuntimeError):
@@ -150,6 +157,13 @@ def lib():
             "mps_batch_scene_info": (C.c_int, [H, C.c_uint32, C.POINTER(mps_scene_info)]),
             "mps_set_body_force": (C.c_int, [H, C.c_uint32, C.c_float, C.c_float]),
             "mps_autotune": (C.c_int, [H, C.c_int, C.POINTER(mps_tune_report)]),
+            "mps_surface_setup": (C.c_int, [H, C.POINTER(mps_surface_grid), C.c_uint32]),
+            "mps_surface_extract_async": (C.c_int, [H]),
+            "mps_surface_extract": (C.c_int, [H, U]),
+            "mps_surface_get": (C.c_int, [H, Fp, Fp, C.c_uint32, U]),
+            "mps_surface_vertex_values": (C.c_int, [H, Fp, Fp]),
+            "mps_surface_write_stl": (C.c_int, [H, C.c_char_p]),
+            "mps_surface_case_table": (C.c_int, [C.POINTER(C.c_uint8), C.POINTER(C.c_int8)]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
@@ -169,6 +183,17 @@ def default_options(**kw) -> mps_options:
 
 def _p(a, t=C.c_float):
     return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def surface_case_table():
+    """The library's generated marching-cubes table: list of triangles
+    (edge triples) per case."""
+    n = (C.c_uint8 * 256)()
+    t = (C.c_int8 * (256 * 16))()
+    st = lib().mps_surface_case_table(n, t)
+    if st != 0:
+        raise MPSError(st, "case table")
+    return [[tuple(t[16 * c + 3 * k + j] for j in range(3)) for k in range(n[c])] for c in range(256)]
 
 
 class Simulation:
@@ -394,6 +419,44 @@ class Simulation:
         self._check(lib().mps_autotune(self.h, steps, C.byref(r)))
         return {"stage_threads": r.stage_threads, "ppe_threads": r.ppe_threads,
                 "stage_ms": list(r.stage_ms), "ppe_ms_per_iter": list(r.ppe_ms_per_iter)}
+
+    # ---- free surface (marching cubes)
+    def surface_setup(self, shape, origin, spacing, max_triangles: int):
+        g = mps_surface_grid()
+        g.nx, g.ny, g.nz = (int(v) for v in shape)
+        for d in range(3):
+            g.origin[d] = origin[d]
+            g.spacing[d] = spacing[d]
+        self._check(lib().mps_surface_setup(self.h, C.byref(g), max_triangles))
+        self._surf_shape = tuple(int(v) for v in shape)
+        self._surf_cap = max_triangles
+
+    def surface_extract(self, wait: bool = True) -> int:
+        if not wait:
+            self._check(lib().mps_surface_extract_async(self.h))
+            return -1
+        n = C.c_uint32()
+        self._check(lib().mps_surface_extract(self.h, C.byref(n)))
+        return n.value
+
+    def surface_triangles(self):
+        n = C.c_uint32()
+        self._check(lib().mps_surface_get(self.h, None, None, 0, C.byref(n)))
+        m = min(n.value, self._surf_cap)
+        pos = np.empty((m, 3, 3), np.float32)
+        nrm = np.empty((m, 3, 3), np.float32)
+        self._check(lib().mps_surface_get(self.h, _p(pos), _p(nrm), m, C.byref(n)))
+        return pos, nrm
+
+    def surface_vertex_values(self):
+        nx, ny, nz = self._surf_shape
+        out = np.empty((nz, ny, nx), np.float32)
+        iso = C.c_float()
+        self._check(lib().mps_surface_vertex_values(self.h, _p(out), C.byref(iso)))
+        return out, iso.value
+
+    def surface_write_stl(self, path: str):
+        self._check(lib().mps_surface_write_stl(self.h, path.encode()))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -16,6 +16,7 @@
 #include "host_io.h"
 #include "physics.cuh"
 #include "ppe.cuh"
+#include "surface.cuh"
 
 using namespace mpsb;
 
@@ -72,6 +73,7 @@ struct mps_handle {
     bool graph_off = false;          // stream capture refused: direct launches
     std::string graph_note;
     int stage_threads = 256;         // block size of the particle-stage kernels (autotuned)
+    SurfaceWork surf;                // marching-cubes free surface
 };
 
 static void drop_graphs(mps_handle* h);
@@ -862,6 +864,7 @@ extern "C" void mps_destroy(mps_handle* h) {
         if (h->graph[b]) cudaGraphExecDestroy(h->graph[b]);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     ppe_free(h->ppe);
+    surface_free(h->surf);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1339,6 +1342,132 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
     drop_graphs(h);
     if (rep) *rep = r;
     return MPS_OK;
+}
+
+// ---------------------------------------------------------------- free surface
+extern "C" mps_status mps_surface_case_table(uint8_t* ntri, int8_t* tri) {
+    if (!ntri || !tri) return MPS_ERR_INVALID;
+    mc_build_table(ntri, reinterpret_cast<int8_t(*)[16]>(tri));
+    return MPS_OK;
+}
+
+static mps_status need_surface(mps_handle* h) {
+    if (!h) return MPS_ERR_INVALID;
+    if (!h->surf.ready) {
+        h->err = "call mps_surface_setup first";
+        return MPS_ERR_INVALID;
+    }
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_setup(mps_handle* h, const mps_surface_grid* g, uint32_t max_triangles) {
+    if (!h || !g || max_triangles == 0) return MPS_ERR_INVALID;
+    if (h->nscenes) {
+        h->err = "surfaces are extracted from single-scene handles";
+        return MPS_ERR_INVALID;
+    }
+    CK(cudaSetDevice(h->dev));
+    SurfaceGrid sg;
+    sg.nx = g->nx;
+    sg.ny = g->ny;
+    sg.nz = g->nz;
+    sg.ox = g->origin[0];
+    sg.oy = g->origin[1];
+    sg.oz = g->origin[2];
+    sg.hx = g->spacing[0];
+    sg.hy = g->spacing[1];
+    sg.hz = g->spacing[2];
+    int e = surface_setup(h->surf, sg, max_triangles, h->stream, &h->err);
+    if (e != MPS_OK) return (mps_status)e;
+    surface_enqueue_iso(h->surf, stage_args(h), h->cap, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    uint32_t bits[2];
+    CK(cudaMemcpy(bits, h->surf.ntri, 8, cudaMemcpyDeviceToHost));
+    memcpy(&h->surf.iso, &bits[1], 4);
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_extract_async(mps_handle* h) {
+    mps_status s = need_surface(h);
+    if (s != MPS_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    surface_enqueue_extract(h->surf, stage_args(h), h->stream);
+    CK(cudaGetLastError());
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_extract(mps_handle* h, uint32_t* ntri) {
+    mps_status s = mps_surface_extract_async(h);
+    if (s != MPS_OK) return s;
+    uint32_t n = 0;
+    CK(cudaMemcpyAsync(&n, h->surf.ntri, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (ntri) *ntri = n;
+    if (n > h->surf.max_tri) {
+        h->err = "the surface has more triangles than the buffer holds (" + std::to_string(n) + ")";
+        return MPS_ERR_CAPACITY;
+    }
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_get(mps_handle* h, float* pos9, float* nrm9, uint32_t max_triangles,
+                                      uint32_t* ntri) {
+    mps_status s = need_surface(h);
+    if (s != MPS_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    uint32_t n = 0;
+    CK(cudaMemcpyAsync(&n, h->surf.ntri, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (ntri) *ntri = n;
+    uint32_t m = n < h->surf.max_tri ? n : h->surf.max_tri;
+    m = m < max_triangles ? m : max_triangles;
+    if (m && pos9) CK(cudaMemcpyAsync(pos9, h->surf.tri_pos, (size_t)m * 36, cudaMemcpyDeviceToHost, h->stream));
+    if (m && nrm9) CK(cudaMemcpyAsync(nrm9, h->surf.tri_nrm, (size_t)m * 36, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_vertex_values(mps_handle* h, float* values, float* iso) {
+    mps_status s = need_surface(h);
+    if (s != MPS_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    const SurfaceGrid& g = h->surf.g;
+    if (values)
+        CK(cudaMemcpyAsync(values, h->surf.vn, (size_t)g.nx * g.ny * g.nz * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (iso) *iso = h->surf.iso;
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_surface_write_stl(mps_handle* h, const char* path) {
+    mps_status s = need_surface(h);
+    if (s != MPS_OK) return s;
+    if (!path) return MPS_ERR_INVALID;
+    uint32_t n = 0;
+    s = mps_surface_get(h, nullptr, nullptr, 0, &n);
+    if (s != MPS_OK) return s;
+    const uint32_t m = n < h->surf.max_tri ? n : h->surf.max_tri;
+    std::vector<float> p((size_t)m * 9), q((size_t)m * 9);
+    s = mps_surface_get(h, p.data(), q.data(), m, &n);
+    if (s != MPS_OK) return s;
+    FILE* f = fopen(path, "wb");
+    if (!f) return MPS_ERR_IO;
+    char header[80];
+    memset(header, 0, sizeof header);
+    snprintf(header, sizeof header, "MPS free surface, %u triangles", m);
+    fwrite(header, 1, 80, f);
+    fwrite(&m, 4, 1, f);
+    for (uint32_t t = 0; t < m; t++) {
+        float rec[12];
+        for (int d = 0; d < 3; d++) rec[d] = (q[9 * t + d] + q[9 * t + 3 + d] + q[9 * t + 6 + d]) / 3.f;
+        for (int k = 0; k < 9; k++) rec[3 + k] = p[9 * (size_t)t + k];
+        fwrite(rec, 4, 12, f);
+        const uint16_t attr = 0;
+        fwrite(&attr, 2, 1, f);
+    }
+    const bool ok = fclose(f) == 0;
+    return ok ? MPS_OK : MPS_ERR_IO;
 }
 
 extern "C" mps_status mps_get_normal_ids(mps_handle* h, uint32_t* normal_id) {

@@ -255,6 +255,15 @@ def batch_scenes(n: int = 64, seed: int = 0):
     return out
 
 
+def surface_grid(scene: Scene, shape):
+    """Origin and spacing of a marching-cubes vertex grid of `shape`
+    (vertices per axis) spanning the tank interior's lattice sites."""
+    S = scene.wall_layers + scene.dummy_layers
+    origin = tuple(S * scene.l0 for _ in range(3))
+    spacing = tuple((n - 1) * scene.l0 / (m - 1) for n, m in zip(scene.interior, shape))
+    return origin, spacing
+
+
 def small_tank(seed: int = 0, interior=(14, 6, 12), fluid=(5, 4, 8), l0: float = 0.02,
                rlap: float = 4.0, dt: float = 1e-4, cs: float = 20.0) -> Scene:
     """A few-thousand-particle tank for parity tests."""
