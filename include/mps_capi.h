@@ -337,15 +337,20 @@ mps_status mps_surface_case_table(uint8_t ntri[256], int8_t tri[256 * 16]);
 /* ---- autotuner ----
  * No counterpart in the reference.  Times, on the handle's own scene with
  * CUDA events over `steps` steps per candidate, the block size of the
- * particle-stage kernels (64, 128, 256 threads) and the shape of the
- * persistent PPE grid (1024, 512 or 256 threads per block at 1024 threads
- * per SM; semi-implicit only), and keeps the fastest of each.  The scene
- * advances by the steps taken (call it during warm-up). */
+ * particle-stage kernels (64, 128, 256 threads) and, for the semi-implicit
+ * PPE, the persistent grid's shape (1024, 512 or 256 threads per block at
+ * 1024 threads per SM) and its SpMV form (weights stored by the assembly,
+ * or recomputed from the positions in every product), and keeps the
+ * fastest of each.  The scene advances by the steps taken (call it during
+ * warm-up). */
 typedef struct mps_tune_report {
     int stage_threads;         /* chosen */
     int ppe_threads;           /* chosen */
+    int ppe_stored_weights;    /* chosen: 1 stored, 0 recomputed */
     float stage_ms[3];         /* visc + collision + pnd + dash per step at 64, 128, 256 */
-    float ppe_ms_per_iter[3];  /* PPE solve ms per PCG iteration at 1024, 512, 256 (-1: not held) */
+    /* PPE solve ms per PCG iteration: [0..2] stored weights at 1024, 512,
+     * 256 threads per block, [3..5] recomputed weights (-1: not held) */
+    float ppe_ms_per_iter[6];
     uint32_t reserved[4];
 } mps_tune_report;
 mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* report);

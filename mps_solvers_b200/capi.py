@@ -84,8 +84,9 @@ class mps_scene_info(C.Structure):
 
 
 class mps_tune_report(C.Structure):
-    _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("stage_ms", C.c_float * 3),
-                ("ppe_ms_per_iter", C.c_float * 3), ("reserved", C.c_uint32 * 4)]
+    _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("ppe_stored_weights", C.c_int),
+                ("stage_ms", C.c_float * 3), ("ppe_ms_per_iter", C.c_float * 6),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class mps_surface_grid(C.Structure):
@@ -418,7 +419,8 @@ class Simulation:
         r = mps_tune_report()
         self._check(lib().mps_autotune(self.h, steps, C.byref(r)))
         return {"stage_threads": r.stage_threads, "ppe_threads": r.ppe_threads,
-                "stage_ms": list(r.stage_ms), "ppe_ms_per_iter": list(r.ppe_ms_per_iter)}
+                "ppe_stored_weights": r.ppe_stored_weights, "stage_ms": list(r.stage_ms),
+                "ppe_ms_per_iter": list(r.ppe_ms_per_iter)}
 
     # ---- free surface (marching cubes)
     def surface_setup(self, shape, origin, spacing, max_triangles: int):

@@ -1279,11 +1279,12 @@ extern "C" mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage
     return read_status(h, nullptr);
 }
 
-// Autotuner: the block size of the particle-stage kernels (64, 128, 256)
-// and the shape of the persistent PPE grid (1024, 512 or 256 threads per
-// block, 1024 threads per SM), each timed with CUDA events over `steps`
-// steps of the handle's own scene; the fastest is kept.  The scene advances
-// by the steps taken.
+// Autotuner: the block size of the particle-stage kernels (64, 128, 256),
+// and for the persistent PPE solver the grid shape (1024, 512 or 256
+// threads per block, 1024 threads per SM) and the SpMV form (stored weights
+// or weights recomputed from positions), each timed with CUDA events over
+// `steps` steps of the handle's own scene; the fastest is kept.  The scene
+// advances by the steps taken.
 extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* rep) {
     if (!h || steps < 1) return MPS_ERR_INVALID;
     CK(cudaSetDevice(h->dev));
@@ -1313,11 +1314,14 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
         const int ppe_cand[3] = {1024, 512, 256};
         best = 1e300;
         int best_p = h->ppe.threads;
-        for (int c = 0; c < 3; c++) {
-            if (ppe_set_threads(h->ppe, ppe_cand[c]) != MPS_OK) {
+        bool best_sw = h->ppe.stored_weights;
+        for (int c = 0; c < 6; c++) {
+            const bool sw = c < 3;
+            if (ppe_set_threads(h->ppe, ppe_cand[c % 3]) != MPS_OK) {
                 r.ppe_ms_per_iter[c] = -1.f;  // the device cannot hold this shape
                 continue;
             }
+            h->ppe.stored_weights = sw;
             drop_graphs(h);
             double tot = 0.0;
             long iters = 0;
@@ -1333,11 +1337,14 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
             r.ppe_ms_per_iter[c] = (float)t;
             if (t < best) {
                 best = t;
-                best_p = ppe_cand[c];
+                best_p = ppe_cand[c % 3];
+                best_sw = sw;
             }
         }
         ppe_set_threads(h->ppe, best_p);
+        h->ppe.stored_weights = best_sw;
         r.ppe_threads = best_p;
+        r.ppe_stored_weights = best_sw ? 1 : 0;
     }
     drop_graphs(h);
     if (rep) *rep = r;

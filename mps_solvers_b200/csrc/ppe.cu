@@ -253,6 +253,7 @@ struct SolveArgs {
     const uint32_t* nrows;
     const uint32_t* off;
     const uint32_t* scols;
+    const float* sw;          // stored weights (same layout as scols)
     const float4* pos;
     float rlap, rlap_thr;
     // learned preconditioner
@@ -297,7 +298,9 @@ __device__ __forceinline__ float lp_packed_row(const uint32_t* __restrict__ off,
     return s;
 }
 
-template <bool EX, int PREC>
+// SW: stored weights (the pack's) instead of recomputing them from the
+// positions; the two give the same matrix, the autotuner picks the faster.
+template <bool EX, int PREC, bool SW>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them
     // are dealt to warps round-robin (4 lanes per row inside a slice); the
@@ -322,12 +325,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             const uint32_t base = __ldg(S.off + sl);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
             const uint32_t* cols = S.scols + base + lane;
+            const float* wts = S.sw + base + lane;
             const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
             const float4 pi = __ldg(S.pos + ii);
             double s = 0.0;
             for (uint32_t t = 0; t < T; t++) {
                 const uint32_t j = __ldg(cols + 32 * t);
-                s += (double)stencil_weight<EX>(S, pi, ii, j) * S.x64[j];
+                const float wt = SW ? __ldg(wts + 32 * t) : stencil_weight<EX>(S, pi, ii, j);
+                s += (double)wt * S.x64[j];
             }
             s += __shfl_xor_sync(0xffffffffu, s, 8);
             s += __shfl_xor_sync(0xffffffffu, s, 16);
@@ -393,6 +398,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const uint32_t base = __ldg(S.off + sl);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
                 const uint32_t* cols = S.scols + base + lane;
+                const float* wts = S.sw + base + lane;
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
@@ -403,7 +409,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     for (int u = 0; u < 4; u++) j[u] = __ldg(cols + 32 * (t + u));
                     float w[4];
 #pragma unroll
-                    for (int u = 0; u < 4; u++) w[u] = stencil_weight<EX>(S, pi, ii, j[u]);
+                    for (int u = 0; u < 4; u++)
+                        w[u] = SW ? __ldg(wts + 32 * (t + u)) : stencil_weight<EX>(S, pi, ii, j[u]);
 #pragma unroll
                     for (int u = 0; u < 4; u += 2) {
                         s0 = fmaf(w[u], fmaf(beta, pcur[j[u]], S.z[j[u]]), s0);
@@ -412,7 +419,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 }
                 for (; t < T; t++) {
                     const uint32_t jj = __ldg(cols + 32 * t);
-                    s0 = fmaf(stencil_weight<EX>(S, pi, ii, jj), fmaf(beta, pcur[jj], S.z[jj]), s0);
+                    const float wt = SW ? __ldg(wts + 32 * t) : stencil_weight<EX>(S, pi, ii, jj);
+                    s0 = fmaf(wt, fmaf(beta, pcur[jj], S.z[jj]), s0);
                 }
                 float s = s0 + s1;
                 s += __shfl_xor_sync(0xffffffffu, s, 8);
@@ -515,6 +523,7 @@ struct BatchSolveArgs {
     const uint32_t* row_scene;
     const uint32_t* off;
     const uint32_t* scols;
+    const float* sw;
     const float4* pos;
     const Phys* phys;
     const double* b64;
@@ -614,7 +623,7 @@ __device__ __forceinline__ float batch_weight(const float4* __restrict__ pos, fl
     return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
 }
 
-template <bool EX>
+template <bool EX, bool SW>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs S) {
     __shared__ double acc[3 * PPE_MAX_SCENES];
     __shared__ double rz[PPE_MAX_SCENES], stop[PPE_MAX_SCENES], alpha[PPE_MAX_SCENES], rel[PPE_MAX_SCENES];
@@ -655,13 +664,15 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             const uint32_t base = __ldg(S.off + sl);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
             const uint32_t* cols = S.scols + base + lane;
+            const float* wts = S.sw + base + lane;
             const float4 pi = __ldg(S.pos + ii);
             const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
             double sum = 0.0;
             if (work)
                 for (uint32_t t = 0; t < T; t++) {
                     const uint32_t j = __ldg(cols + 32 * t);
-                    sum += (double)batch_weight<EX>(S.pos, rl, thr, pi, ii, j) * S.x64[j];
+                    const float wt = SW ? __ldg(wts + 32 * t) : batch_weight<EX>(S.pos, rl, thr, pi, ii, j);
+                    sum += (double)wt * S.x64[j];
                 }
             sum += __shfl_xor_sync(0xffffffffu, sum, 8);
             sum += __shfl_xor_sync(0xffffffffu, sum, 16);
@@ -723,6 +734,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const uint32_t base = __ldg(S.off + sl);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
                 const uint32_t* cols = S.scols + base + lane;
+                const float* wts = S.sw + base + lane;
                 const float4 pi = __ldg(S.pos + ii);
                 const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
                 const float bs = beta[s];
@@ -730,7 +742,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 if (work)
                     for (uint32_t t = 0; t < T; t++) {
                         const uint32_t j = __ldg(cols + 32 * t);
-                        sum = fmaf(batch_weight<EX>(S.pos, rl, thr, pi, ii, j), fmaf(bs, pcur[j], S.z[j]), sum);
+                        const float wt = SW ? __ldg(wts + 32 * t) : batch_weight<EX>(S.pos, rl, thr, pi, ii, j);
+                        sum = fmaf(wt, fmaf(bs, pcur[j], S.z[j]), sum);
                     }
                 sum += __shfl_xor_sync(0xffffffffu, sum, 8);
                 sum += __shfl_xor_sync(0xffffffffu, sum, 16);
@@ -905,10 +918,16 @@ __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__
     width[s] = SELL_C * ((m + 3u) & ~3u);
 }
 
+// Columns, and their weights w(r; rlap) computed from the positions by the
+// function the assembly used for the diagonal (0 on padding entries, whose
+// column is the row itself).
+template <bool EX>
 __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm,
                                                    const uint32_t* __restrict__ rlen, const uint32_t* __restrict__ rowlist,
                                                    const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
-                                                   uint32_t* __restrict__ scols) {
+                                                   uint32_t* __restrict__ scols, float* __restrict__ sw,
+                                                   const float4* __restrict__ pos, Phys P,
+                                                   const Phys* __restrict__ phys, const uint32_t* __restrict__ row_scene) {
     const uint32_t R = *nrows;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
     const uint32_t slice = k / SELL_C, r = k % SELL_C;
@@ -919,9 +938,24 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
     const uint32_t i = has ? rowlist[k] : 0u;
     const uint32_t len = has ? rlen[i] : 0u;
     const uint32_t* rc = cols_rm + (size_t)i * PPE_W;
+    float rl = P.rlap, thr = P.rlap_thr;
+    if (phys && has) {
+        rl = phys[row_scene[k]].rlap;
+        thr = phys[row_scene[k]].rlap_thr;
+    }
+    const float4 pi = pos[i];
     for (uint32_t e = 0; e < W; e++) {
         const bool real = e < len;
-        scols[base + SELL_C * e + r] = real ? rc[e] : i;
+        const uint32_t j = real ? rc[e] : i;
+        float w = 0.f;
+        if (real) {
+            const float4 pj = pos[j];
+            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+            w = rr < thr ? weight_rr<EX>(rl, rr) : 0.f;
+        }
+        scols[base + SELL_C * e + r] = j;
+        sw[base + SELL_C * e + r] = w;
     }
 }
 
@@ -1026,6 +1060,16 @@ void launch_n0_lambda64(const StageArgs& a, const double* n64, double* out, cuda
 }
 
 // ---------------------------------------------------------------- host side
+// every variant of the persistent solver (cooperative launches must fit)
+static std::vector<const void*> solve_kernels() {
+    return {(const void*)k_ppe_solve<true, 0, true>,    (const void*)k_ppe_solve<false, 0, true>,
+            (const void*)k_ppe_solve<true, 1, true>,    (const void*)k_ppe_solve<false, 1, true>,
+            (const void*)k_ppe_solve<true, 0, false>,   (const void*)k_ppe_solve<false, 0, false>,
+            (const void*)k_ppe_solve<true, 1, false>,   (const void*)k_ppe_solve<false, 1, false>,
+            (const void*)k_ppe_solve_batch<true, true>, (const void*)k_ppe_solve_batch<false, true>,
+            (const void*)k_ppe_solve_batch<true, false>, (const void*)k_ppe_solve_batch<false, false>};
+}
+
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_params& prm, cudaStream_t st,
               std::string* err) {
     w.cap = cap;
@@ -1056,6 +1100,7 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.id_snap, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.sell_off, ((size_t)cap / SELL_C + 4) * sizeof(uint32_t));
     ok &= al((void**)&w.sell_cols, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(uint32_t));
+    ok &= al((void**)&w.sell_w, ((size_t)cap + 8) * (PPE_W + 4) * sizeof(float));
     ok &= al((void**)&w.tilecnt, ((size_t)cap / 2048 + 2) * sizeof(uint32_t));
     ok &= al((void**)&w.nrows, sizeof(uint32_t));
     if (!ok) {
@@ -1067,15 +1112,12 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     {
-        int o[6] = {0, 0, 0, 0, 0, 0};
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], k_ppe_solve<true, 0>, PPE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], k_ppe_solve<false, 0>, PPE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], k_ppe_solve<true, 1>, PPE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], k_ppe_solve<false, 1>, PPE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[4], k_ppe_solve_batch<true>, PPE_THREADS, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[5], k_ppe_solve_batch<false>, PPE_THREADS, 0);
-        per_sm = o[0];
-        for (int q = 1; q < 6; q++) per_sm = o[q] < per_sm ? o[q] : per_sm;
+        per_sm = 1 << 30;
+        for (const void* f : solve_kernels()) {
+            int o = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, PPE_THREADS, 0);
+            per_sm = o < per_sm ? o : per_sm;
+        }
     }
     if (!coop || per_sm < 1) {
         *err = "device cannot run the cooperative PPE solver";
@@ -1157,8 +1199,16 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
     k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
     launch_scan_exclusive(w.sell_off, maxslices + 1, st);
-    k_sell_pack<<<blocks_for(maxslices * SELL_C, 256), 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows,
-                                                                     w.sell_off, w.sell_cols);
+    {
+        const Phys* phys = a.batch.n ? a.batch.phys : nullptr;
+        const uint32_t nb = blocks_for(maxslices * SELL_C, 256);
+        if (a.exact)
+            k_sell_pack<true><<<nb, 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows, w.sell_off, w.sell_cols,
+                                                  w.sell_w, a.cur.pos, a.P, phys, w.row_scene);
+        else
+            k_sell_pack<false><<<nb, 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows, w.sell_off, w.sell_cols,
+                                                   w.sell_w, a.cur.pos, a.P, phys, w.row_scene);
+    }
     // the state this system was assembled from
     cudaMemcpyAsync(w.pos_snap, a.cur.pos, (size_t)cap * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
@@ -1217,6 +1267,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.nrows = w.nrows;
     S.off = w.sell_off;
     S.scols = w.sell_cols;
+    S.sw = w.sell_w;
     S.pos = a.cur.pos;
     S.rlap = a.P.rlap;
     S.rlap_thr = a.P.rlap_thr;
@@ -1240,6 +1291,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.row_scene = w.row_scene;
         B.off = w.sell_off;
         B.scols = w.sell_cols;
+        B.sw = w.sell_w;
         B.pos = a.cur.pos;
         B.phys = a.batch.phys;
         B.b64 = w.b64;
@@ -1265,15 +1317,24 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.inner_cap = S.inner_cap;
         B.max_outer = S.max_outer;
         void* bargs[] = {&B};
-        const void* bfn = a.exact ? (const void*)k_ppe_solve_batch<true> : (const void*)k_ppe_solve_batch<false>;
+        const void* bfn = w.stored_weights
+                              ? (a.exact ? (const void*)k_ppe_solve_batch<true, true>
+                                         : (const void*)k_ppe_solve_batch<false, true>)
+                              : (a.exact ? (const void*)k_ppe_solve_batch<true, false>
+                                         : (const void*)k_ppe_solve_batch<false, false>);
         w.launch_err = launch_cooperative(bfn, w.blocks, w.threads, bargs, st);
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
     void* args[] = {&S};
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
-    const void* fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1> : (const void*)k_ppe_solve<true, 0>)
-                             : (learned ? (const void*)k_ppe_solve<false, 1> : (const void*)k_ppe_solve<false, 0>);
+    const void* fn;
+    if (w.stored_weights)
+        fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1, true> : (const void*)k_ppe_solve<true, 0, true>)
+                     : (learned ? (const void*)k_ppe_solve<false, 1, true> : (const void*)k_ppe_solve<false, 0, true>);
+    else
+        fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1, false> : (const void*)k_ppe_solve<true, 0, false>)
+                     : (learned ? (const void*)k_ppe_solve<false, 1, false> : (const void*)k_ppe_solve<false, 0, false>);
     w.launch_err = launch_cooperative(fn, w.blocks, w.threads, args, st);
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
     return 2;
@@ -1282,10 +1343,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
 int ppe_set_threads(PpeWork& w, int threads) {
     if (threads != 256 && threads != 512 && threads != 1024) return MPS_ERR_INVALID;
     const int per_sm = PPE_THREADS / threads;
-    const void* fns[] = {(const void*)k_ppe_solve<true, 0>, (const void*)k_ppe_solve<false, 0>,
-                         (const void*)k_ppe_solve<true, 1>, (const void*)k_ppe_solve<false, 1>,
-                         (const void*)k_ppe_solve_batch<true>, (const void*)k_ppe_solve_batch<false>};
-    for (const void* f : fns) {
+    for (const void* f : solve_kernels()) {
         int o = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, threads, 0) != cudaSuccess || o < per_sm)
             return MPS_ERR_INVALID;
@@ -1328,7 +1386,7 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar,
-                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.y, w.ralt, w.pos_snap, w.n_snap,
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
                   w.id_snap, w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
                   w.scene_relres};
     lp_free(w.lp);

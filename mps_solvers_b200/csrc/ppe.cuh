@@ -56,6 +56,8 @@ struct PpeWork {
     uint32_t* nrows = nullptr;
     uint32_t* sell_off = nullptr;      // slice offsets (exclusive scan of 32 * width)
     uint32_t* sell_cols = nullptr;
+    float* sell_w = nullptr;           // the entries' weights, same layout
+    bool stored_weights = true;        // SpMV reads sell_w (else recomputes from positions)
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
     // learned preconditioner (set up on first use)
     LearnedWork lp;

@@ -32,7 +32,8 @@ def test_autotune_semi_shapes(capi, tmp_path):
     with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
         rep = s.autotune(2)
         assert rep["ppe_threads"] in (256, 512, 1024)
-        assert rep["ppe_ms_per_iter"][0] > 0   # the default shape always runs
+        assert rep["ppe_ms_per_iter"][0] > 0 and rep["ppe_ms_per_iter"][3] > 0  # default shape
+        assert rep["ppe_stored_weights"] in (0, 1)
         for _ in range(3):
             st = s.step(1)
             assert st.status == 0 and st.cg_relres <= 1e-8
