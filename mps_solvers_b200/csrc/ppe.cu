@@ -283,6 +283,20 @@ __device__ __forceinline__ float stencil_weight(const SolveArgs& S, const float4
     return (j != i && rr < S.rlap_thr) ? weight_rr<EX>(S.rlap, rr) : 0.f;
 }
 
+// The weights of one lane's 4 entries: stored, or recomputed from positions.
+template <bool EX, bool SW>
+__device__ __forceinline__ float4 chunk_weights(const float4* __restrict__ w4, const float4* __restrict__ pos, float rlap,
+                                                float thr, const float4& pi, uint32_t i, const uint4& c) {
+    if (SW) return __ldg(w4);
+    auto one = [&](uint32_t j) {
+        const float4 pj = __ldg(pos + j);
+        const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+        const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+        return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
+    };
+    return make_float4(one(c.x), one(c.y), one(c.z), one(c.w));
+}
+
 // Row position k of the learned factor's packed layout: sum over its
 // entries of val * x(col), x given as a functor of the column.
 template <class X>
@@ -323,16 +337,17 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         for (uint32_t sl = gw; sl < nslices; sl += nw) {
             const uint32_t k = sl * SELL_C + rsub;
             const uint32_t base = __ldg(S.off + sl);
-            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
-            const uint32_t* cols = S.scols + base + lane;
-            const float* wts = S.sw + base + lane;
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
+            const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+            const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
             const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
             const float4 pi = __ldg(S.pos + ii);
             double s = 0.0;
             for (uint32_t t = 0; t < T; t++) {
-                const uint32_t j = __ldg(cols + 32 * t);
-                const float wt = SW ? __ldg(wts + 32 * t) : stencil_weight<EX>(S, pi, ii, j);
-                s += (double)wt * S.x64[j];
+                const uint4 c = __ldg(cols + 32 * t);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                s += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
+                     (double)w.w * S.x64[c.w];
             }
             s += __shfl_xor_sync(0xffffffffu, s, 8);
             s += __shfl_xor_sync(0xffffffffu, s, 16);
@@ -396,31 +411,20 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             for (uint32_t sl = gw; sl < nslices; sl += nw) {
                 const uint32_t k = sl * SELL_C + rsub;
                 const uint32_t base = __ldg(S.off + sl);
-                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;  // W / 4
-                const uint32_t* cols = S.scols + base + lane;
-                const float* wts = S.sw + base + lane;
+                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
+                const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+                const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
-                uint32_t t = 0;
-                for (; t + 4 <= T; t += 4) {
-                    uint32_t j[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) j[u] = __ldg(cols + 32 * (t + u));
-                    float w[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++)
-                        w[u] = SW ? __ldg(wts + 32 * (t + u)) : stencil_weight<EX>(S, pi, ii, j[u]);
-#pragma unroll
-                    for (int u = 0; u < 4; u += 2) {
-                        s0 = fmaf(w[u], fmaf(beta, pcur[j[u]], S.z[j[u]]), s0);
-                        s1 = fmaf(w[u + 1], fmaf(beta, pcur[j[u + 1]], S.z[j[u + 1]]), s1);
-                    }
-                }
-                for (; t < T; t++) {
-                    const uint32_t jj = __ldg(cols + 32 * t);
-                    const float wt = SW ? __ldg(wts + 32 * t) : stencil_weight<EX>(S, pi, ii, jj);
-                    s0 = fmaf(wt, fmaf(beta, pcur[jj], S.z[jj]), s0);
+#pragma unroll 2
+                for (uint32_t t = 0; t < T; t++) {
+                    const uint4 c = __ldg(cols + 32 * t);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                    s0 = fmaf(w.x, fmaf(beta, pcur[c.x], S.z[c.x]), s0);
+                    s1 = fmaf(w.y, fmaf(beta, pcur[c.y], S.z[c.y]), s1);
+                    s0 = fmaf(w.z, fmaf(beta, pcur[c.z], S.z[c.z]), s0);
+                    s1 = fmaf(w.w, fmaf(beta, pcur[c.w], S.z[c.w]), s1);
                 }
                 float s = s0 + s1;
                 s += __shfl_xor_sync(0xffffffffu, s, 8);
@@ -662,17 +666,18 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             const bool work = has && !done[s];
             if (!__any_sync(0xffffffffu, work)) continue;
             const uint32_t base = __ldg(S.off + sl);
-            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
-            const uint32_t* cols = S.scols + base + lane;
-            const float* wts = S.sw + base + lane;
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+            const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+            const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
             const float4 pi = __ldg(S.pos + ii);
             const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
             double sum = 0.0;
             if (work)
                 for (uint32_t t = 0; t < T; t++) {
-                    const uint32_t j = __ldg(cols + 32 * t);
-                    const float wt = SW ? __ldg(wts + 32 * t) : batch_weight<EX>(S.pos, rl, thr, pi, ii, j);
-                    sum += (double)wt * S.x64[j];
+                    const uint4 c = __ldg(cols + 32 * t);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, rl, thr, pi, ii, c);
+                    sum += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
+                           (double)w.w * S.x64[c.w];
                 }
             sum += __shfl_xor_sync(0xffffffffu, sum, 8);
             sum += __shfl_xor_sync(0xffffffffu, sum, 16);
@@ -732,19 +737,23 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const bool work = has && active[s];
                 if (!__any_sync(0xffffffffu, work)) continue;
                 const uint32_t base = __ldg(S.off + sl);
-                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 5;
-                const uint32_t* cols = S.scols + base + lane;
-                const float* wts = S.sw + base + lane;
+                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+                const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+                const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
                 const float4 pi = __ldg(S.pos + ii);
                 const float rl = S.phys[s].rlap, thr = S.phys[s].rlap_thr;
                 const float bs = beta[s];
-                float sum = 0.f;
+                float sum = 0.f, sum1 = 0.f;
                 if (work)
                     for (uint32_t t = 0; t < T; t++) {
-                        const uint32_t j = __ldg(cols + 32 * t);
-                        const float wt = SW ? __ldg(wts + 32 * t) : batch_weight<EX>(S.pos, rl, thr, pi, ii, j);
-                        sum = fmaf(wt, fmaf(bs, pcur[j], S.z[j]), sum);
+                        const uint4 c = __ldg(cols + 32 * t);
+                        const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, rl, thr, pi, ii, c);
+                        sum = fmaf(w.x, fmaf(bs, pcur[c.x], S.z[c.x]), sum);
+                        sum1 = fmaf(w.y, fmaf(bs, pcur[c.y], S.z[c.y]), sum1);
+                        sum = fmaf(w.z, fmaf(bs, pcur[c.z], S.z[c.z]), sum);
+                        sum1 = fmaf(w.w, fmaf(bs, pcur[c.w], S.z[c.w]), sum1);
                     }
+                sum += sum1;
                 sum += __shfl_xor_sync(0xffffffffu, sum, 8);
                 sum += __shfl_xor_sync(0xffffffffu, sum, 16);
                 const bool contrib = q == 0 && work;
@@ -897,11 +906,13 @@ __global__ void __launch_bounds__(256) k_rows_scatter(const uint32_t* __restrict
 
 // ---------------------------------------------------------------- SELL-8
 // Sliced ELL: slice s holds rows rowlist[8s .. 8s+7], width W_s = the
-// longest of them rounded up to a multiple of 4, entries column-major
-// (entry e of row r at sell_off[s] + 8e + r), padded with the row's own index
-// and weight 0.  A warp takes one slice with 4 lanes per row: lane L = 8q + r
-// reads entries e = 4t + q, i.e. address 32t + L, so every load is one
-// coalesced 128-byte line.
+// longest of them rounded up to a multiple of 16, padded with the row's own
+// index and weight 0.  A warp takes one slice with 4 lanes per row; lane
+// L = 8q + r owns, in every chunk t of 16 entries of row r, the 4 entries
+// 16t + 4q .. 16t + 4q + 3, stored together at word
+// sell_off[s] + 4 (32t + L), so each lane reads them (columns, and weights
+// in the same layout) as one 16-byte vector and a warp's load is one
+// contiguous 512-byte block.
 __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__ rlen,
                                                     const uint32_t* __restrict__ rowlist,
                                                     const uint32_t* __restrict__ nrows, uint32_t* __restrict__ width,
@@ -915,7 +926,7 @@ __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__
         const uint32_t k = k0 + r;
         if (k < R) m = max(m, rlen[rowlist[k]]);
     }
-    width[s] = SELL_C * ((m + 3u) & ~3u);
+    width[s] = SELL_C * ((m + 15u) & ~15u);
 }
 
 // Columns, and their weights w(r; rlap) computed from the positions by the
@@ -954,8 +965,10 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
             const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
             w = rr < thr ? weight_rr<EX>(rl, rr) : 0.f;
         }
-        scols[base + SELL_C * e + r] = j;
-        sw[base + SELL_C * e + r] = w;
+        // entry e of row r: chunk e / 16, lane r + 8 ((e / 4) % 4), slot e % 4
+        const uint32_t at = base + (((e >> 4) * 32u + r + SELL_C * ((e >> 2) & 3u)) << 2) + (e & 3u);
+        scols[at] = j;
+        sw[at] = w;
     }
 }
 
