@@ -242,10 +242,9 @@ struct SolveArgs {
     const double* b64;
     double* x64;
     float* r;
-    float* z;
+    float2* zp0;   // (z, p) per row, two buffers: current and next
+    float2* zp1;
     float* q;
-    float* p0;
-    float* p1;
     double* part;
     double* result;
     unsigned* bar;
@@ -329,8 +328,10 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     int total = 0, outers = 0;
     double relres = 0.0;
     bool converged = false;
-    float* pcur = S.p0;
-    float* pnew = S.p1;
+    // (z, p) of every row, interleaved so that a neighbour's pair is one
+    // 8-byte load; zc is read by the products, zn receives the next pair
+    float2* zc = S.zp0;
+    float2* zn = S.zp1;
     for (int outer = 0; outer < S.max_outer; outer++) {
         // ---- true residual r64 = b - A x64 (FP64), inner start: z = M^-1 r, p = 0
         double acc[3] = {0.0, 0.0, 0.0};  // |r64|^2, |b|^2, r.z
@@ -357,13 +358,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const double ri = bi - (S.diag64[i] * S.x64[i] + s);
                 const float rf = (float)ri;
                 S.r[i] = rf;
-                pcur[i] = 0.f;
                 acc[0] += ri * ri;
                 acc[1] += bi * bi;
                 if (PREC == 0) {
                     const float zf = rf * S.inv_diag[i];
-                    S.z[i] = zf;
+                    zc[i] = make_float2(zf, 0.f);
                     acc[2] += (double)rf * (double)zf;
+                } else {
+                    zc[i].y = 0.f;
                 }
             }
         }
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const uint32_t i = __ldg(rowlist + kk);
                 const float* y = S.y;
                 const float zi = lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
-                S.z[i] = zi;
+                zc[i].x = zi;
                 rzp[0] += (double)S.r[i] * (double)zi;
             }
             double tz[1];
@@ -421,19 +423,21 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 for (uint32_t t = 0; t < T; t++) {
                     const uint4 c = __ldg(cols + 32 * t);
                     const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
-                    s0 = fmaf(w.x, fmaf(beta, pcur[c.x], S.z[c.x]), s0);
-                    s1 = fmaf(w.y, fmaf(beta, pcur[c.y], S.z[c.y]), s1);
-                    s0 = fmaf(w.z, fmaf(beta, pcur[c.z], S.z[c.z]), s0);
-                    s1 = fmaf(w.w, fmaf(beta, pcur[c.w], S.z[c.w]), s1);
+                    const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
+                    s0 = fmaf(w.x, fmaf(beta, a0.y, a0.x), s0);
+                    s1 = fmaf(w.y, fmaf(beta, a1.y, a1.x), s1);
+                    s0 = fmaf(w.z, fmaf(beta, a2.y, a2.x), s0);
+                    s1 = fmaf(w.w, fmaf(beta, a3.y, a3.x), s1);
                 }
                 float s = s0 + s1;
                 s += __shfl_xor_sync(0xffffffffu, s, 8);
                 s += __shfl_xor_sync(0xffffffffu, s, 16);
                 if (q == 0 && k < R) {
                     const uint32_t i = __ldg(rowlist + k);
-                    const float pn = fmaf(beta, pcur[i], S.z[i]);
+                    const float2 o = zc[i];
+                    const float pn = fmaf(beta, o.y, o.x);
                     const float qi = fmaf(S.diag32[i], pn, s);
-                    pnew[i] = pn;
+                    zn[i].y = pn;
                     S.q[i] = qi;
                     pq[0] += (double)pn * (double)qi;
                 }
@@ -448,12 +452,12 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             if (PREC == 0) {
                 for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                     const uint32_t i = __ldg(rowlist + kk);
-                    const float pn = pnew[i];
+                    const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
                     const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
                     const float zi = ri * S.inv_diag[i];
                     S.r[i] = ri;
-                    S.z[i] = zi;
+                    zn[i] = make_float2(zi, pn);
                     acc2[0] += (double)ri * (double)zi;
                     acc2[1] += (double)ri * (double)ri;
                 }
@@ -464,7 +468,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 float* rnew = S.ralt;
                 for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                     const uint32_t i = __ldg(rowlist + kk);
-                    const float pn = pnew[i];
+                    const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
                     const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
                     rnew[i] = ri;
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     const float* y = S.y;
                     const float zi =
                         lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
-                    S.z[i] = zi;
+                    zn[i].x = zi;
                     rzp[0] += (double)rnew[i] * (double)zi;
                 }
                 double trz[1];
@@ -496,9 +500,9 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             total++;
             beta = (float)(tot2[0] / rz);
             rz = tot2[0];
-            float* t = pcur;
-            pcur = pnew;
-            pnew = t;
+            float2* t = zc;
+            zc = zn;
+            zn = t;
             if (tot2[1] <= stop) break;
         }
         // the last inner iteration ended on a grid-wide reduction, so every
@@ -535,7 +539,8 @@ struct BatchSolveArgs {
     const float* diag32;
     const float* inv_diag;
     double* x64;
-    float *r, *z, *q, *p0, *p1;
+    float *r, *q;
+    float2 *zp0, *zp1;
     double* part;
     double* result;
     unsigned* bar;
@@ -652,8 +657,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
         rel[s] = 0.0;
     }
     int total = 0;
-    float* pcur = S.p0;
-    float* pnew = S.p1;
+    float2* zc = S.zp0;   // (z, p) per row, current and next
+    float2* zn = S.zp1;
     for (int outer = 0; outer < S.max_outer; outer++) {
         for (uint32_t t = threadIdx.x; t < 3 * ns; t += blockDim.x) acc[t] = 0.0;
         __syncthreads();
@@ -689,8 +694,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const float rf = (float)ri;
                 const float zf = rf * S.inv_diag[ii];
                 S.r[ii] = rf;
-                S.z[ii] = zf;
-                pcur[ii] = 0.f;
+                zc[ii] = make_float2(zf, 0.f);
                 v[0] = ri * ri;
                 v[1] = bi * bi;
                 v[2] = (double)rf * (double)zf;
@@ -748,10 +752,11 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                     for (uint32_t t = 0; t < T; t++) {
                         const uint4 c = __ldg(cols + 32 * t);
                         const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, rl, thr, pi, ii, c);
-                        sum = fmaf(w.x, fmaf(bs, pcur[c.x], S.z[c.x]), sum);
-                        sum1 = fmaf(w.y, fmaf(bs, pcur[c.y], S.z[c.y]), sum1);
-                        sum = fmaf(w.z, fmaf(bs, pcur[c.z], S.z[c.z]), sum);
-                        sum1 = fmaf(w.w, fmaf(bs, pcur[c.w], S.z[c.w]), sum1);
+                        const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
+                        sum = fmaf(w.x, fmaf(bs, a0.y, a0.x), sum);
+                        sum1 = fmaf(w.y, fmaf(bs, a1.y, a1.x), sum1);
+                        sum = fmaf(w.z, fmaf(bs, a2.y, a2.x), sum);
+                        sum1 = fmaf(w.w, fmaf(bs, a3.y, a3.x), sum1);
                     }
                 sum += sum1;
                 sum += __shfl_xor_sync(0xffffffffu, sum, 8);
@@ -759,9 +764,10 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const bool contrib = q == 0 && work;
                 double v[1] = {0.0};
                 if (contrib) {
-                    const float pn = fmaf(bs, pcur[ii], S.z[ii]);
+                    const float2 o = zc[ii];
+                    const float pn = fmaf(bs, o.y, o.x);
                     const float qi = fmaf(S.diag32[ii], pn, sum);
-                    pnew[ii] = pn;
+                    zn[ii].y = pn;
                     S.q[ii] = qi;
                     v[0] = (double)pn * (double)qi;
                 }
@@ -783,12 +789,12 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 if (contrib) {
                     const uint32_t i = __ldg(rowlist + kk);
                     const double al = alpha[s];
-                    const float pn = pnew[i];
+                    const float pn = zn[i].y;
                     S.x64[i] += al * (double)pn;
                     const float ri = fmaf(-(float)al, S.q[i], S.r[i]);
                     const float zi = ri * S.inv_diag[i];
                     S.r[i] = ri;
-                    S.z[i] = zi;
+                    zn[i] = make_float2(zi, pn);
                     v[0] = (double)ri * (double)zi;
                     v[1] = (double)ri * (double)ri;
                 }
@@ -810,9 +816,9 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             }
             __syncthreads();
             total++;
-            float* t = pcur;
-            pcur = pnew;
-            pnew = t;
+            float2* t = zc;
+            zc = zn;
+            zn = t;
             if (n_active == 0) break;
         }
     }
@@ -1101,10 +1107,9 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.b64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.x64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.r, (size_t)cap * sizeof(float));
-    ok &= al((void**)&w.z, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.zp[0], (size_t)cap * sizeof(float2));
+    ok &= al((void**)&w.zp[1], (size_t)cap * sizeof(float2));
     ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
-    ok &= al((void**)&w.p[0], (size_t)cap * sizeof(float));
-    ok &= al((void**)&w.p[1], (size_t)cap * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.y, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.ralt, (size_t)cap * sizeof(float));
@@ -1269,10 +1274,9 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.b64 = w.b64;
     S.x64 = w.x64;
     S.r = w.r;
-    S.z = w.z;
+    S.zp0 = w.zp[0];
+    S.zp1 = w.zp[1];
     S.q = w.q;
-    S.p0 = w.p[0];
-    S.p1 = w.p[1];
     S.part = w.part;
     S.result = w.result;
     S.bar = w.bar;
@@ -1313,10 +1317,9 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.inv_diag = w.inv_diag;
         B.x64 = w.x64;
         B.r = w.r;
-        B.z = w.z;
+        B.zp0 = w.zp[0];
+        B.zp1 = w.zp[1];
         B.q = w.q;
-        B.p0 = w.p[0];
-        B.p1 = w.p[1];
         B.part = w.bpart;
         B.result = w.bresult;
         B.bar = w.bar;
@@ -1398,7 +1401,7 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
-                  w.r,    w.z,    w.q,    w.p[0],   w.p[1],   w.part,     w.result, w.bar,
+                  w.r,    w.zp[0], w.zp[1], w.q,    w.part,     w.result, w.bar,
                   w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
                   w.id_snap, w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
                   w.scene_relres};

@@ -48,7 +48,8 @@ struct PpeWork {
     float* inv_diag = nullptr;
     double* b64 = nullptr;
     double* x64 = nullptr;
-    float *r = nullptr, *z = nullptr, *q = nullptr, *p[2] = {nullptr, nullptr};
+    float *r = nullptr, *q = nullptr;
+    float2* zp[2] = {nullptr, nullptr};  // (z, p) per row: current and next
     double* part = nullptr;            // blocks * PPE_PARTS
     double* result = nullptr;          // PPE_PARTS grid totals
     uint32_t* rowlist = nullptr;       // non-Dirichlet rows in particle order
