@@ -78,8 +78,9 @@ __global__ void __launch_bounds__(256) k_lp_stencil(LpSystem S, uint32_t* __rest
     uint32_t* out = scols + (size_t)i * LP_GW;
     const uint32_t c = __ldg(S.cell + i);
     const int rows = link_rows(S.g);
+    const CellNear nr = cell_near(S.g, c, pi.x, pi.y, pi.z, S.P.rzero);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(S.g, S.cell_start, c, row);
+        const RowRange rg = link_row_near(S.g, S.cell_start, c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             bool hit = false;

@@ -156,4 +156,59 @@ __device__ __forceinline__ RowRange link_row(const Grid& g, const uint32_t* __re
 
 __device__ __forceinline__ int link_rows(const Grid& g) { return g.dim == 3 ? 9 : 3; }
 
+// Culling of the linked cells: the distances from a particle to the faces of
+// its own cell bound the distance to any particle of a neighbouring cell.  A
+// row (or its first or last cell) farther than re plus a margin cannot hold
+// a particle that passes a stage's distance test, so leaving it out removes
+// only candidates that contribute nothing: the remaining candidates keep the
+// reference's order and every sum is unchanged.  The margin (1e-4 of a cell)
+// covers the rounding of the cell assignment and of the face positions.
+struct CellNear {
+    float xl, xr, yl, yr, zl, zr;  // to the low / high face along each axis
+    float re2;                     // (re + margin)^2
+};
+
+__device__ __forceinline__ CellNear cell_near(const Grid& g, uint32_t c, float x, float y, float z, float re) {
+    const uint32_t cz = c / g.sheet, rem = c - cz * g.sheet;
+    const uint32_t cy = rem / g.cdx, cx = rem - cy * g.cdx;
+    const float x0 = g.left + g.cell_size * (float)cx;
+    const float y0 = g.back + g.cell_size * (float)cy;
+    const float z0 = g.bottom + g.cell_size * (float)cz;
+    CellNear n;
+    n.xl = fmaxf(x - x0, 0.f);
+    n.xr = fmaxf(x0 + g.cell_size - x, 0.f);
+    n.yl = fmaxf(y - y0, 0.f);
+    n.yr = fmaxf(y0 + g.cell_size - y, 0.f);
+    n.zl = fmaxf(z - z0, 0.f);
+    n.zr = fmaxf(z0 + g.cell_size - z, 0.f);
+    const float r = re + 1e-4f * g.cell_size;
+    n.re2 = r * r;
+    return n;
+}
+
+// link_row restricted to the cells that can hold a particle within re
+__device__ __forceinline__ RowRange link_row_near(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
+                                                  int row, const CellNear& n) {
+    int dz, dy;
+    if (g.dim == 3) { dz = row / 3 - 1; dy = row % 3 - 1; }
+    else { dz = 0; dy = row - 1; }
+    float d2 = 0.f;
+    if (dy < 0) d2 += n.yl * n.yl;
+    else if (dy > 0) d2 += n.yr * n.yr;
+    if (dz < 0) d2 += n.zl * n.zl;
+    else if (dz > 0) d2 += n.zr * n.zr;
+    RowRange r{0u, 0u};
+    if (d2 >= n.re2) return r;
+    const bool wa = d2 + n.xl * n.xl < n.re2, wb = d2 + n.xr * n.xr < n.re2;
+    const uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
+    const uint32_t a = c0 - 1u, b = c0 + 1u;
+    const bool va = wa && a < g.ncells, v0 = c0 < g.ncells, vb = wb && b < g.ncells;
+    uint32_t first, last;
+    if (va) first = a; else if (v0) first = c0; else if (vb) first = b; else return r;
+    if (vb) last = b; else if (v0) last = c0; else last = a;
+    r.lo = __ldg(cell_start + first);
+    r.hi = __ldg(cell_start + last + 1u);
+    return r;
+}
+
 }  // namespace mpsb

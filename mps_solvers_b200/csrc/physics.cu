@@ -256,8 +256,9 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     const float re = P.rlap, thr = P.rlap_thr;
     float ax = 0.f, ay = 0.f, az = 0.f;
     const int rows = link_rows(L.g);
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -325,8 +326,9 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     const Local L = local_of<BT>(a, i);
     const Phys P = phys_of<BT>(a, L.s);
     const int rows = link_rows(L.g);
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, P.col_dis);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -380,8 +382,9 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     const float re = P.rzero, thr = P.rzero_thr;
     float acc = 0.f;
     const int rows = link_rows(L.g);
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float w = 0.f;
@@ -418,10 +421,11 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const Phys P = phys_of<BT>(a, L.s);
     const int rows = link_rows(L.g);
     const float r02 = P.rzero2;
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, P.rzero);
     // p_hat: a minimum, independent of order
     float hat = press[i];
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             if (j < rg.hi) {
@@ -443,7 +447,7 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const bool skip_dummy = a.semi != 0;
     float gx = 0.f, gy = 0.f, gz = 0.f;
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
@@ -692,8 +696,9 @@ __global__ void k_lambda(StageArgs a, const unsigned long long* best, float* out
     const Phys P = phys_of(a, L.s);
     float lam = 0.f;
     const int rows = link_rows(L.g);
+    const CellNear nr = cell_near(L.g, L.c, pt.x, pt.y, pt.z, P.rzero);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t j = rg.lo; j < rg.hi; j++) {
             if (j == t) continue;
             const float4 pj = a.cur.pos[j];

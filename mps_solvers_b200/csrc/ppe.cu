@@ -190,8 +190,9 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     double diag = 0.0;
     const int rows = link_rows(L.g);
     const uint32_t lt = (1u << lane) - 1u;
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             bool app = false;
