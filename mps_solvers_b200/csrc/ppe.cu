@@ -133,6 +133,7 @@ __device__ bool grid_reduce(const double (&v)[K], double* part, double* result, 
 struct AsmArgs {
     StageArgs a;
     uint32_t* cols;
+    float* wrm;              // the entries' weights, beside cols
     uint32_t* rlen;
     double* diag64;
     float* diag32;
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const float re = P.rlap, thr = P.rlap_thr;
     const double bthr = beta * n0;
     uint32_t* cols = A.cols + (size_t)i * PPE_W;
+    float* wrow = A.wrm + (size_t)i * PPE_W;
     uint32_t count = 0;
     double diag = 0.0;
     const int rows = link_rows(L.g);
@@ -212,7 +214,10 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
             const uint32_t m = __ballot_sync(0xffffffffu, app);
             if (app) {
                 const uint32_t k = count + __popc(m & lt);
-                if (k < PPE_W) cols[k] = j;
+                if (k < PPE_W) {
+                    cols[k] = j;
+                    wrow[k] = w;
+                }
             }
             count += __popc(m);
         }
@@ -936,46 +941,43 @@ __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__
     width[s] = SELL_C * ((m + 15u) & ~15u);
 }
 
-// Columns, and their weights w(r; rlap) computed from the positions by the
-// function the assembly used for the diagonal (0 on padding entries, whose
-// column is the row itself).
-template <bool EX>
-__global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm,
+// Columns and weights of the assembly, repacked (padding: the row's own
+// index, weight 0).  One warp per slice: in chunk t, lane L = r + 8q moves
+// the 4 entries 16t + 4q .. 16t + 4q + 3 of row r as one 16-byte load from
+// the row-major scratch and one 16-byte store, so the warp writes its 512
+// bytes contiguously.
+__global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ cols_rm, const float* __restrict__ w_rm,
                                                    const uint32_t* __restrict__ rlen, const uint32_t* __restrict__ rowlist,
                                                    const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
-                                                   uint32_t* __restrict__ scols, float* __restrict__ sw,
-                                                   const float4* __restrict__ pos, Phys P,
-                                                   const Phys* __restrict__ phys, const uint32_t* __restrict__ row_scene) {
+                                                   uint32_t* __restrict__ scols, float* __restrict__ sw) {
     const uint32_t R = *nrows;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // row position in the list
-    const uint32_t slice = k / SELL_C, r = k % SELL_C;
+    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31, r = lane & 7, q = lane >> 3;
     if (slice >= (R + SELL_C - 1) / SELL_C) return;
     const uint32_t base = off[slice];
-    const uint32_t W = (off[slice + 1] - base) / SELL_C;
+    const uint32_t T = (off[slice + 1] - base) >> 7;  // chunks of 16 entries per row
+    const uint32_t k = slice * SELL_C + r;
     const bool has = k < R;
     const uint32_t i = has ? rowlist[k] : 0u;
     const uint32_t len = has ? rlen[i] : 0u;
-    const uint32_t* rc = cols_rm + (size_t)i * PPE_W;
-    float rl = P.rlap, thr = P.rlap_thr;
-    if (phys && has) {
-        rl = phys[row_scene[k]].rlap;
-        thr = phys[row_scene[k]].rlap_thr;
-    }
-    const float4 pi = pos[i];
-    for (uint32_t e = 0; e < W; e++) {
-        const bool real = e < len;
-        const uint32_t j = real ? rc[e] : i;
-        float w = 0.f;
-        if (real) {
-            const float4 pj = pos[j];
-            const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-            const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-            w = rr < thr ? weight_rr<EX>(rl, rr) : 0.f;
+    const uint4* rc = reinterpret_cast<const uint4*>(cols_rm + (size_t)i * PPE_W);
+    const float4* rw = reinterpret_cast<const float4*>(w_rm + (size_t)i * PPE_W);
+    uint4* dc = reinterpret_cast<uint4*>(scols + base) + lane;
+    float4* dw = reinterpret_cast<float4*>(sw + base) + lane;
+    for (uint32_t t = 0; t < T; t++) {
+        const uint32_t e = 16u * t + 4u * q;
+        uint4 c = make_uint4(i, i, i, i);
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < len) {
+            const uint4 lc = rc[e >> 2];
+            const float4 lw = rw[e >> 2];
+            c.x = lc.x; w.x = lw.x;
+            if (e + 1 < len) { c.y = lc.y; w.y = lw.y; }
+            if (e + 2 < len) { c.z = lc.z; w.z = lw.z; }
+            if (e + 3 < len) { c.w = lc.w; w.w = lw.w; }
         }
-        // entry e of row r: chunk e / 16, lane r + 8 ((e / 4) % 4), slot e % 4
-        const uint32_t at = base + (((e >> 4) * 32u + r + SELL_C * ((e >> 2) & 3u)) << 2) + (e & 3u);
-        scols[at] = j;
-        sw[at] = w;
+        dc[32 * t] = c;
+        dw[32 * t] = w;
     }
 }
 
@@ -1101,6 +1103,7 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     };
     bool ok = true;
     ok &= al((void**)&w.cols, (size_t)cap * PPE_W * sizeof(uint32_t));
+    ok &= al((void**)&w.wrm, (size_t)cap * PPE_W * sizeof(float));
     ok &= al((void**)&w.rlen, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.diag64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.diag32, (size_t)cap * sizeof(float));
@@ -1179,6 +1182,7 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     AsmArgs A;
     A.a = a;
     A.cols = w.cols;
+    A.wrm = w.wrm;
     A.rlen = w.rlen;
     A.diag64 = w.diag64;
     A.diag32 = w.diag32;
@@ -1218,16 +1222,8 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
     k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
     launch_scan_exclusive(w.sell_off, maxslices + 1, st);
-    {
-        const Phys* phys = a.batch.n ? a.batch.phys : nullptr;
-        const uint32_t nb = blocks_for(maxslices * SELL_C, 256);
-        if (a.exact)
-            k_sell_pack<true><<<nb, 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows, w.sell_off, w.sell_cols,
-                                                  w.sell_w, a.cur.pos, a.P, phys, w.row_scene);
-        else
-            k_sell_pack<false><<<nb, 256, 0, st>>>(w.cols, w.rlen, w.rowlist, w.nrows, w.sell_off, w.sell_cols,
-                                                   w.sell_w, a.cur.pos, a.P, phys, w.row_scene);
-    }
+    k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.wrm, w.rlen, w.rowlist, w.nrows,
+                                                                  w.sell_off, w.sell_cols, w.sell_w);
     // the state this system was assembled from
     cudaMemcpyAsync(w.pos_snap, a.cur.pos, (size_t)cap * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
@@ -1401,7 +1397,7 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 }
 
 void ppe_free(PpeWork& w) {
-    void* ps[] = {w.cols, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
+    void* ps[] = {w.cols, w.wrm, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.zp[0], w.zp[1], w.q,    w.part,     w.result, w.bar,
                   w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
                   w.id_snap, w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,

@@ -42,6 +42,7 @@ struct PpeWork {
     int threads = PPE_THREADS;         // its block size (1024 / threads blocks per SM)
     int sms = 0;
     uint32_t* cols = nullptr;          // cap * PPE_W
+    float* wrm = nullptr;              // their weights
     uint32_t* rlen = nullptr;          // off-diagonal count, PPE_DIRICHLET for Dirichlet rows
     double* diag64 = nullptr;
     float* diag32 = nullptr;
