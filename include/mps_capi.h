@@ -88,7 +88,10 @@ typedef struct {
                             true-residual checks (0: 1000)                   */
     int precond;         /* MPS_PRECOND_*                                     */
     uint32_t capacity;   /* particle capacity (0: the scene's np)             */
-    uint32_t reserved[8];
+    int cg_inner_digits; /* PPE: the most decimal digits one FP32 inner solve
+                            may reduce the residual by before the next FP64
+                            check (0: 4)                                      */
+    uint32_t reserved[7];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

@@ -244,6 +244,7 @@ extern "C" void mps_default_options(mps_options* o) {
     o->cg_tol = 1e-8;
     o->cg_max_iter = 10000;
     o->cg_check_every = 1000;
+    o->cg_inner_digits = 4;
     o->precond = MPS_PRECOND_DIAGONAL;
     o->capacity = 0;
 }
@@ -482,6 +483,7 @@ static mps_status create_common(mps_handle** out, const mps_options* opt) {
     else mps_default_options(&h->opt);
     if (h->opt.cg_max_iter <= 0) h->opt.cg_max_iter = 10000;
     if (h->opt.cg_check_every <= 0) h->opt.cg_check_every = 1000;
+    if (h->opt.cg_inner_digits <= 0) h->opt.cg_inner_digits = 4;
     if (h->opt.cg_tol <= 0) h->opt.cg_tol = 1e-8;
     *out = h;
     return MPS_OK;

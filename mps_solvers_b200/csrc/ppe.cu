@@ -272,6 +272,7 @@ struct SolveArgs {
     float* ralt;
     Scalars* sc;
     double tol;
+    double eta_min;   // smallest inner reduction asked of one FP32 solve
     int max_iter;
     int inner_cap;
     int max_outer;
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         }
         // inner target |r| <= eta |r64|
         double eta = 0.3 * S.tol / relres;
-        if (eta < 1e-4) eta = 1e-4;
+        if (eta < S.eta_min) eta = S.eta_min;
         if (eta > 0.5) eta = 0.5;
         const double stop = eta * eta * rr64;
         double rz = tot[2];
@@ -556,6 +557,7 @@ struct BatchSolveArgs {
     double* relres;
     uint32_t ns;
     double tol;
+    double eta_min;
     int max_iter, inner_cap, max_outer;
 };
 
@@ -719,7 +721,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 active[s] = 0;
             } else {
                 double eta = 0.3 * S.tol / relres;
-                if (eta < 1e-4) eta = 1e-4;
+                if (eta < S.eta_min) eta = S.eta_min;
                 if (eta > 0.5) eta = 0.5;
                 active[s] = 1;
                 rz[s] = acc[2 * ns + s];
@@ -1297,6 +1299,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.tol = opt.cg_tol;
     S.max_iter = opt.cg_max_iter;
     S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
+    S.eta_min = pow(10.0, -(double)(opt.cg_inner_digits > 0 ? opt.cg_inner_digits : 4));
     S.max_outer = 40;
     if (a.batch.n) {
         BatchSolveArgs B;
@@ -1329,6 +1332,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.max_iter = S.max_iter;
         B.inner_cap = S.inner_cap;
         B.max_outer = S.max_outer;
+        B.eta_min = S.eta_min;
         void* bargs[] = {&B};
         const void* bfn = w.stored_weights
                               ? (a.exact ? (const void*)k_ppe_solve_batch<true, true>
