@@ -91,7 +91,9 @@ typedef struct {
     int cg_inner_digits; /* PPE: the most decimal digits one FP32 inner solve
                             may reduce the residual by before the next FP64
                             check (0: 4)                                      */
-    uint32_t reserved[7];
+    int ppe_pipelined;   /* PPE: 1 = pipelined single-reduction PCG (diagonal
+                            scaling, single scenes); mps_autotune may change it */
+    uint32_t reserved[6];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after
@@ -342,18 +344,20 @@ mps_status mps_surface_case_table(uint8_t ntri[256], int8_t tri[256 * 16]);
  * CUDA events over `steps` steps per candidate, the block size of the
  * particle-stage kernels (64, 128, 256 threads) and, for the semi-implicit
  * PPE, the persistent grid's shape (1024, 512 or 256 threads per block at
- * 1024 threads per SM) and its SpMV form (weights stored by the assembly,
- * or recomputed from the positions in every product), and keeps the
+ * 1024 threads per SM) and the solver's form (weights stored by the
+ * assembly, weights recomputed from the positions in every product, or
+ * stored weights with the pipelined single-reduction PCG), and keeps the
  * fastest of each.  The scene advances by the steps taken (call it during
  * warm-up). */
 typedef struct mps_tune_report {
     int stage_threads;         /* chosen */
     int ppe_threads;           /* chosen */
     int ppe_stored_weights;    /* chosen: 1 stored, 0 recomputed */
+    int ppe_pipelined;         /* chosen: 1 pipelined PCG */
     float stage_ms[3];         /* visc + collision + pnd + dash per step at 64, 128, 256 */
-    /* PPE solve ms per PCG iteration: [0..2] stored weights at 1024, 512,
-     * 256 threads per block, [3..5] recomputed weights (-1: not held) */
-    float ppe_ms_per_iter[6];
+    /* PPE solve ms per step: [3 f + t] for form f (0 stored, 1 recomputed,
+     * 2 pipelined) at 1024, 512, 256 threads per block (-1: not run) */
+    float ppe_ms[9];
     uint32_t reserved[4];
 } mps_tune_report;
 mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* report);

@@ -49,7 +49,7 @@ class mps_options(C.Structure):
     _fields_ = [("method", C.c_int), ("arith", C.c_int), ("device", C.c_int),
                 ("use_graph", C.c_int), ("cg_tol", C.c_double), ("cg_max_iter", C.c_int),
                 ("cg_check_every", C.c_int), ("precond", C.c_int), ("capacity", C.c_uint32),
-                ("cg_inner_digits", C.c_int), ("reserved", C.c_uint32 * 7)]
+                ("cg_inner_digits", C.c_int), ("ppe_pipelined", C.c_int), ("reserved", C.c_uint32 * 6)]
 
 
 class mps_params(C.Structure):
@@ -85,7 +85,7 @@ class mps_scene_info(C.Structure):
 
 class mps_tune_report(C.Structure):
     _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("ppe_stored_weights", C.c_int),
-                ("stage_ms", C.c_float * 3), ("ppe_ms_per_iter", C.c_float * 6),
+                ("ppe_pipelined", C.c_int), ("stage_ms", C.c_float * 3), ("ppe_ms", C.c_float * 9),
                 ("reserved", C.c_uint32 * 4)]
 
 
@@ -419,8 +419,8 @@ class Simulation:
         r = mps_tune_report()
         self._check(lib().mps_autotune(self.h, steps, C.byref(r)))
         return {"stage_threads": r.stage_threads, "ppe_threads": r.ppe_threads,
-                "ppe_stored_weights": r.ppe_stored_weights, "stage_ms": list(r.stage_ms),
-                "ppe_ms_per_iter": list(r.ppe_ms_per_iter)}
+                "ppe_stored_weights": r.ppe_stored_weights, "ppe_pipelined": r.ppe_pipelined,
+                "stage_ms": list(r.stage_ms), "ppe_ms": list(r.ppe_ms)}
 
     # ---- free surface (marching cubes)
     def surface_setup(self, shape, origin, spacing, max_triangles: int):

@@ -468,6 +468,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
         int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
+        h->ppe.pipelined = h->opt.ppe_pipelined != 0;
         if (h->opt.precond == MPS_PRECOND_LEARNED) {
             e = ppe_enable_learned(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
@@ -1283,10 +1284,11 @@ extern "C" mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage
 
 // Autotuner: the block size of the particle-stage kernels (64, 128, 256),
 // and for the persistent PPE solver the grid shape (1024, 512 or 256
-// threads per block, 1024 threads per SM) and the SpMV form (stored weights
-// or weights recomputed from positions), each timed with CUDA events over
-// `steps` steps of the handle's own scene; the fastest is kept.  The scene
-// advances by the steps taken.
+// threads per block, 1024 threads per SM) and its form (stored weights,
+// weights recomputed from positions, or stored weights with the pipelined
+// single-reduction PCG), each timed with CUDA events over `steps` steps of
+// the handle's own scene; the fastest is kept.  The scene advances by the
+// steps taken.
 extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* rep) {
     if (!h || steps < 1) return MPS_ERR_INVALID;
     CK(cudaSetDevice(h->dev));
@@ -1313,40 +1315,46 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
     r.stage_threads = best_t;
     r.ppe_threads = h->ppe.threads;
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        // forms: 0 stored weights, 1 recomputed weights, 2 stored weights
+        // with the pipelined (single-reduction) PCG; the learned and batched
+        // solvers have no pipelined form
         const int ppe_cand[3] = {1024, 512, 256};
+        const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
+        const int nforms = (learned || h->nscenes) ? 2 : 3;
         best = 1e300;
         int best_p = h->ppe.threads;
-        bool best_sw = h->ppe.stored_weights;
-        for (int c = 0; c < 6; c++) {
-            const bool sw = c < 3;
+        bool best_sw = h->ppe.stored_weights, best_pipe = h->ppe.pipelined;
+        for (int c = 0; c < 3 * nforms; c++) {
+            const int form = c / 3;
             if (ppe_set_threads(h->ppe, ppe_cand[c % 3]) != MPS_OK) {
-                r.ppe_ms_per_iter[c] = -1.f;  // the device cannot hold this shape
+                r.ppe_ms[c] = -1.f;  // the device cannot hold this shape
                 continue;
             }
-            h->ppe.stored_weights = sw;
+            h->ppe.stored_weights = form != 1;
+            h->ppe.pipelined = form == 2;
             drop_graphs(h);
             double tot = 0.0;
-            long iters = 0;
             for (int k = 0; k < steps; k++) {
                 mps_status st = mps_profile_steps(h, 1, ms.data(), 32, &nst);
                 if (st != MPS_OK) return st;
-                Scalars sc;
-                if (read_status(h, &sc) == MPS_ERR_CUDA) return MPS_ERR_CUDA;
                 tot += ms[ST_PPE_SOLVE];
-                iters += sc.cg_iters > 0 ? sc.cg_iters : 1;
             }
-            const double t = tot / (double)iters;
-            r.ppe_ms_per_iter[c] = (float)t;
+            const double t = tot / steps;
+            r.ppe_ms[c] = (float)t;
             if (t < best) {
                 best = t;
                 best_p = ppe_cand[c % 3];
-                best_sw = sw;
+                best_sw = form != 1;
+                best_pipe = form == 2;
             }
         }
+        for (int c = 3 * nforms; c < 9; c++) r.ppe_ms[c] = -1.f;
         ppe_set_threads(h->ppe, best_p);
         h->ppe.stored_weights = best_sw;
+        h->ppe.pipelined = best_pipe;
         r.ppe_threads = best_p;
         r.ppe_stored_weights = best_sw ? 1 : 0;
+        r.ppe_pipelined = best_pipe ? 1 : 0;
     }
     drop_graphs(h);
     if (rep) *rep = r;

@@ -523,6 +523,216 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     }
 }
 
+// ---------------------------------------------------------------- pipelined solve
+// Diagonally scaled PCG in the pipelined form of Ghysels and Vanroose (2014)
+// with the recurrences of Chronopoulos and Gear: per iteration one product
+// n = A m (m = M w) and one grid-wide reduction of (r.u, w.u, r.r), where
+// the standard form needs two reductions.  Algebraically the same iterates
+// as PCG; in floating point the recursive residual drifts more, which the
+// FP64 true-residual passes absorb (the solve still ends on
+// |b - A x| <= tol |b| in FP64).  The neighbours' m_j = M w_j are read from a
+// double buffer written by the previous iteration, one 4-byte load each.
+struct PipeArgs {
+    const uint32_t* rowlist;
+    const uint32_t* nrows;
+    const uint32_t* off;
+    const uint32_t* scols;
+    const float* sw;
+    const float4* pos;
+    float rlap, rlap_thr;
+    const double* b64;
+    const double* diag64;
+    const float* diag32;
+    const float* inv_diag;
+    double* x64;
+    float *r, *u, *w, *z, *q, *s, *p;
+    float *m0, *m1;
+    double* part;
+    double* result;
+    unsigned* bar;
+    Scalars* sc;
+    double tol, eta_min;
+    int max_iter, inner_cap, max_outer;
+};
+
+template <bool EX, bool SW>
+__global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
+    const uint32_t R = *S.nrows;
+    const uint32_t nslices = (R + SELL_C - 1) / SELL_C;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t rsub = lane & 7, q = lane >> 3;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t* __restrict__ rowlist = S.rowlist;
+    int total = 0, outers = 0;
+    double relres = 0.0;
+    bool converged = false;
+    float* mc = S.m0;   // m = M w read by this iteration's product
+    float* mn = S.m1;   // m of the next iteration
+    for (int outer = 0; outer < S.max_outer; outer++) {
+        // ---- FP64 true residual; r, u = M r
+        double acc[2] = {0.0, 0.0};  // |r64|^2, |b|^2
+        for (uint32_t sl = gw; sl < nslices; sl += nw) {
+            const uint32_t k = sl * SELL_C + rsub;
+            const uint32_t base = __ldg(S.off + sl);
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+            const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+            const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
+            const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
+            const float4 pi = __ldg(S.pos + ii);
+            double sum = 0.0;
+            for (uint32_t t = 0; t < T; t++) {
+                const uint4 c = __ldg(cols + 32 * t);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                sum += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
+                       (double)w.w * S.x64[c.w];
+            }
+            sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+            if (q == 0 && k < R) {
+                const double bi = S.b64[ii];
+                const double ri = bi - (S.diag64[ii] * S.x64[ii] + sum);
+                const float rf = (float)ri;
+                S.r[ii] = rf;
+                S.u[ii] = rf * S.inv_diag[ii];
+                acc[0] += ri * ri;
+                acc[1] += bi * bi;
+            }
+        }
+        double tot[2];
+        if (!grid_reduce<2>(acc, S.part, S.result, S.bar, S.sc, tot)) return;
+        outers++;
+        const double rr64 = tot[0], bb = tot[1];
+        relres = bb > 0.0 ? sqrt(rr64 / bb) : 0.0;
+        if (relres <= S.tol) {
+            converged = true;
+            break;
+        }
+        if (total >= S.max_iter) break;
+        // ---- w = A u, m = M w; gamma = r.u, delta = w.u; z = q = s = p = 0
+        double g0[3] = {0.0, 0.0, 0.0};
+        for (uint32_t sl = gw; sl < nslices; sl += nw) {
+            const uint32_t k = sl * SELL_C + rsub;
+            const uint32_t base = __ldg(S.off + sl);
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+            const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+            const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
+            const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
+            const float4 pi = __ldg(S.pos + ii);
+            float s0 = 0.f, s1 = 0.f;
+            for (uint32_t t = 0; t < T; t++) {
+                const uint4 c = __ldg(cols + 32 * t);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                s0 = fmaf(w.x, S.u[c.x], s0);
+                s1 = fmaf(w.y, S.u[c.y], s1);
+                s0 = fmaf(w.z, S.u[c.z], s0);
+                s1 = fmaf(w.w, S.u[c.w], s1);
+            }
+            float sum = s0 + s1;
+            sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+            if (q == 0 && k < R) {
+                const float ui = S.u[ii];
+                const float wi = fmaf(S.diag32[ii], ui, sum);
+                S.w[ii] = wi;
+                mc[ii] = wi * S.inv_diag[ii];
+                S.z[ii] = 0.f;
+                S.q[ii] = 0.f;
+                S.s[ii] = 0.f;
+                S.p[ii] = 0.f;
+                const float ri = S.r[ii];
+                g0[0] += (double)ri * (double)ui;
+                g0[1] += (double)wi * (double)ui;
+                g0[2] += (double)ri * (double)ri;
+            }
+        }
+        double gt[3];
+        if (!grid_reduce<3>(g0, S.part, S.result, S.bar, S.sc, gt)) return;
+        double eta = 0.3 * S.tol / relres;
+        if (eta < S.eta_min) eta = S.eta_min;
+        if (eta > 0.5) eta = 0.5;
+        const double stop = eta * eta * rr64;
+        double gamma = gt[0], delta = gt[1], gamma_old = 1.0, alpha_old = 1.0;
+        for (int it = 0; it < S.inner_cap && total < S.max_iter; it++) {
+            double beta = 0.0, alpha;
+            if (it == 0) {
+                alpha = gamma / delta;
+            } else {
+                beta = gamma / gamma_old;
+                alpha = gamma / (delta - beta * gamma / alpha_old);
+            }
+            const float bf = (float)beta, af = (float)alpha;
+            // ---- n = A m; z, q, s, p, x, r, u, w updates; r.u, w.u, r.r
+            double g[3] = {0.0, 0.0, 0.0};
+            for (uint32_t sl = gw; sl < nslices; sl += nw) {
+                const uint32_t k = sl * SELL_C + rsub;
+                const uint32_t base = __ldg(S.off + sl);
+                const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+                const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+                const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
+                const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
+                const float4 pi = __ldg(S.pos + ii);
+                float s0 = 0.f, s1 = 0.f;
+#pragma unroll 2
+                for (uint32_t t = 0; t < T; t++) {
+                    const uint4 c = __ldg(cols + 32 * t);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                    s0 = fmaf(w.x, mc[c.x], s0);
+                    s1 = fmaf(w.y, mc[c.y], s1);
+                    s0 = fmaf(w.z, mc[c.z], s0);
+                    s1 = fmaf(w.w, mc[c.w], s1);
+                }
+                float sum = s0 + s1;
+                sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+                if (q == 0 && k < R) {
+                    const float mi = mc[ii];
+                    const float ni = fmaf(S.diag32[ii], mi, sum);
+                    const float zi = fmaf(bf, S.z[ii], ni);
+                    const float qi = fmaf(bf, S.q[ii], mi);
+                    const float wi0 = S.w[ii];
+                    const float si = fmaf(bf, S.s[ii], wi0);
+                    const float pin = fmaf(bf, S.p[ii], S.u[ii]);
+                    S.x64[ii] += alpha * (double)pin;
+                    const float ri = fmaf(-af, si, S.r[ii]);
+                    const float ui = fmaf(-af, qi, S.u[ii]);
+                    const float wi = fmaf(-af, zi, wi0);
+                    S.z[ii] = zi;
+                    S.q[ii] = qi;
+                    S.s[ii] = si;
+                    S.p[ii] = pin;
+                    S.r[ii] = ri;
+                    S.u[ii] = ui;
+                    S.w[ii] = wi;
+                    mn[ii] = wi * S.inv_diag[ii];
+                    g[0] += (double)ri * (double)ui;
+                    g[1] += (double)wi * (double)ui;
+                    g[2] += (double)ri * (double)ri;
+                }
+            }
+            double gg[3];
+            if (!grid_reduce<3>(g, S.part, S.result, S.bar, S.sc, gg)) return;
+            total++;
+            gamma_old = gamma;
+            alpha_old = alpha;
+            gamma = gg[0];
+            delta = gg[1];
+            float* t = mc;
+            mc = mn;
+            mn = t;
+            if (gg[2] <= stop) break;
+        }
+        // the last iteration ended on a grid-wide reduction, so every x64
+        // update is visible to the residual pass of the next round
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S.sc->cg_iters = total;
+        S.sc->cg_outer = outers;
+        S.sc->cg_relres = relres;
+        if (!converged) atomicOr(&S.sc->err, ERR_CG_NOT_CONVERGED);
+    }
+}
+
 // ---------------------------------------------------------------- batched solve
 // The scenes of a batch in one persistent launch.  Each scene runs its own
 // diagonally scaled PCG (its own alpha, beta, inner stop and FP64 true
@@ -1091,7 +1301,9 @@ static std::vector<const void*> solve_kernels() {
             (const void*)k_ppe_solve<true, 0, false>,   (const void*)k_ppe_solve<false, 0, false>,
             (const void*)k_ppe_solve<true, 1, false>,   (const void*)k_ppe_solve<false, 1, false>,
             (const void*)k_ppe_solve_batch<true, true>, (const void*)k_ppe_solve_batch<false, true>,
-            (const void*)k_ppe_solve_batch<true, false>, (const void*)k_ppe_solve_batch<false, false>};
+            (const void*)k_ppe_solve_batch<true, false>, (const void*)k_ppe_solve_batch<false, false>,
+            (const void*)k_ppe_solve_pipe<true, true>,  (const void*)k_ppe_solve_pipe<false, true>,
+            (const void*)k_ppe_solve_pipe<true, false>, (const void*)k_ppe_solve_pipe<false, false>};
 }
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_params& prm, cudaStream_t st,
@@ -1113,6 +1325,8 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.b64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.x64, (size_t)cap * sizeof(double));
     ok &= al((void**)&w.r, (size_t)cap * sizeof(float));
+    for (float** v : {&w.pu, &w.pw, &w.pz, &w.pq, &w.ps, &w.pp, &w.pm[0], &w.pm[1]})
+        ok &= al((void**)v, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.zp[0], (size_t)cap * sizeof(float2));
     ok &= al((void**)&w.zp[1], (size_t)cap * sizeof(float2));
     ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
@@ -1343,8 +1557,49 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
-    void* args[] = {&S};
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+    if (w.pipelined && !learned) {
+        PipeArgs Pa;
+        Pa.rowlist = w.rowlist;
+        Pa.nrows = w.nrows;
+        Pa.off = w.sell_off;
+        Pa.scols = w.sell_cols;
+        Pa.sw = w.sell_w;
+        Pa.pos = a.cur.pos;
+        Pa.rlap = a.P.rlap;
+        Pa.rlap_thr = a.P.rlap_thr;
+        Pa.b64 = w.b64;
+        Pa.diag64 = w.diag64;
+        Pa.diag32 = w.diag32;
+        Pa.inv_diag = w.inv_diag;
+        Pa.x64 = w.x64;
+        Pa.r = w.r;
+        Pa.u = w.pu;
+        Pa.w = w.pw;
+        Pa.z = w.pz;
+        Pa.q = w.pq;
+        Pa.s = w.ps;
+        Pa.p = w.pp;
+        Pa.m0 = w.pm[0];
+        Pa.m1 = w.pm[1];
+        Pa.part = w.part;
+        Pa.result = w.result;
+        Pa.bar = w.bar;
+        Pa.sc = a.sc;
+        Pa.tol = S.tol;
+        Pa.eta_min = S.eta_min;
+        Pa.max_iter = S.max_iter;
+        Pa.inner_cap = S.inner_cap;
+        Pa.max_outer = S.max_outer;
+        void* pargs[] = {&Pa};
+        const void* pfn = w.stored_weights
+                              ? (a.exact ? (const void*)k_ppe_solve_pipe<true, true> : (const void*)k_ppe_solve_pipe<false, true>)
+                              : (a.exact ? (const void*)k_ppe_solve_pipe<true, false> : (const void*)k_ppe_solve_pipe<false, false>);
+        w.launch_err = launch_cooperative(pfn, w.blocks, w.threads, pargs, st);
+        k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
+        return 2;
+    }
+    void* args[] = {&S};
     const void* fn;
     if (w.stored_weights)
         fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1, true> : (const void*)k_ppe_solve<true, 0, true>)
@@ -1404,7 +1659,7 @@ void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.wrm, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.zp[0], w.zp[1], w.q,    w.part,     w.result, w.bar,
                   w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
-                  w.id_snap, w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
+                  w.id_snap, w.pu, w.pw, w.pz, w.pq, w.ps, w.pp, w.pm[0], w.pm[1], w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
                   w.scene_relres};
     lp_free(w.lp);
     for (void* p : ps)

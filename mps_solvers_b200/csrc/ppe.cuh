@@ -60,6 +60,10 @@ struct PpeWork {
     uint32_t* sell_cols = nullptr;
     float* sell_w = nullptr;           // the entries' weights, same layout
     bool stored_weights = true;        // SpMV reads sell_w (else recomputes from positions)
+    bool pipelined = false;            // single-reduction pipelined PCG (diagonal scaling)
+    // vectors of the pipelined solver
+    float *pu = nullptr, *pw = nullptr, *pz = nullptr, *pq = nullptr, *ps = nullptr, *pp = nullptr;
+    float* pm[2] = {nullptr, nullptr};
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
     // learned preconditioner (set up on first use)
     LearnedWork lp;

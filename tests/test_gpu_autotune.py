@@ -32,14 +32,14 @@ def test_autotune_semi_shapes(capi, tmp_path):
     with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
         rep = s.autotune(2)
         assert rep["ppe_threads"] in (256, 512, 1024)
-        assert rep["ppe_ms_per_iter"][0] > 0 and rep["ppe_ms_per_iter"][3] > 0  # default shape
-        assert rep["ppe_stored_weights"] in (0, 1)
+        assert rep["ppe_ms"][0] > 0 and rep["ppe_ms"][3] > 0 and rep["ppe_ms"][6] > 0  # 1024 threads
+        assert rep["ppe_stored_weights"] in (0, 1) and rep["ppe_pipelined"] in (0, 1)
         for _ in range(3):
             st = s.step(1)
             assert st.status == 0 and st.cg_relres <= 1e-8
         tuned = s.state(capi.ORDER_BY_ID)
     with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s:
-        held = sum(1 for t in rep["ppe_ms_per_iter"] if t > 0)
+        held = sum(1 for t in rep["ppe_ms"] if t > 0)
         s.step(3 * 2 + held * 2 + 3)   # the steps the tuner took, then the same 3
         plain = s.state(capi.ORDER_BY_ID)
     assert rel_err(tuned["press"], plain["press"]) < 1e-4

@@ -120,3 +120,19 @@ def test_semi_graph_replay_equals_direct_launches(capi, tmp_path):
             out.append(s.state())
     for f in ("pos", "vel", "press"):
         assert np.array_equal(out[0][f], out[1][f]), f
+
+
+def test_pipelined_pcg_matches_fp64_oracle(capi, oracle_mod, tmp_path):
+    """The single-reduction pipelined PCG reaches the same FP64 tolerance and
+    the same state as the standard form, within the stated tolerances."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    orc = oracle_mod.Oracle(d, oracle_mod.SEMI_JACOBI, 64)
+    orc.set_cg(True, 1e-12, 100000)
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, ppe_pipelined=1) as s:
+        for k in range(8):
+            st = s.step(1)
+            orc.step(1)
+            assert st.cg_relres <= 1e-8 and st.cg_iters > 0
+        ex, eu, ep = compare(s.state(), orc.state())
+    assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
