@@ -260,9 +260,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         n = len(pos0)
         sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
                               precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+    tc_diff = None
     if method == capi.METHOD_SEMI_IMPLICIT and precond == capi.PRECOND_LEARNED:
         from mps_solvers_b200 import precond_weights
         sim.set_precond_params(precond_weights.load())
+        sim.step(1)  # a PPE system for the tensor-core check
+        tc_diff = sim.precond_tensor_cores(True)
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
@@ -274,7 +277,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         surface = {"grid": list(SURFACE_SHAPE), "every": SURFACE_EVERY}
     # launch shapes picked by the library's autotuner on this scene, then
     # warm-up (also captures the step graphs)
-    tune = sim.autotune(2)
+    tune = sim.autotune(2) if not args.no_autotune else None
     for _ in range(args.warmup):
         sim.step_async(1)
     sim.step(0)
@@ -393,6 +396,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "autotune": tune,
+        "learned_tensor_core_rel_diff": tc_diff,
         "surface": surface,
         "ppe_compare": compare,
         "batch": None if scene_iters is None else {
@@ -418,6 +422,8 @@ def ppe_compare(case_dir: str, arith: int, device: int, warm: int, steps: int):
                              precond=pc) as s:
             if pc == capi.PRECOND_LEARNED:
                 s.set_precond_params(precond_weights.load())
+                s.step(1)
+                out["learned_tensor_core_rel_diff"] = s.precond_tensor_cores(True)
             s.step(warm)
             iters, worst = 0, 0.0
             for _ in range(steps):
@@ -474,6 +480,8 @@ def main():
                     help="PPE preconditioner of the semi-implicit timed run")
     ap.add_argument("--no-ppe-compare", action="store_true",
                     help="skip the diagonal-vs-learned PPE comparison (semi-implicit)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (short launch lists for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

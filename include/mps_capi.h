@@ -229,6 +229,12 @@ mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint64_t seed, 
 /* The state the last PPE system was assembled from (np entries each):
  * x y z type-bits per particle, n, GEO index, 1 for a solved (non-Dirichlet)
  * row, the diagonal of A. */
+/* Run the network forward on the last PPE system with its 64 -> 64 layers
+ * in FP32 on the CUDA cores and with BF16 activations on the tensor cores
+ * (tcgen05, accumulators in tensor memory), report the largest difference
+ * of the factor's entries relative to the largest entry, and keep the
+ * tensor cores for inference when enable != 0 (training always uses FP32). */
+mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double* max_rel_diff);
 mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
                             double* diag, uint32_t* count);
 

@@ -42,7 +42,7 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force",
            "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
            "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
-           "mps_surface_case_table")
+           "mps_surface_case_table", "mps_precond_tensor_cores")
 
 
 class mps_options(C.Structure):
@@ -165,6 +165,7 @@ def lib():
             "mps_surface_vertex_values": (C.c_int, [H, Fp, Fp]),
             "mps_surface_write_stl": (C.c_int, [H, C.c_char_p]),
             "mps_surface_case_table": (C.c_int, [C.POINTER(C.c_uint8), C.POINTER(C.c_int8)]),
+            "mps_precond_tensor_cores": (C.c_int, [H, C.c_int, C.POINTER(C.c_double)]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
@@ -392,6 +393,13 @@ class Simulation:
         a, b = C.c_double(), C.c_double()
         self._check(lib().mps_precond_train(self.h, iters, lr, seed, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def precond_tensor_cores(self, enable: bool = True) -> float:
+        """Compare the tensor-core forward with the FP32 one on the last
+        system (max relative difference of G) and use it when enabled."""
+        d = C.c_double()
+        self._check(lib().mps_precond_tensor_cores(self.h, int(enable), C.byref(d)))
+        return d.value
 
     def ppe_snapshot(self) -> Dict[str, np.ndarray]:
         n = self.counts()["np"]

@@ -5,6 +5,7 @@
 // table, the per-step device scalars, and one stream.  Every step is the
 // reference's stage order; with use_graph the launches of a step are
 // captured once per buffer parity and replayed.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1221,12 +1222,50 @@ extern "C" mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint
         lp_adam(h->ppe.lp, lr, h->stream);
     }
     // refresh G for the current system with the updated weights
-    lp_forward(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, h->cap, h->stream);
+    lp_forward(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, h->cap, h->stream, h->ppe.lp.tensor_cores);
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaGetLastError());
     if (loss_first) *loss_first = first;
     if (loss_last) *loss_last = last;
     return MPS_OK;
+}
+
+// Run the network forward on the last PPE system with the 64 -> 64 layers in
+// FP32 on the CUDA cores and with BF16 activations on the tensor cores,
+// report the largest difference of the factor's entries relative to the
+// largest entry, and use the tensor cores for inference from now on when
+// `enable` is set.
+extern "C" mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double* max_rel_diff) {
+    mps_status s = need_snapshot(h);
+    if (s != MPS_OK) return s;
+    CK(cudaSetDevice(h->dev));
+    const LpSystem L = ppe_lp_system(h->ppe, stage_args(h));
+    const bool exact = h->opt.arith == MPS_ARITH_EXACT;
+    const size_t ng = (size_t)h->cap * LP_GW, nd = h->cap;
+    std::vector<float> g0(ng), d0(nd), g1(ng), d1(nd);
+    for (int pass = 0; pass < 2; pass++) {
+        lp_forward(h->ppe.lp, L, exact, h->cap, h->stream, pass == 1);
+        CK(cudaMemcpyAsync(pass ? g1.data() : g0.data(), h->ppe.lp.gval, ng * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(pass ? d1.data() : d0.data(), h->ppe.lp.gdiag, nd * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaGetLastError());
+    }
+    double mx = 0.0, md = 0.0;
+    for (size_t k = 0; k < ng; k++) {
+        mx = std::max(mx, (double)std::fabs(g0[k]));
+        md = std::max(md, (double)std::fabs(g0[k] - g1[k]));
+    }
+    for (size_t k = 0; k < nd; k++) {
+        mx = std::max(mx, (double)std::fabs(d0[k]));
+        md = std::max(md, (double)std::fabs(d0[k] - d1[k]));
+    }
+    if (max_rel_diff) *max_rel_diff = mx > 0.0 ? md / mx : md;
+    h->ppe.lp.tensor_cores = enable != 0;
+    lp_forward(h->ppe.lp, L, exact, h->cap, h->stream, h->ppe.lp.tensor_cores);
+    CK(cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    Scalars sc;
+    return read_status(h, &sc);
 }
 
 extern "C" mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,

@@ -793,6 +793,169 @@ __global__ void __launch_bounds__(256) k_lp_pack(const uint32_t* __restrict__ sc
     }
 }
 
+// ---------------------------------------------------------------- tensor-core dense layer
+// The same 64 -> 64 layer on the fifth-generation tensor cores (inference):
+// out = act(x W^T + b) + resid for a tile of 128 rows per step of a
+// persistent CTA of 128 threads.  x is rounded to BF16 on its way into shared
+// memory (W is BF16 already); the product accumulates in FP32 in tensor
+// memory.  Operands use the no-swizzle K-major core-matrix layout (8 rows x
+// 16 bytes per core matrix; element (m, k) at byte
+// ((k / 8) * (M / 8) + m / 8) * 128 + (m % 8) * 16 + (k % 8) * 2), so one
+// MMA of K = 16 reads two core-matrix columns: leading byte offset =
+// M / 8 * 128 (the next 8 k), stride byte offset = 128 (the next 8 rows).
+// One thread issues the 4 MMAs (K = 64) and commits them to an mbarrier;
+// every thread waits on it (bounded), and each warp reads its 32 accumulator
+// lanes with tcgen05.ld.
+constexpr int TC_M = 128;
+constexpr uint32_t TC_IDESC = (1u << 4)                  // accumulator F32
+                              | (1u << 7) | (1u << 10)   // A, B BF16
+                              | ((64u >> 3) << 17)       // N = 64
+                              | ((128u >> 4) << 24);     // M = 128
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of this architecture; no swizzle, base offset 0
+    return d;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+
+__global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ x, const __nv_bfloat16* __restrict__ w,
+                                                      int woff, int boff, const float* __restrict__ resid,
+                                                      float* __restrict__ pre_out, float* __restrict__ out, int act,
+                                                      const uint32_t* __restrict__ rowlist,
+                                                      const uint32_t* __restrict__ nrows, uint32_t* __restrict__ err) {
+    __shared__ __align__(1024) uint8_t sA[TC_M * LP_H * 2];
+    __shared__ __align__(1024) uint8_t sB[LP_H * LP_H * 2];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    const uint32_t R = *nrows;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) failed = 0;
+    // W (n, k) into the K-major layout, N / 8 = 8 row groups
+    for (uint32_t e = tid; e < LP_H * LP_H / 8; e += TC_M) {
+        const uint32_t n = e / 8, kc = e % 8;  // row n, 8-element chunk kc
+        const uint4 v = *reinterpret_cast<const uint4*>(w + woff + n * LP_H + kc * 8);
+        *reinterpret_cast<uint4*>(sB + (kc * 8 + n / 8) * 128 + (n % 8) * 16) = v;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(64));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    const float bias_scale = boff >= 0 ? 1.f : 0.f;
+    uint32_t phase = 0;
+    const uint32_t ntiles = (R + TC_M - 1) / TC_M;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // A: row m = tid of the tile, converted to BF16
+        {
+            const uint32_t k = tile * TC_M + tid;
+            const bool has = k < R;
+            const uint32_t i = has ? __ldg(rowlist + k) : 0u;
+            const float4* src = reinterpret_cast<const float4*>(x + (size_t)i * LP_H);
+#pragma unroll
+            for (int kc = 0; kc < 8; kc++) {
+                float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+                if (has) {
+                    a = src[2 * kc];
+                    b = src[2 * kc + 1];
+                }
+                __nv_bfloat162 p0 = __floats2bfloat162_rn(a.x, a.y), p1 = __floats2bfloat162_rn(a.z, a.w);
+                __nv_bfloat162 p2 = __floats2bfloat162_rn(b.x, b.y), p3 = __floats2bfloat162_rn(b.z, b.w);
+                uint4 u;
+                u.x = *reinterpret_cast<uint32_t*>(&p0);
+                u.y = *reinterpret_cast<uint32_t*>(&p1);
+                u.z = *reinterpret_cast<uint32_t*>(&p2);
+                u.w = *reinterpret_cast<uint32_t*>(&p3);
+                *reinterpret_cast<uint4*>(sA + (kc * (TC_M / 8) + tid / 8) * 128 + (tid % 8) * 16) = u;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int kk = 0; kk < LP_H / 16; kk++) {
+                const uint64_t da = umma_desc(smem_addr(sA) + kk * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
+                const uint64_t db = umma_desc(smem_addr(sB) + kk * 2 * (LP_H / 8) * 128, (LP_H / 8) * 128, 128);
+                const uint32_t acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_addr(&mbar)));
+        }
+        // bounded wait for the MMAs of this tile
+        {
+            uint32_t done = 0;
+            for (uint32_t spin = 0; spin < (1u << 22) && !done; spin++) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(smem_addr(&mbar)), "r"(phase));
+                if (!done) __nanosleep(20);
+            }
+            if (!done) failed = 1;
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (failed) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        float v[LP_H];
+        const uint32_t lane_base = (warp * 32u) << 16;
+#pragma unroll
+        for (int c = 0; c < LP_H / 16; c++) tmem_ld16(tmem + lane_base + c * 16, v + 16 * c);
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        const uint32_t k = tile * TC_M + warp * 32 + lane;
+        if (k < R) {
+            const uint32_t i = __ldg(rowlist + k);
+#pragma unroll
+            for (int n = 0; n < LP_H; n++) {
+                const float sv = v[n] + bias_scale * __bfloat162float(w[(boff >= 0 ? boff : 0) + n]);
+                if (pre_out) pre_out[(size_t)i * LP_H + n] = sv;
+                float o = act ? gelu_t(sv, nullptr) : sv;
+                if (resid) o += resid[(size_t)i * LP_H + n];
+                out[(size_t)i * LP_H + n] = o;
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    if (tid == 0 && failed) atomicOr(err, ERR_DEVICE_TIMEOUT);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+    }
+}
+
 // ---------------------------------------------------------------- host side
 int lp_setup(LearnedWork& L, uint32_t cap, std::string* err) {
     L.cap = cap;
@@ -926,19 +1089,27 @@ void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStrea
                                                              const_cast<Scalars*>(S.sc));
 }
 
-void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st) {
+void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores) {
     (void)exact;
     const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
     const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
     const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;
+    const uint32_t tgrid = blocks_for(cap, TC_M) < 148u * 4u ? blocks_for(cap, TC_M) : 148u * 4u;
+    uint32_t* err = const_cast<uint32_t*>(&S.sc->err);
+    auto dense = [&](const float* x, int woff, int boff, const float* resid, float* pre, float* out, int act) {
+        if (tensor_cores)
+            k_lp_dense_tc<<<tgrid, TC_M, 0, st>>>(x, L.w16, woff, boff, resid, pre, out, act, S.rowlist, S.nrows, err);
+        else
+            k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(x, L.w16, woff, boff, resid, pre, out, act, S.rowlist, S.nrows);
+    };
     FwdArgs A = fwd_args(L, S);
     k_lp_edge_fwd<1><<<wb, 256, 0, st>>>(A);
-    k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(L.a1, L.w16, LP_V1, LP_C1, nullptr, L.pre1, L.h1, 1, S.rowlist, S.nrows);
-    k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(L.h1, L.w16, LP_U2, -1, nullptr, nullptr, L.uh1, 0, S.rowlist, S.nrows);
+    dense(L.a1, LP_V1, LP_C1, nullptr, L.pre1, L.h1, 1);
+    dense(L.h1, LP_U2, -1, nullptr, nullptr, L.uh1, 0);
     k_lp_edge_fwd<2><<<wb, 256, 0, st>>>(A);
-    k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(L.a2, L.w16, LP_V2, LP_C2, L.h1, L.pre2, L.h2, 1, S.rowlist, S.nrows);
-    k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(L.h2, L.w16, LP_RA, -1, nullptr, nullptr, L.ra, 0, S.rowlist, S.nrows);
-    k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(L.h2, L.w16, LP_RB, -1, nullptr, nullptr, L.rb, 0, S.rowlist, S.nrows);
+    dense(L.a2, LP_V2, LP_C2, L.h1, L.pre2, L.h2, 1);
+    dense(L.h2, LP_RA, -1, nullptr, nullptr, L.ra, 0);
+    dense(L.h2, LP_RB, -1, nullptr, nullptr, L.rb, 0);
     k_lp_readout_fwd<<<wb, 256, 0, st>>>(A);
     k_lp_transpose<<<blocks_for(cap, 256), 256, 0, st>>>(L.scols, L.scnt, L.nlow, L.gval, S.rowlist, S.nrows);
     // the solve layout
@@ -954,7 +1125,7 @@ void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cud
 
 int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, uint32_t cap, cudaStream_t st) {
     if (lp_setup_training(L) != MPS_OK) return MPS_ERR_CUDA;
-    lp_forward(L, S, exact, cap, st);
+    lp_forward(L, S, exact, cap, st, false);  // training: FP32 activations (the oracle's network)
     const uint32_t tb = blocks_for(cap, 256), wb = blocks_for(cap * 32u, 256);
     const uint32_t db = blocks_for(cap, 4);
     const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;

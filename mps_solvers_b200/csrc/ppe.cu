@@ -1448,7 +1448,7 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     if (w.lp.ready) {
         const LpSystem L = ppe_lp_system(w, a);
         lp_build_stencil(w.lp, L, cap, st);
-        lp_forward(w.lp, L, a.exact, cap, st);
+        lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores);
         launched += 10;
     }
     return launched;

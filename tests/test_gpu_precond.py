@@ -118,3 +118,19 @@ def test_trained_network_reduces_cg_iterations(capi, tmp_path):
                 tot += st.cg_iters
             it[name] = tot
     assert it["learned"] < it["diag"], it
+
+
+def test_tensor_core_forward_matches_fp32(capi, tmp_path):
+    """The network's 64 -> 64 layers on tcgen05 (BF16 activations, FP32
+    accumulation in tensor memory) against the FP32 CUDA-core forward: the
+    factor's entries agree to BF16 rounding, and the solver converges with it."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, precond=capi.PRECOND_LEARNED) as s:
+        s.set_precond_params(random_params(capi, 0, om_scale=0.3))
+        s.step(3)
+        diff = s.precond_tensor_cores(True)
+        assert 0.0 < diff < 2e-2, diff
+        for _ in range(3):
+            st = s.step(1)
+            assert st.status == 0 and st.cg_relres <= 1e-8
