@@ -93,7 +93,11 @@ typedef struct {
                             check (0: 4)                                      */
     int ppe_pipelined;   /* PPE: 1 = pipelined single-reduction PCG (diagonal
                             scaling, single scenes); mps_autotune may change it */
-    uint32_t reserved[6];
+    int ppe_l2_keep_mb;  /* PPE: MiB of the stored matrix read as evict_last so
+                            it stays in L2 across CG iterations while the rest
+                            streams as evict_first (0: half the L2; -1: no
+                            hints)                                            */
+    uint32_t reserved[5];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

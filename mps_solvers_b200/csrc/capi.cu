@@ -470,6 +470,13 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
         h->ppe.pipelined = h->opt.ppe_pipelined != 0;
+        size_t keep_bytes = (size_t)h->opt.ppe_l2_keep_mb << 20;
+        if (h->opt.ppe_l2_keep_mb == 0) {  // half the L2: the best of a sweep at 310,912 particles
+            int l2 = 0;
+            cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->opt.device);
+            keep_bytes = (size_t)l2 / 2;
+        }
+        h->ppe.l2_keep_entries = h->opt.ppe_l2_keep_mb < 0 ? 0xFFFFFFFFu : (uint32_t)(keep_bytes / 8);
         if (h->opt.precond == MPS_PRECOND_LEARNED) {
             e = ppe_enable_learned(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;

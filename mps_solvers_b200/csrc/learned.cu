@@ -834,13 +834,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
+// Shared memory of k_lp_dense_tc: A tile (BF16, K-major core matrices),
+// W (BF16, same layout), and the FP32 accumulator staged for coalesced
+// stores (row stride 68 floats: the row-per-thread writes and the
+// half-warp-per-row reads are both free of bank conflicts).
+constexpr uint32_t TC_SA = 0, TC_SB = TC_M * LP_H * 2, TC_SC = TC_SB + LP_H * LP_H * 2;
+constexpr uint32_t TC_CST = LP_H + 4;
+constexpr uint32_t TC_SMEM = TC_SC + TC_M * TC_CST * 4;
+
 __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ x, const __nv_bfloat16* __restrict__ w,
                                                       int woff, int boff, const float* __restrict__ resid,
                                                       float* __restrict__ pre_out, float* __restrict__ out, int act,
                                                       const uint32_t* __restrict__ rowlist,
                                                       const uint32_t* __restrict__ nrows, uint32_t* __restrict__ err) {
-    __shared__ __align__(1024) uint8_t sA[TC_M * LP_H * 2];
-    __shared__ __align__(1024) uint8_t sB[LP_H * LP_H * 2];
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sA = smem + TC_SA;
+    uint8_t* sB = smem + TC_SB;
+    float* sC = reinterpret_cast<float*>(smem + TC_SC);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int failed;
@@ -866,32 +876,48 @@ __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ 
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_slot;
-    const float bias_scale = boff >= 0 ? 1.f : 0.f;
+    // epilogue columns of this lane (half-warp per row): 4 * (lane % 16) .. + 3
+    const uint32_t ec = 4u * (lane & 15u);
+    float4 bias = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (boff >= 0)
+        bias = make_float4(__bfloat162float(w[boff + ec]), __bfloat162float(w[boff + ec + 1]),
+                           __bfloat162float(w[boff + ec + 2]), __bfloat162float(w[boff + ec + 3]));
     uint32_t phase = 0;
     const uint32_t ntiles = (R + TC_M - 1) / TC_M;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // A: row m = tid of the tile, converted to BF16
+        // A: warp w loads rows 32w .. 32w + 31 of the tile, 8 rows x 64 bytes
+        // per instruction (lane: row r8 = lane / 4, float4 (lane % 4) of the
+        // 64-byte column group g), converted to BF16 into the core matrices
         {
-            const uint32_t k = tile * TC_M + tid;
-            const bool has = k < R;
-            const uint32_t i = has ? __ldg(rowlist + k) : 0u;
-            const float4* src = reinterpret_cast<const float4*>(x + (size_t)i * LP_H);
+            const uint32_t r8 = lane >> 2, c4l = lane & 3u;
+            uint32_t src[4];
 #pragma unroll
-            for (int kc = 0; kc < 8; kc++) {
-                float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-                if (has) {
-                    a = src[2 * kc];
-                    b = src[2 * kc + 1];
-                }
-                __nv_bfloat162 p0 = __floats2bfloat162_rn(a.x, a.y), p1 = __floats2bfloat162_rn(a.z, a.w);
-                __nv_bfloat162 p2 = __floats2bfloat162_rn(b.x, b.y), p3 = __floats2bfloat162_rn(b.z, b.w);
-                uint4 u;
-                u.x = *reinterpret_cast<uint32_t*>(&p0);
-                u.y = *reinterpret_cast<uint32_t*>(&p1);
-                u.z = *reinterpret_cast<uint32_t*>(&p2);
-                u.w = *reinterpret_cast<uint32_t*>(&p3);
-                *reinterpret_cast<uint4*>(sA + (kc * (TC_M / 8) + tid / 8) * 128 + (tid % 8) * 16) = u;
+            for (int rg = 0; rg < 4; rg++) {
+                const uint32_t k = tile * TC_M + warp * 32 + rg * 8 + r8;
+                src[rg] = k < R ? __ldg(rowlist + k) : 0xFFFFFFFFu;
             }
+            float4 v[16];
+#pragma unroll
+            for (int rg = 0; rg < 4; rg++)
+#pragma unroll
+                for (int g = 0; g < 4; g++) {
+                    const uint32_t i = src[rg];
+                    v[rg * 4 + g] = i != 0xFFFFFFFFu
+                                        ? __ldg(reinterpret_cast<const float4*>(x + (size_t)i * LP_H) + 4 * g + c4l)
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+            for (int rg = 0; rg < 4; rg++)
+#pragma unroll
+                for (int g = 0; g < 4; g++) {
+                    const float4 a = v[rg * 4 + g];
+                    const uint32_t c4 = 4 * g + c4l, m8 = warp * 4 + rg;  // float4 column, row group of 8
+                    __nv_bfloat162 p0 = __floats2bfloat162_rn(a.x, a.y), p1 = __floats2bfloat162_rn(a.z, a.w);
+                    uint2 u;
+                    u.x = *reinterpret_cast<uint32_t*>(&p0);
+                    u.y = *reinterpret_cast<uint32_t*>(&p1);
+                    *reinterpret_cast<uint2*>(sA + ((c4 >> 1) * (TC_M / 8) + m8) * 128 + r8 * 16 + (c4 & 1u) * 8) = u;
+                }
         }
         asm volatile("fence.proxy.async.shared::cta;");
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -928,21 +954,41 @@ __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ 
         __syncthreads();
         if (failed) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        float v[LP_H];
-        const uint32_t lane_base = (warp * 32u) << 16;
+        // TMEM lane = row of the tile: warp w reads rows 32w .. 32w + 31 and
+        // stages them; the same warp then writes them out coalesced
+        {
+            float v[LP_H];
+            const uint32_t lane_base = (warp * 32u) << 16;
 #pragma unroll
-        for (int c = 0; c < LP_H / 16; c++) tmem_ld16(tmem + lane_base + c * 16, v + 16 * c);
-        asm volatile("tcgen05.wait::ld.sync.aligned;");
-        const uint32_t k = tile * TC_M + warp * 32 + lane;
-        if (k < R) {
-            const uint32_t i = __ldg(rowlist + k);
+            for (int c = 0; c < LP_H / 16; c++) tmem_ld16(tmem + lane_base + c * 16, v + 16 * c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            float* row = sC + tid * TC_CST;
 #pragma unroll
-            for (int n = 0; n < LP_H; n++) {
-                const float sv = v[n] + bias_scale * __bfloat162float(w[(boff >= 0 ? boff : 0) + n]);
-                if (pre_out) pre_out[(size_t)i * LP_H + n] = sv;
-                float o = act ? gelu_t(sv, nullptr) : sv;
-                if (resid) o += resid[(size_t)i * LP_H + n];
-                out[(size_t)i * LP_H + n] = o;
+            for (int c = 0; c < LP_H / 4; c++)
+                *reinterpret_cast<float4*>(row + 4 * c) = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+        }
+        __syncwarp();
+#pragma unroll 4
+        for (uint32_t it = 0; it < 16; it++) {
+            const uint32_t m = warp * 32 + 2 * it + (lane >> 4);
+            const uint32_t k = tile * TC_M + m;
+            if (k < R) {
+                const uint32_t i = __ldg(rowlist + k);
+                const float4 a = *reinterpret_cast<const float4*>(sC + m * TC_CST + ec);
+                const float4 sv = make_float4(a.x + bias.x, a.y + bias.y, a.z + bias.z, a.w + bias.w);
+                const size_t o = (size_t)i * LP_H + ec;
+                if (pre_out) *reinterpret_cast<float4*>(pre_out + o) = sv;
+                float4 r = act ? make_float4(gelu_t(sv.x, nullptr), gelu_t(sv.y, nullptr), gelu_t(sv.z, nullptr),
+                                             gelu_t(sv.w, nullptr))
+                               : sv;
+                if (resid) {
+                    const float4 e = __ldg(reinterpret_cast<const float4*>(resid + o));
+                    r.x += e.x;
+                    r.y += e.y;
+                    r.z += e.z;
+                    r.w += e.w;
+                }
+                *reinterpret_cast<float4*>(out + o) = r;
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -1094,11 +1140,22 @@ void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cud
     const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
     const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
     const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;
-    const uint32_t tgrid = blocks_for(cap, TC_M) < 148u * 4u ? blocks_for(cap, TC_M) : 148u * 4u;
+    // one resident wave of the tensor-core kernel (it loops over the tiles)
+    static uint32_t tc_resident = 0;
+    if (tensor_cores && tc_resident == 0) {
+        cudaFuncSetAttribute(k_lp_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+        int per_sm = 0, dev = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lp_dense_tc, TC_M, TC_SMEM);
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        tc_resident = (uint32_t)((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148));
+    }
+    const uint32_t tgrid = blocks_for(cap, TC_M) < tc_resident ? blocks_for(cap, TC_M) : tc_resident;
     uint32_t* err = const_cast<uint32_t*>(&S.sc->err);
     auto dense = [&](const float* x, int woff, int boff, const float* resid, float* pre, float* out, int act) {
-        if (tensor_cores)
-            k_lp_dense_tc<<<tgrid, TC_M, 0, st>>>(x, L.w16, woff, boff, resid, pre, out, act, S.rowlist, S.nrows, err);
+        if (tensor_cores)  // inference only: the pre-activations feed nothing but the backward pass
+            k_lp_dense_tc<<<tgrid, TC_M, TC_SMEM, st>>>(x, L.w16, woff, boff, resid, nullptr, out, act, S.rowlist,
+                                                        S.nrows, err);
         else
             k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(x, L.w16, woff, boff, resid, pre, out, act, S.rowlist, S.nrows);
     };

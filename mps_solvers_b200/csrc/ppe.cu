@@ -273,6 +273,7 @@ struct SolveArgs {
     Scalars* sc;
     double tol;
     double eta_min;   // smallest inner reduction asked of one FP32 solve
+    uint32_t keep;    // matrix entries read as evict_last (mat_policy)
     int max_iter;
     int inner_cap;
     int max_outer;
@@ -289,11 +290,47 @@ __device__ __forceinline__ float stencil_weight(const SolveArgs& S, const float4
     return (j != i && rr < S.rlap_thr) ? weight_rr<EX>(S.rlap, rr) : 0.f;
 }
 
+// L2 residency of the stored matrix.  Every CG iteration streams the whole
+// matrix in the same order; once it is larger than L2 a plain LRU keeps none
+// of it from one iteration to the next.  The entries before `keep` (the
+// leading slices) are read as evict_last and the rest as evict_first, so the
+// streamed tail displaces itself and the head stays in L2.  The matrix is
+// read once per product, so it bypasses L1 (which keeps the gathered
+// neighbour vectors instead).  keep = 0xFFFFFFFF reads everything with the
+// default policy.
+__device__ __forceinline__ uint64_t mat_policy(uint32_t base, uint32_t keep) {
+    uint64_t p;
+    if (keep == 0xFFFFFFFFu)
+        asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    else if (base < keep)
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint4 ld_mat(const uint4* p, uint64_t pol) {
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ float4 ld_mat(const float4* p, uint64_t pol) {
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p), "l"(pol));
+    return v;
+}
+
 // The weights of one lane's 4 entries: stored, or recomputed from positions.
 template <bool EX, bool SW>
-__device__ __forceinline__ float4 chunk_weights(const float4* __restrict__ w4, const float4* __restrict__ pos, float rlap,
-                                                float thr, const float4& pi, uint32_t i, const uint4& c) {
-    if (SW) return __ldg(w4);
+__device__ __forceinline__ float4 chunk_weights(const float4* __restrict__ w4, uint64_t pol,
+                                                const float4* __restrict__ pos, float rlap, float thr,
+                                                const float4& pi, uint32_t i, const uint4& c) {
+    if (SW) return ld_mat(w4, pol);
     auto one = [&](uint32_t j) {
         const float4 pj = __ldg(pos + j);
         const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
@@ -345,6 +382,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         for (uint32_t sl = gw; sl < nslices; sl += nw) {
             const uint32_t k = sl * SELL_C + rsub;
             const uint32_t base = __ldg(S.off + sl);
+            const uint64_t pol = mat_policy(base, S.keep);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
             const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
             const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -352,8 +390,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             const float4 pi = __ldg(S.pos + ii);
             double s = 0.0;
             for (uint32_t t = 0; t < T; t++) {
-                const uint4 c = __ldg(cols + 32 * t);
-                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                const uint4 c = ld_mat(cols + 32 * t, pol);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                 s += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
                      (double)w.w * S.x64[c.w];
             }
@@ -420,6 +458,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             for (uint32_t sl = gw; sl < nslices; sl += nw) {
                 const uint32_t k = sl * SELL_C + rsub;
                 const uint32_t base = __ldg(S.off + sl);
+                const uint64_t pol = mat_policy(base, S.keep);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
                 const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
                 const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -428,8 +467,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 float s0 = 0.f, s1 = 0.f;
 #pragma unroll 2
                 for (uint32_t t = 0; t < T; t++) {
-                    const uint4 c = __ldg(cols + 32 * t);
-                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                    const uint4 c = ld_mat(cols + 32 * t, pol);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                     const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
                     s0 = fmaf(w.x, fmaf(beta, a0.y, a0.x), s0);
                     s1 = fmaf(w.y, fmaf(beta, a1.y, a1.x), s1);
@@ -552,6 +591,7 @@ struct PipeArgs {
     unsigned* bar;
     Scalars* sc;
     double tol, eta_min;
+    uint32_t keep;
     int max_iter, inner_cap, max_outer;
 };
 
@@ -575,6 +615,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
         for (uint32_t sl = gw; sl < nslices; sl += nw) {
             const uint32_t k = sl * SELL_C + rsub;
             const uint32_t base = __ldg(S.off + sl);
+            const uint64_t pol = mat_policy(base, S.keep);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
             const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
             const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -582,8 +623,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
             const float4 pi = __ldg(S.pos + ii);
             double sum = 0.0;
             for (uint32_t t = 0; t < T; t++) {
-                const uint4 c = __ldg(cols + 32 * t);
-                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                const uint4 c = ld_mat(cols + 32 * t, pol);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                 sum += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
                        (double)w.w * S.x64[c.w];
             }
@@ -614,6 +655,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
         for (uint32_t sl = gw; sl < nslices; sl += nw) {
             const uint32_t k = sl * SELL_C + rsub;
             const uint32_t base = __ldg(S.off + sl);
+            const uint64_t pol = mat_policy(base, S.keep);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
             const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
             const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -621,8 +663,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
             const float4 pi = __ldg(S.pos + ii);
             float s0 = 0.f, s1 = 0.f;
             for (uint32_t t = 0; t < T; t++) {
-                const uint4 c = __ldg(cols + 32 * t);
-                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                const uint4 c = ld_mat(cols + 32 * t, pol);
+                const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                 s0 = fmaf(w.x, S.u[c.x], s0);
                 s1 = fmaf(w.y, S.u[c.y], s1);
                 s0 = fmaf(w.z, S.u[c.z], s0);
@@ -667,6 +709,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
             for (uint32_t sl = gw; sl < nslices; sl += nw) {
                 const uint32_t k = sl * SELL_C + rsub;
                 const uint32_t base = __ldg(S.off + sl);
+                const uint64_t pol = mat_policy(base, S.keep);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
                 const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
                 const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -675,8 +718,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
                 float s0 = 0.f, s1 = 0.f;
 #pragma unroll 2
                 for (uint32_t t = 0; t < T; t++) {
-                    const uint4 c = __ldg(cols + 32 * t);
-                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
+                    const uint4 c = ld_mat(cols + 32 * t, pol);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                     s0 = fmaf(w.x, mc[c.x], s0);
                     s1 = fmaf(w.y, mc[c.y], s1);
                     s0 = fmaf(w.z, mc[c.z], s0);
@@ -768,6 +811,7 @@ struct BatchSolveArgs {
     uint32_t ns;
     double tol;
     double eta_min;
+    uint32_t keep;
     int max_iter, inner_cap, max_outer;
 };
 
@@ -889,6 +933,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             const bool work = has && !done[s];
             if (!__any_sync(0xffffffffu, work)) continue;
             const uint32_t base = __ldg(S.off + sl);
+            const uint64_t pol = mat_policy(base, S.keep);
             const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
             const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
             const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -897,8 +942,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             double sum = 0.0;
             if (work)
                 for (uint32_t t = 0; t < T; t++) {
-                    const uint4 c = __ldg(cols + 32 * t);
-                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, rl, thr, pi, ii, c);
+                    const uint4 c = ld_mat(cols + 32 * t, pol);
+                    const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, rl, thr, pi, ii, c);
                     sum += (double)w.x * S.x64[c.x] + (double)w.y * S.x64[c.y] + (double)w.z * S.x64[c.z] +
                            (double)w.w * S.x64[c.w];
                 }
@@ -959,6 +1004,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const bool work = has && active[s];
                 if (!__any_sync(0xffffffffu, work)) continue;
                 const uint32_t base = __ldg(S.off + sl);
+                const uint64_t pol = mat_policy(base, S.keep);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
                 const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
                 const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
@@ -968,8 +1014,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 float sum = 0.f, sum1 = 0.f;
                 if (work)
                     for (uint32_t t = 0; t < T; t++) {
-                        const uint4 c = __ldg(cols + 32 * t);
-                        const float4 w = chunk_weights<EX, SW>(wts + 32 * t, S.pos, rl, thr, pi, ii, c);
+                        const uint4 c = ld_mat(cols + 32 * t, pol);
+                        const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, rl, thr, pi, ii, c);
                         const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
                         sum = fmaf(w.x, fmaf(bs, a0.y, a0.x), sum);
                         sum1 = fmaf(w.y, fmaf(bs, a1.y, a1.x), sum1);
@@ -1515,6 +1561,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.inner_cap = opt.cg_check_every > 0 ? opt.cg_check_every : 500;
     S.eta_min = pow(10.0, -(double)(opt.cg_inner_digits > 0 ? opt.cg_inner_digits : 4));
     S.max_outer = 40;
+    S.keep = w.l2_keep_entries;
     if (a.batch.n) {
         BatchSolveArgs B;
         B.rowlist = w.rowlist;
@@ -1547,6 +1594,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.inner_cap = S.inner_cap;
         B.max_outer = S.max_outer;
         B.eta_min = S.eta_min;
+        B.keep = S.keep;
         void* bargs[] = {&B};
         const void* bfn = w.stored_weights
                               ? (a.exact ? (const void*)k_ppe_solve_batch<true, true>
@@ -1588,6 +1636,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         Pa.sc = a.sc;
         Pa.tol = S.tol;
         Pa.eta_min = S.eta_min;
+        Pa.keep = S.keep;
         Pa.max_iter = S.max_iter;
         Pa.inner_cap = S.inner_cap;
         Pa.max_outer = S.max_outer;

@@ -61,6 +61,7 @@ struct PpeWork {
     float* sell_w = nullptr;           // the entries' weights, same layout
     bool stored_weights = true;        // SpMV reads sell_w (else recomputes from positions)
     bool pipelined = false;            // single-reduction pipelined PCG (diagonal scaling)
+    uint32_t l2_keep_entries = 0xFFFFFFFFu;  // matrix entries kept in L2 across iterations (all: no hints)
     // vectors of the pipelined solver
     float *pu = nullptr, *pw = nullptr, *pz = nullptr, *pq = nullptr, *ps = nullptr, *pp = nullptr;
     float* pm[2] = {nullptr, nullptr};
