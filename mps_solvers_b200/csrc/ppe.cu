@@ -38,95 +38,92 @@ __device__ __forceinline__ float warp_sum_f(float v) {
     return v;
 }
 
-// fixed-order block sum of up to PPE_PARTS doubles, written to part[block]
+// Grid-wide sum of K doubles fused with a grid barrier.  bar[0] counts
+// arrivals and only grows during a launch (the assembly kernel empties it
+// before every solve), so the e-th barrier of a launch completes when it
+// reaches (e + 1) * gridDim.x and a block learns e from the count it saw
+// before arriving.  Each block writes its fixed-order block sum into slot
+// [e & 1][block] (two buffers: a block can write the slot of barrier e + 1
+// only after every block has finished reading those of barrier e), arrives,
+// waits for the count, and then adds all the slots itself in block order
+// (lane-strided, then a fixed shuffle tree): the totals are identical in
+// every block and on every run, and no block waits for another to publish
+// them.  The wait is bounded: after 1 s (global timer) it sets
+// ERR_DEVICE_TIMEOUT and returns false.
 template <int K>
-__device__ void block_partials(const double (&v)[K], double* part) {
+__device__ bool grid_reduce(const double (&v)[K], double* part, double* /*result*/, unsigned* bar, Scalars* sc,
+                            double (&out)[K]) {
     __shared__ double sm[K][32];
+    __shared__ double tot_s[K];
+    __shared__ unsigned ep_s;
+    __shared__ int ok_s;
+    const unsigned G = gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned seen = 0;
+    if (threadIdx.x == 0)  // the barrier's index, loaded early so the block sum hides the latency
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(bar) : "memory");
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        double t = warp_sum_d(v[k]);
+        const double t = warp_sum_d(v[k]);
         if (lane == 0) sm[k][warp] = t;
     }
     __syncthreads();
     if (warp == 0) {
+        double t[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) t[k] = warp_sum_d(lane < nw ? sm[k][lane] : 0.0);
+        if (lane == 0) {
+            const unsigned e = seen / G;
+            double* slot = part + ((size_t)(e & 1u) * G + blockIdx.x) * PPE_PARTS;
+#pragma unroll
+            for (int k = 0; k < K; k++) slot[k] = t[k];
+            __threadfence();  // this block's writes (slot and vectors) before the arrival
+            atomicAdd(bar, 1u);
+            const unsigned target = (e + 1) * G;
+            int ok = 1;
+            unsigned cur;
+            uint64_t t0;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+            for (;;) {
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+                if ((int)(cur - target) >= 0) break;
+                uint64_t t1;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+                if (t1 - t0 > 1000000000ull) {
+                    atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+            __threadfence();
+            ep_s = e;
+            ok_s = ok;
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const double* buf = part + (size_t)(ep_s & 1u) * G * PPE_PARTS;
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            double t = lane < nw ? sm[k][lane] : 0.0;
+            // up to 8 partials per lane loaded before adding (latency)
+            double v8[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const unsigned b = lane + 32u * u;
+                v8[u] = b < G ? __ldcg(buf + b * PPE_PARTS + k) : 0.0;
+            }
+            double t = 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; u++) t += v8[u];
+            for (unsigned b = lane + 256u; b < G; b += 32) t += __ldcg(buf + b * PPE_PARTS + k);
             t = warp_sum_d(t);
-            if (lane == 0) part[blockIdx.x * PPE_PARTS + k] = t;
+            if (lane == 0) tot_s[k] = t;
         }
     }
     __syncthreads();
-}
-
-// Grid-wide sum of K doubles fused with a grid barrier.  Every block writes
-// its fixed-order block sum to part[block]; the last block to arrive adds the
-// partials in block order (lane-strided, then a fixed shuffle tree), writes
-// the totals to result[] and releases the others, which then read result[].
-// The totals are therefore identical in every block and on every run.  The
-// wait is bounded: after ~1 s it sets ERR_DEVICE_TIMEOUT and returns false.
-template <int K>
-__device__ bool grid_reduce(const double (&v)[K], double* part, double* result, unsigned* bar, Scalars* sc,
-                            double (&out)[K]) {
-    block_partials<K>(v, part);
-    __shared__ int last, ok;
-    __shared__ unsigned gen0;
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile unsigned* gen = bar + 1;
-        gen0 = *gen;
-        __threadfence();
-        last = atomicAdd(bar, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (last) {
-        if (threadIdx.x < 32) {
-            __threadfence();
-            const int lane = threadIdx.x;
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                // up to 8 partials per lane loaded before adding (latency)
-                double v8[8];
-#pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const unsigned b = lane + 32u * u;
-                    v8[u] = b < gridDim.x ? __ldcg(part + b * PPE_PARTS + k) : 0.0;
-                }
-                double t = 0.0;
-#pragma unroll
-                for (int u = 0; u < 8; u++) t += v8[u];
-                for (unsigned b = lane + 256u; b < gridDim.x; b += 32) t += __ldcg(part + b * PPE_PARTS + k);
-                t = warp_sum_d(t);
-                if (lane == 0) result[k] = t;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence();
-                atomicExch(bar, 0u);
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            }
-        }
-    } else if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
-        unsigned long long it = 0;
-        while (*gen == gen0) {
-            if (++it > (1ull << 24)) {
-                atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
-                ok = 0;
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; k++) out[k] = __ldcg(result + k);
-    const bool good = ok != 0;
-    __syncthreads();
-    return good;
+    for (int k = 0; k < K; k++) out[k] = tot_s[k];
+    return ok_s != 0;
 }
 
 // ---------------------------------------------------------------- assembly
@@ -1412,7 +1409,7 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     w.threads = PPE_THREADS;
     w.blocks = sms * per_sm;
     // partials sized for the smallest block shape (4 blocks per SM)
-    ok &= al((void**)&w.part, (size_t)sms * 4 * PPE_PARTS * sizeof(double));
+    ok &= al((void**)&w.part, (size_t)sms * 4 * 2 * PPE_PARTS * sizeof(double));  // two buffers (grid_reduce)
     ok &= al((void**)&w.result, PPE_PARTS * sizeof(double));
     ok &= al((void**)&w.bar, 2 * sizeof(unsigned));
     if (!ok) {
