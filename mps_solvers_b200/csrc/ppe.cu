@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
-#pragma unroll 2
+#pragma unroll 4  // measured: 4 chunks per step beat 2 (and a cp.async ring)
                 for (uint32_t t = 0; t < T; t++) {
                     const uint4 c = ld_mat(cols + 32 * t, pol);
                     const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
@@ -713,7 +713,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_pipe(PipeArgs S) {
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
-#pragma unroll 2
+#pragma unroll 4
                 for (uint32_t t = 0; t < T; t++) {
                     const uint4 c = ld_mat(cols + 32 * t, pol);
                     const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
