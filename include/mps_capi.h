@@ -318,6 +318,25 @@ mps_status mps_batch_scene_info(mps_handle* h, uint32_t scene, mps_scene_info* i
 /* Set the tank acceleration of a scene (scene 0 of a single-scene handle). */
 mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float accel_amp, float accel_freq);
 
+/* ---- prescribed boundary motion ----
+ * Replaces the reference's hook MOTION::doMotion(pos, vel, np)
+ * (MPS_CAL_/MOTION.cpp:11-16), which MPS_GPU::motion (MPS_CAL_/MPS_GPU.cpp:
+ * 1670-1673) calls as the first, commented-out statement of a step, before
+ * divideCell (MPS_CAL_/MPS_GPU_EXPL.cpp:93-95).  mps_add_wall_motion selects
+ * the wall and dummy particles (types 1 and 2) that lie inside [lo, hi] now
+ * and belong to no earlier motion, and moves them rigidly from then on: at the
+ * start of every step, with tau = time - (time of this call),
+ *   x = x0 + vel tau + amp (sin(omega tau + phase) - sin(phase)),
+ *   u = vel + amp omega cos(omega tau + phase),   omega = 2 pi freq,
+ * x0 the position at selection, followed by a cell rebuild (a wave maker,
+ * piston or oscillating plate).  Up to 8 motions per handle; single-scene
+ * handles only.  *selected (may be NULL) receives the number of particles
+ * taken.  The particles must stay inside the grid. */
+mps_status mps_add_wall_motion(mps_handle* h, const float lo[3], const float hi[3], const float vel[3],
+                               const float amp[3], float freq, float phase, uint32_t* selected);
+/* Stop every motion; the moved particles stay where they are, at rest. */
+mps_status mps_clear_wall_motion(mps_handle* h);
+
 /* ---- free surface by marching cubes ----
  * The reference's iso-surface (MPS_CAL_expl_gl_v3.1: MPS_GPU::calVertex_n,
  * calTriangle, calNorm) as a headless triangle buffer.  Vertex value n_v =

@@ -42,7 +42,8 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_batch_create", "mps_batch_step", "mps_batch_scene_info", "mps_set_body_force",
            "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
            "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
-           "mps_surface_case_table", "mps_precond_tensor_cores")
+           "mps_surface_case_table", "mps_precond_tensor_cores", "mps_add_wall_motion",
+           "mps_clear_wall_motion")
 
 
 class mps_options(C.Structure):
@@ -158,6 +159,8 @@ def lib():
             "mps_batch_step": (C.c_int, [H, C.c_int, C.POINTER(mps_step_stats)]),
             "mps_batch_scene_info": (C.c_int, [H, C.c_uint32, C.POINTER(mps_scene_info)]),
             "mps_set_body_force": (C.c_int, [H, C.c_uint32, C.c_float, C.c_float]),
+            "mps_add_wall_motion": (C.c_int, [H, Fp, Fp, Fp, Fp, C.c_float, C.c_float, U]),
+            "mps_clear_wall_motion": (C.c_int, [H]),
             "mps_autotune": (C.c_int, [H, C.c_int, C.POINTER(mps_tune_report)]),
             "mps_surface_setup": (C.c_int, [H, C.POINTER(mps_surface_grid), C.c_uint32]),
             "mps_surface_extract_async": (C.c_int, [H]),
@@ -417,6 +420,21 @@ class Simulation:
     def set_body_force(self, accel_amp: float, accel_freq: float, scene: int = 0):
         """Tank acceleration accel_amp*sin(2*pi*accel_freq*t) along x."""
         self._check(lib().mps_set_body_force(self.h, scene, accel_amp, accel_freq))
+
+    def add_wall_motion(self, lo, hi, vel=(0.0, 0.0, 0.0), amp=(0.0, 0.0, 0.0), freq: float = 0.0,
+                        phase: float = 0.0) -> int:
+        """Move the wall and dummy particles inside the box [lo, hi] rigidly
+        from now on: x = x0 + vel*tau + amp*(sin(2*pi*freq*tau + phase) -
+        sin(phase)), tau = time since this call.  Returns how many were taken."""
+        f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+        n = C.c_uint32()
+        self._check(lib().mps_add_wall_motion(self.h, f3(lo), f3(hi), f3(vel), f3(amp), freq, phase,
+                                              C.byref(n)))
+        return n.value
+
+    def clear_wall_motion(self):
+        """Stop every wall motion (the moved particles stay, at rest)."""
+        self._check(lib().mps_clear_wall_motion(self.h))
 
     def scene_info(self, scene: int = 0) -> mps_scene_info:
         info = mps_scene_info()

@@ -75,6 +75,11 @@ struct mps_handle {
     std::string graph_note;
     int stage_threads = 256;         // block size of the particle-stage kernels (autotuned)
     SurfaceWork surf;                // marching-cubes free surface
+    // prescribed boundary motions (allocated by the first mps_add_wall_motion)
+    MotionSet mot{};
+    uint32_t* motion_of = nullptr;   // per GEO.dat id
+    float4* motion_x0 = nullptr;     // per GEO.dat id
+    uint32_t* motion_count = nullptr;
 };
 
 static void drop_graphs(mps_handle* h);
@@ -142,10 +147,11 @@ static StageArgs stage_args(mps_handle* h) {
 
 // Stage tags of mps_profile_steps (names in kStageNames).
 enum { ST_UPDATE_DT = 0, ST_VISC, ST_COLLISION, ST_PND, ST_PRESSURE, ST_DASH, ST_STEP_END, ST_KEYS, ST_SORT,
-       ST_CELLS, ST_GATHER, ST_PPE_SOLVE, ST_COUNT };
+       ST_CELLS, ST_GATHER, ST_PPE_SOLVE, ST_MOTION, ST_COUNT };
 static const char* kStageNames[ST_COUNT] = {"update_dt", "visc",       "collision",  "pnd",
                                             "pressure",  "dash",       "step_end",   "cell_keys",
-                                            "radix_sort", "cell_table", "gather",     "ppe_solve"};
+                                            "radix_sort", "cell_table", "gather",     "ppe_solve",
+                                            "motion"};
 
 static void mark(mps_handle* h, int tag) {
     if (!h->prof_on) return;
@@ -187,6 +193,12 @@ static void enqueue_step(mps_handle* h) {
     cudaStream_t st = h->stream;
     const uint32_t cap = h->cap;
     h->launches = 0;
+    if (h->mot.n) {  // the reference's motion(); divideCell(); at the top of a step
+        mark(h, ST_MOTION);
+        launch_motion(h->S[h->cur], h->sc, h->motion_of, h->motion_x0, h->mot, cap, st);
+        rebuild(h, APPLY_NONE);
+        h->launches += 1;
+    }
     mark(h, ST_UPDATE_DT);
     launch_update_dt(stage_args(h), cap, st);
     mark(h, ST_VISC);
@@ -863,6 +875,62 @@ extern "C" mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float ac
     h->P.body_omega = omega;
     // the captured steps hold the old constants
     CK(cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    return MPS_OK;
+}
+
+// ---------------------------------------------------------------- boundary motion
+extern "C" mps_status mps_add_wall_motion(mps_handle* h, const float lo[3], const float hi[3], const float vel[3],
+                                          const float amp[3], float freq, float phase, uint32_t* selected) {
+    if (!h || !lo || !hi || !vel || !amp) return MPS_ERR_INVALID;
+    if (h->nscenes) {
+        h->err = "wall motions are for single-scene handles";
+        return MPS_ERR_INVALID;
+    }
+    if (h->mot.n >= MPS_MAX_MOTIONS) {
+        h->err = "at most " + std::to_string(MPS_MAX_MOTIONS) + " wall motions";
+        return MPS_ERR_INVALID;
+    }
+    CK(cudaSetDevice(h->dev));
+    if (!h->motion_of) {
+        CK(dalloc(h, &h->motion_of, h->cap));
+        CK(dalloc(h, &h->motion_x0, h->cap));
+        CK(dalloc(h, &h->motion_count, 1));
+        CK(cudaMemsetAsync(h->motion_of, 0xFF, (size_t)h->cap * 4, h->stream));
+    }
+    const int m = h->mot.n;
+    CK(cudaMemsetAsync(h->motion_count, 0, 4, h->stream));
+    launch_motion_select(h->S[h->cur], h->sc, lo, hi, (uint32_t)m, h->motion_of, h->motion_x0, h->motion_count,
+                         h->cap, h->stream);
+    CK(cudaGetLastError());
+    uint32_t count = 0;
+    Scalars sc;
+    CK(cudaMemcpyAsync(&count, h->motion_count, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&sc, h->sc, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->mot.t0[m] = (double)sc.time;
+    for (int c = 0; c < 3; c++) {
+        h->mot.vel[m][c] = (double)vel[c];
+        h->mot.amp[m][c] = (double)amp[c];
+    }
+    h->mot.omega[m] = 2.0 * M_PI * (double)freq;
+    h->mot.phase[m] = (double)phase;
+    h->mot.n = m + 1;
+    if (selected) *selected = count;
+    drop_graphs(h);  // the captured steps hold the old motion set
+    return MPS_OK;
+}
+
+extern "C" mps_status mps_clear_wall_motion(mps_handle* h) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    if (h->motion_of) {
+        launch_motion_stop(h->S[h->cur], h->sc, h->motion_of, h->cap, h->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemsetAsync(h->motion_of, 0xFF, (size_t)h->cap * 4, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->mot.n = 0;
     drop_graphs(h);
     return MPS_OK;
 }

@@ -769,4 +769,70 @@ void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint3
     k_normals<<<blocks_for(cap, 256), 256, 0, st>>>(a, reach, normal_id_of);
 }
 
+// ---------------------------------------------------------------- boundary motion
+// The reference's hook MOTION::doMotion(pos, vel, np) (MPS_CAL_/MOTION.cpp:11-16,
+// an empty loop there) is called by MPS_GPU::motion (MPS_CAL_/MPS_GPU.cpp:
+// 1670-1673) as the first, commented-out statement of a step, followed by
+// divideCell (MPS_CAL_/MPS_GPU_EXPL.cpp:93-95).  This is one concrete motion
+// law for it; the arithmetic is spelled out (no contraction) so it matches
+// the oracle's double expressions.
+__global__ void k_motion_select(State s, const Scalars* sc, float3 lo, float3 hi, uint32_t m,
+                                uint32_t* __restrict__ motion_of, float4* __restrict__ x0, uint32_t* count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sc->np) return;
+    const float4 p = s.pos[i];
+    const uint32_t t = ptype(p);
+    if (t != T_WALL && t != T_DUMMY) return;
+    if (p.x < lo.x || p.x > hi.x || p.y < lo.y || p.y > hi.y || p.z < lo.z || p.z > hi.z) return;
+    const uint32_t id = s.id[i];
+    if (motion_of[id] != NO_MOTION) return;
+    motion_of[id] = m;
+    x0[id] = p;
+    atomicAdd(count, 1u);
+}
+
+__global__ void k_motion(State s, const Scalars* sc, const uint32_t* __restrict__ motion_of,
+                         const float4* __restrict__ x0, MotionSet M) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sc->np) return;
+    const uint32_t m = motion_of[s.id[i]];
+    if (m == NO_MOTION) return;
+    const float4 a = x0[s.id[i]];
+    const double tau = __dsub_rn((double)sc->time, M.t0[m]);
+    const double arg = __dadd_rn(__dmul_rn(M.omega[m], tau), M.phase[m]);
+    const double sn = __dsub_rn(sin(arg), sin(M.phase[m]));
+    const double cs = __dmul_rn(M.omega[m], cos(arg));
+    const double xa[3] = {(double)a.x, (double)a.y, (double)a.z};
+    float xn[3], un[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        xn[c] = (float)__dadd_rn(__dadd_rn(xa[c], __dmul_rn(M.vel[m][c], tau)), __dmul_rn(M.amp[m][c], sn));
+        un[c] = (float)__dadd_rn(M.vel[m][c], __dmul_rn(M.amp[m][c], cs));
+    }
+    const float4 p = s.pos[i];
+    s.pos[i] = make_float4(xn[0], xn[1], xn[2], p.w);
+    s.vel[i] = make_float4(un[0], un[1], un[2], s.vel[i].w);
+}
+
+__global__ void k_motion_stop(State s, const Scalars* sc, const uint32_t* __restrict__ motion_of) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sc->np || motion_of[s.id[i]] == NO_MOTION) return;
+    s.vel[i] = make_float4(0.f, 0.f, 0.f, s.vel[i].w);
+}
+
+void launch_motion_stop(const State& s, const Scalars* sc, const uint32_t* motion_of, uint32_t cap, cudaStream_t st) {
+    k_motion_stop<<<blocks_for(cap, 256), 256, 0, st>>>(s, sc, motion_of);
+}
+
+void launch_motion_select(const State& s, const Scalars* sc, const float lo[3], const float hi[3], uint32_t m,
+                          uint32_t* motion_of, float4* x0, uint32_t* count, uint32_t cap, cudaStream_t st) {
+    k_motion_select<<<blocks_for(cap, 256), 256, 0, st>>>(s, sc, make_float3(lo[0], lo[1], lo[2]),
+                                                         make_float3(hi[0], hi[1], hi[2]), m, motion_of, x0, count);
+}
+
+void launch_motion(const State& s, const Scalars* sc, const uint32_t* motion_of, const float4* x0,
+                   const MotionSet& M, uint32_t cap, cudaStream_t st) {
+    k_motion<<<blocks_for(cap, 256), 256, 0, st>>>(s, sc, motion_of, x0, M);
+}
+
 }  // namespace mpsb

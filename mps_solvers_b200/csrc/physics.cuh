@@ -127,4 +127,26 @@ void launch_lambda(const StageArgs& a, const unsigned long long* best, float* la
 // type-2 particle, stored by GEO.dat index
 void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint32_t cap, cudaStream_t st);
 
+// Prescribed rigid motions of boundary particles (the reference's
+// MOTION::doMotion hook).  Motion m moves its particles to
+// x0 + vel tau + amp (sin(omega tau + phase) - sin(phase)) with velocity
+// vel + amp omega cos(omega tau + phase), tau = time - t0 (double, rounded
+// once to float), at the start of every step.
+constexpr int MPS_MAX_MOTIONS = 8;
+constexpr uint32_t NO_MOTION = 0xFFFFFFFFu;
+struct MotionSet {
+    int n = 0;
+    double t0[MPS_MAX_MOTIONS], vel[MPS_MAX_MOTIONS][3], amp[MPS_MAX_MOTIONS][3], omega[MPS_MAX_MOTIONS],
+        phase[MPS_MAX_MOTIONS];
+};
+// give motion m to the wall and dummy particles inside [lo, hi] that have
+// none (motion_of and x0 are indexed by GEO.dat id); adds the count to *count
+void launch_motion_select(const State& s, const Scalars* sc, const float lo[3], const float hi[3], uint32_t m,
+                          uint32_t* motion_of, float4* x0, uint32_t* count, uint32_t cap, cudaStream_t st);
+// set the velocity of every particle with a motion to zero
+void launch_motion_stop(const State& s, const Scalars* sc, const uint32_t* motion_of, uint32_t cap, cudaStream_t st);
+// place the moving particles for the step starting at sc->time
+void launch_motion(const State& s, const Scalars* sc, const uint32_t* motion_of, const float4* x0,
+                   const MotionSet& M, uint32_t cap, cudaStream_t st);
+
 }  // namespace mpsb

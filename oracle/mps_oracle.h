@@ -49,6 +49,10 @@ typedef struct orc_state orc_state;
     int orc_step_##S(orc_state* st);                                                   \
     void orc_set_cg_##S(orc_state* st, int relative, double tol, int max_iter);        \
     void orc_set_body_force_##S(orc_state* st, double amp, double freq);               \
+    int orc_add_wall_motion_##S(orc_state* st, const double* lo, const double* hi,      \
+                                const double* vel, const double* amp, double freq,     \
+                                double phase);                                         \
+    void orc_clear_wall_motion_##S(orc_state* st);                                     \
     void orc_counts_##S(const orc_state* st, uint32_t* np, uint32_t* nb2,              \
                         uint32_t* nb1, uint32_t* nexcl, uint32_t* ncells);             \
     void orc_scalars_##S(const orc_state* st, double* out16);                          \

@@ -54,6 +54,10 @@ def lib():
             getattr(L, f"orc_step_{s}").restype = C.c_int
             getattr(L, f"orc_set_cg_{s}").argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
             getattr(L, f"orc_set_body_force_{s}").argtypes = [C.c_void_p, C.c_double, C.c_double]
+            D3 = C.c_double * 3
+            getattr(L, f"orc_add_wall_motion_{s}").argtypes = [C.c_void_p, D3, D3, D3, D3, C.c_double, C.c_double]
+            getattr(L, f"orc_add_wall_motion_{s}").restype = C.c_int
+            getattr(L, f"orc_clear_wall_motion_{s}").argtypes = [C.c_void_p]
             getattr(L, f"orc_counts_{s}").argtypes = [C.c_void_p] + [U] * 5
             getattr(L, f"orc_scalars_{s}").argtypes = [C.c_void_p, C.POINTER(C.c_double)]
             getattr(L, f"orc_get_state_{s}").argtypes = [C.c_void_p, U, U, P, P, P, P]
@@ -111,6 +115,22 @@ class Oracle:
         taken as float32 values, as the GPU API takes them)."""
         self._f("set_body_force")(self.h, C.c_double(float(np.float32(amp))),
                                   C.c_double(float(np.float32(freq))))
+
+    def add_wall_motion(self, lo, hi, vel=(0.0, 0.0, 0.0), amp=(0.0, 0.0, 0.0), freq: float = 0.0,
+                        phase: float = 0.0) -> int:
+        """Prescribed motion of the wall and dummy particles inside [lo, hi]
+        (all values taken as float32, as the GPU API takes them); returns the
+        number selected."""
+        D3 = C.c_double * 3
+        f = lambda v: D3(*[float(np.float32(x)) for x in v])
+        n = self._f("add_wall_motion")(self.h, f(lo), f(hi), f(vel), f(amp), float(np.float32(freq)),
+                                       float(np.float32(phase)))
+        if n < 0:
+            raise RuntimeError("too many wall motions")
+        return n
+
+    def clear_wall_motion(self):
+        self._f("clear_wall_motion")(self.h)
 
     def step(self, n: int = 1) -> int:
         st = 0
