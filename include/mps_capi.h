@@ -97,7 +97,11 @@ typedef struct {
                             it stays in L2 across CG iterations while the rest
                             streams as evict_first (0: half the L2; -1: no
                             hints)                                            */
-    uint32_t reserved[5];
+    int visc_implicit;   /* semi-implicit single scenes: 1 = viscosity by
+                            Crank-Nicolson, three PCG solves a step (the
+                            reference's MPS_CPU_IMPL / MPS_GPU_IMPL step,
+                            MPS_CAL_v4.0/MPS_CPU_IMPL.cpp:79-338); 0 = explicit */
+    uint32_t reserved[4];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

@@ -48,6 +48,7 @@ struct mps_handle {
     unsigned long long* best = nullptr;
     float* lambda_dev = nullptr;
     PpeWork ppe{};
+    PpeWork cn{};  // Crank-Nicolson viscosity system (options.visc_implicit)
     Staging stage{};
     // graphs, one per buffer parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -202,8 +203,16 @@ static void enqueue_step(mps_handle* h) {
     mark(h, ST_UPDATE_DT);
     launch_update_dt(stage_args(h), cap, st);
     mark(h, ST_VISC);
-    launch_visc(stage_args(h), cap, st);
-    rebuild(h, APPLY_SET_VEL);
+    if (h->cn.ready) {  // MPS_CPU_IMPL::visCrankNicolson: x, y, z in turn, then divideCell
+        for (int c = 0; c < (int)h->g.dim; c++) {
+            h->launches += ppe_enqueue_cn(h->cn, stage_args(h), h->opt, c, h->ppe.n0_64, h->ppe.lambda64, cap, st);
+            if (h->cn.launch_err != cudaSuccess) h->launch_err = h->cn.launch_err;
+        }
+        rebuild(h, APPLY_NONE);
+    } else {
+        launch_visc(stage_args(h), cap, st);
+        rebuild(h, APPLY_SET_VEL);
+    }
     mark(h, ST_COLLISION);
     launch_collision(stage_args(h), cap, st);
     rebuild(h, APPLY_ADD_VEL);
@@ -478,6 +487,10 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     }
     apply_constants(P, h->hc);
 
+    if (h->opt.visc_implicit && h->opt.method != MPS_METHOD_SEMI_IMPLICIT) {
+        h->err = "Crank-Nicolson viscosity needs the semi-implicit method";
+        return MPS_ERR_INVALID;
+    }
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
         int e = ppe_setup(h->ppe, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
@@ -492,6 +505,12 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         if (h->opt.precond == MPS_PRECOND_LEARNED) {
             e = ppe_enable_learned(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
+        }
+        if (h->opt.visc_implicit) {
+            e = ppe_setup(h->cn, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
+            if (e != MPS_OK) return (mps_status)e;
+            h->cn.write_pressure = false;
+            h->cn.l2_keep_entries = h->ppe.l2_keep_entries;
         }
     }
     Scalars s;
@@ -800,6 +819,10 @@ extern "C" mps_status mps_batch_create(const mps_scene_spec* scenes, uint32_t ns
         h->err = "a batch holds at most " + std::to_string(PPE_MAX_SCENES) + " scenes";
         return MPS_ERR_INVALID;
     }
+    if (h->opt.visc_implicit) {
+        h->err = "Crank-Nicolson viscosity is for single-scene handles";
+        return MPS_ERR_INVALID;
+    }
     std::vector<mps_params> prms(nscenes);
     std::vector<Geo> geos(nscenes);
     for (uint32_t s = 0; s < nscenes; s++) {
@@ -943,6 +966,7 @@ extern "C" void mps_destroy(mps_handle* h) {
         if (h->graph[b]) cudaGraphExecDestroy(h->graph[b]);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     ppe_free(h->ppe);
+    ppe_free(h->cn);
     surface_free(h->surf);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);

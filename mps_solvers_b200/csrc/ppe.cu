@@ -1436,6 +1436,28 @@ static cudaError_t launch_cooperative(const void* fn, int blocks, int threads, v
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
+// The ordered list of non-Dirichlet rows and their SELL-8 layout (with the
+// stored weights), from the assembled row-major system.
+static int enqueue_rows_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
+    k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
+    launch_scan_exclusive(w.tilecnt, ntiles, st);
+    k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
+    int launched = 6;
+    if (a.batch.n) {
+        k_row_scene<<<blocks_for(cap, 256), 256, 0, st>>>(w.rowlist, w.nrows, a.cur.id, a.batch.sid_of_id, w.row_scene,
+                                                          cap);
+        launched++;
+    }
+    // SELL-8 layout of the non-Dirichlet rows
+    const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
+    k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
+    launch_scan_exclusive(w.sell_off, maxslices + 1, st);
+    k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.wrm, w.rlen, w.rowlist, w.nrows,
+                                                                  w.sell_off, w.sell_cols, w.sell_w);
+    return launched;
+}
+
 int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {
     (void)opt;
     AsmArgs A;
@@ -1467,22 +1489,7 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         if (a.exact) k_ppe_assemble<true, false><<<warps_blocks, 256, 0, st>>>(A);
         else k_ppe_assemble<false, false><<<warps_blocks, 256, 0, st>>>(A);
     }
-    const uint32_t ntiles = (cap + ROW_TILE - 1) / ROW_TILE;
-    k_rows_count<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt);
-    launch_scan_exclusive(w.tilecnt, ntiles, st);
-    k_rows_scatter<<<ntiles, 256, 0, st>>>(w.rlen, a.sc, w.tilecnt, ntiles, w.rowlist, w.nrows);
-    int launched = 7;
-    if (a.batch.n) {
-        k_row_scene<<<blocks_for(cap, 256), 256, 0, st>>>(w.rowlist, w.nrows, a.cur.id, a.batch.sid_of_id, w.row_scene,
-                                                          cap);
-        launched++;
-    }
-    // SELL-8 layout of the non-Dirichlet rows
-    const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
-    k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
-    launch_scan_exclusive(w.sell_off, maxslices + 1, st);
-    k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.wrm, w.rlen, w.rowlist, w.nrows,
-                                                                  w.sell_off, w.sell_cols, w.sell_w);
+    int launched = 1 + enqueue_rows_pack(w, a, cap, st);
     // the state this system was assembled from
     cudaMemcpyAsync(w.pos_snap, a.cur.pos, (size_t)cap * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
@@ -1599,6 +1606,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
                               : (a.exact ? (const void*)k_ppe_solve_batch<true, false>
                                          : (const void*)k_ppe_solve_batch<false, false>);
         w.launch_err = launch_cooperative(bfn, w.blocks, w.threads, bargs, st);
+        if (!w.write_pressure) return 1;
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
@@ -1642,6 +1650,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
                               ? (a.exact ? (const void*)k_ppe_solve_pipe<true, true> : (const void*)k_ppe_solve_pipe<false, true>)
                               : (a.exact ? (const void*)k_ppe_solve_pipe<true, false> : (const void*)k_ppe_solve_pipe<false, false>);
         w.launch_err = launch_cooperative(pfn, w.blocks, w.threads, pargs, st);
+        if (!w.write_pressure) return 1;
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
@@ -1654,8 +1663,156 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1, false> : (const void*)k_ppe_solve<true, 0, false>)
                      : (learned ? (const void*)k_ppe_solve<false, 1, false> : (const void*)k_ppe_solve<false, 0, false>);
     w.launch_err = launch_cooperative(fn, w.blocks, w.threads, args, st);
+    if (!w.write_pressure) return 1;
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
     return 2;
+}
+
+// ---------------------------------------------------------------- Crank-Nicolson viscosity
+// MPS_CPU_IMPL::buildCG_CN<dir> (MPS_CAL_v4.0/MPS_CPU_IMPL.cpp:195-305) for
+// velocity component c, on the PPE's data layout: a fluid row holds
+//   A_ij = w_ij (fluid j), A_ii = -sum_j w_ij - 1/R,
+//   b_i = -sum_j w_ij (u_j - u_i) - sum_{j boundary} w_ij u_j - u_i/R - dt g_c/R
+// over every neighbour j != i within rlap (all types; w = rlap/r - 1), with
+// 1/R = lambda n0 / (dim niu dt) and g the step's body force; other rows are
+// Dirichlet (the reference's identity rows, x = u).  x starts at u.  One warp
+// per particle scans the full 27 linked cells: components after the first
+// see positions the earlier ones moved since the last cell rebuild, which
+// the distance culling of the stage kernels does not allow for.
+struct CnArgs {
+    StageArgs a;
+    int c;
+    uint32_t* cols;
+    float* wrm;
+    uint32_t* rlen;
+    double* diag64;
+    float* diag32;
+    float* inv_diag;
+    double* b64;
+    double* x64;
+    unsigned* bar;
+    double lambda_n0_over_dim_niu;  // lambda n0 / (dim niu): 1/R = this / dt
+};
+
+__device__ __forceinline__ float comp(const float4& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+template <bool EX>
+__global__ void __launch_bounds__(256) k_cn_assemble(CnArgs A) {
+    const StageArgs& a = A.a;
+    const uint32_t n = a.sc->np;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.bar[0] = 0u;  // the solver's barrier starts empty
+    if (i >= n) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 pi = pos[i];
+    const double ui = (double)comp(vel[i], A.c);
+    if (ptype(pi) != T_FLUID) {
+        if (lane == 0) {
+            A.rlen[i] = PPE_DIRICHLET;
+            A.diag64[i] = 1.0;
+            A.diag32[i] = 1.0f;
+            A.inv_diag[i] = 1.0f;
+            A.b64[i] = ui;
+            A.x64[i] = ui;
+        }
+        return;
+    }
+    const Local L = local_of<false>(a, i);
+    const float re = a.P.rlap, thr = a.P.rlap_thr;
+    uint32_t* cols = A.cols + (size_t)i * PPE_W;
+    float* wrow = A.wrm + (size_t)i * PPE_W;
+    uint32_t count = 0;
+    double diag = 0.0, bi = 0.0;
+    const int rows = link_rows(L.g);
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int row = 0; row < rows; row++) {
+        const RowRange rg = link_row(L.g, L.cs, L.c, row);
+        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+            const uint32_t j = base + lane;
+            bool app = false;
+            float w = 0.f;
+            if (j < rg.hi && j != i) {
+                const float4 pj = __ldg(pos + j);
+                const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                if (rr < thr) w = weight_rr<EX>(re, rr);
+                if (w > 0.f) {
+                    const double uj = (double)comp(__ldg(vel + j), A.c);
+                    bi -= (uj - ui) * (double)w;
+                    if (ptype(pj) != T_FLUID) bi -= (double)w * uj;
+                    else app = true;
+                }
+            }
+            diag += (double)w;
+            const uint32_t m = __ballot_sync(0xffffffffu, app);
+            if (app) {
+                const uint32_t k = count + __popc(m & lt);
+                if (k < PPE_W) {
+                    cols[k] = j;
+                    wrow[k] = w;
+                }
+            }
+            count += __popc(m);
+        }
+    }
+    diag = warp_sum_d(diag);
+    bi = warp_sum_d(bi);
+    if (lane == 0) {
+        if (count > PPE_W) {
+            atomicOr(&a.sc->err, ERR_CAPACITY);
+            count = PPE_W;
+        }
+        const double one_over_R = A.lambda_n0_over_dim_niu / (double)a.sc->dt;
+        const double dg = -diag - one_over_R;
+        A.rlen[i] = count;
+        A.diag64[i] = dg;
+        A.diag32[i] = (float)dg;
+        A.inv_diag[i] = (float)(1.0 / dg);
+        A.b64[i] = bi - (one_over_R * ui + A.lambda_n0_over_dim_niu * (double)a.sc->g_eff[A.c]);
+        A.x64[i] = ui;
+    }
+}
+
+// MPS_CPU_IMPL::updatePosVel<dir> (MPS_CAL_v4.0/MPS_CPU_IMPL.cpp:129-190):
+// fluid u_c = x, x_c += dt u_c.
+__global__ void k_cn_finish(const double* __restrict__ x64, const uint32_t* __restrict__ rlen, State s, int c,
+                            const Scalars* sc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sc->np || rlen[i] == PPE_DIRICHLET) return;
+    const float x = (float)x64[i];
+    float4 u = s.vel[i], p = s.pos[i];
+    const float np_ = __fadd_rn(comp(p, c), __fmul_rn(sc->dt, x));
+    if (c == 0) { u.x = x; p.x = np_; }
+    else if (c == 1) { u.y = x; p.y = np_; }
+    else { u.z = x; p.z = np_; }
+    s.vel[i] = u;
+    s.pos[i] = p;
+}
+
+int ppe_enqueue_cn(PpeWork& w, const StageArgs& a, const mps_options& opt, int c, double n0, double lambda,
+                   uint32_t cap, cudaStream_t st) {
+    CnArgs A;
+    A.a = a;
+    A.c = c;
+    A.cols = w.cols;
+    A.wrm = w.wrm;
+    A.rlen = w.rlen;
+    A.diag64 = w.diag64;
+    A.diag32 = w.diag32;
+    A.inv_diag = w.inv_diag;
+    A.b64 = w.b64;
+    A.x64 = w.x64;
+    A.bar = w.bar;
+    A.lambda_n0_over_dim_niu = lambda * n0 / ((double)a.P.dim_f * (double)a.P.niu);
+    const uint32_t warps_blocks = blocks_for(cap * 32u, 256);
+    if (a.exact) k_cn_assemble<true><<<warps_blocks, 256, 0, st>>>(A);
+    else k_cn_assemble<false><<<warps_blocks, 256, 0, st>>>(A);
+    int launched = 1 + enqueue_rows_pack(w, a, cap, st);
+    launched += ppe_enqueue_solve(w, a, opt, cap, st);
+    k_cn_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur, c, a.sc);
+    return launched + 1;
 }
 
 int ppe_set_threads(PpeWork& w, int threads) {

@@ -61,6 +61,7 @@ struct PpeWork {
     float* sell_w = nullptr;           // the entries' weights, same layout
     bool stored_weights = true;        // SpMV reads sell_w (else recomputes from positions)
     bool pipelined = false;            // single-reduction pipelined PCG (diagonal scaling)
+    bool write_pressure = true;        // the solve ends by writing p = max(x, 0) (the PPE; not the viscosity)
     uint32_t l2_keep_entries = 0xFFFFFFFFu;  // matrix entries kept in L2 across iterations (all: no hints)
     // vectors of the pipelined solver
     float *pu = nullptr, *pw = nullptr, *pz = nullptr, *pq = nullptr, *ps = nullptr, *pp = nullptr;
@@ -100,6 +101,11 @@ LpSystem ppe_lp_system(const PpeWork& w, const StageArgs& a);
 int ppe_enable_learned(PpeWork& w, std::string* err);
 // the persistent solve and p = max(x, 0); returns the kernels enqueued
 int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
+// Crank-Nicolson viscosity (MPS_CPU_IMPL::visCrankNicolson) for velocity
+// component c on a PpeWork of its own: assembly, rows, pack, the persistent
+// PCG, and u_c = x, x_c += dt u_c for the fluid.  Returns the launches.
+int ppe_enqueue_cn(PpeWork& w, const StageArgs& a, const mps_options& opt, int c, double n0, double lambda,
+                   uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);
 // the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
 // either way); MPS_ERR_INVALID when the device cannot hold that shape

@@ -53,6 +53,7 @@ typedef struct orc_state orc_state;
                                 const double* vel, const double* amp, double freq,     \
                                 double phase);                                         \
     void orc_clear_wall_motion_##S(orc_state* st);                                     \
+    void orc_set_visc_implicit_##S(orc_state* st, int on);                             \
     void orc_counts_##S(const orc_state* st, uint32_t* np, uint32_t* nb2,              \
                         uint32_t* nb1, uint32_t* nexcl, uint32_t* ncells);             \
     void orc_scalars_##S(const orc_state* st, double* out16);                          \

@@ -58,6 +58,7 @@ def lib():
             getattr(L, f"orc_add_wall_motion_{s}").argtypes = [C.c_void_p, D3, D3, D3, D3, C.c_double, C.c_double]
             getattr(L, f"orc_add_wall_motion_{s}").restype = C.c_int
             getattr(L, f"orc_clear_wall_motion_{s}").argtypes = [C.c_void_p]
+            getattr(L, f"orc_set_visc_implicit_{s}").argtypes = [C.c_void_p, C.c_int]
             getattr(L, f"orc_counts_{s}").argtypes = [C.c_void_p] + [U] * 5
             getattr(L, f"orc_scalars_{s}").argtypes = [C.c_void_p, C.POINTER(C.c_double)]
             getattr(L, f"orc_get_state_{s}").argtypes = [C.c_void_p, U, U, P, P, P, P]
@@ -128,6 +129,10 @@ class Oracle:
         if n < 0:
             raise RuntimeError("too many wall motions")
         return n
+
+    def set_visc_implicit(self, on: bool = True):
+        """Viscosity by Crank-Nicolson (the reference's MPS_CPU_IMPL step)."""
+        self._f("set_visc_implicit")(self.h, int(on))
 
     def clear_wall_motion(self):
         self._f("clear_wall_motion")(self.h)
