@@ -11,8 +11,11 @@
 //   REF_SEMI build: drives MPS_CPU_EXPL from MPS_CAL_v4.0 (real = double),
 //                   the semi-implicit step with the dense PPE + CG
 //                   (MPS_CAL_v4.0/MPS_CPU_EXPL.cpp:79-135).
+//   REF_IMPL build: drives MPS_CPU_IMPL from MPS_CAL_v4.0, the same step with
+//                   the viscosity by Crank-Nicolson (three dense CG solves)
+//                   (MPS_CAL_v4.0/MPS_CPU_IMPL.cpp:79-338).
 //
-// usage: ref_{expl,semi} <workdir> <nsteps> <dump_every> <out.bin> <threads>
+// usage: ref_{expl,semi,impl} <workdir> <nsteps> <dump_every> <out.bin> <threads>
 //   workdir holds input.dat and GEO.dat (the reference reads both from the
 //   current directory); stdout of the reference goes to workdir/stdout.txt.
 //   Prints one JSON line on stderr with the step-loop wall time.
@@ -30,6 +33,9 @@
 #include "MPS_GPU_EXPL.h"
 using namespace mytype;
 typedef MPS_GPU_EXPL RefBase;
+#elif defined(REF_IMPL)
+#include "MPS_CPU_IMPL.h"
+typedef MPS_CPU_IMPL RefBase;
 #else
 #include "MPS_CPU_EXPL.h"
 typedef MPS_CPU_EXPL RefBase;

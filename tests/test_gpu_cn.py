@@ -71,3 +71,21 @@ def test_cn_needs_semi_single_scene(capi, tmp_path):
         capi.Simulation(d, method=capi.METHOD_EXPLICIT, visc_implicit=1)
     with pytest.raises(capi.MPSError):
         capi.Simulation.batch([d, d], method=capi.METHOD_SEMI_IMPLICIT, visc_implicit=1)
+
+
+def test_cn_vs_reference_golden(capi, tmp_path):
+    """Against the reference's own MPS_CPU_IMPL build (MPS_CAL_v4.0, double,
+    dense CG, sequential collision), 6 steps at niu = 0.01, within the
+    semi-implicit tolerances."""
+    from helpers import load_golden, write_golden_case
+    g = load_golden("impl_tank")
+    d = write_golden_case(g, str(tmp_path / "impl"))
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, visc_implicit=1) as s:
+        s.step(6)
+        a = by_id(s.state())
+    b = by_id({f: g[f"s6_{f}"] for f in ("id", "type", "pos", "vel", "press", "n")})
+    assert np.array_equal(a["id"], b["id"]) and np.array_equal(a["type"], b["type"])
+    ext = np.abs(b["pos"]).max()
+    assert np.abs(a["pos"] - b["pos"]).max() / ext < 1e-6
+    assert rel_err(a["vel"], b["vel"]) < 1e-3
+    assert rel_err(a["press"], b["press"]) < 2e-3

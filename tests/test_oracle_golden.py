@@ -1,8 +1,9 @@
 """The CPU oracle against the reference's own outputs.
 
 The golden fixtures were produced by the reference's CPU step classes built
-from the reference sources (tests/golden/make_golden.py); the oracle must
-reproduce them bit for bit.  When the reference build is present
+from the reference sources (tests/golden/make_golden.py): the explicit EOS
+step, the semi-implicit step and the semi-implicit step with Crank-Nicolson
+viscosity; the oracle must reproduce them bit for bit.  When the reference build is present
 (oracle/_ref), a fresh seed is also run through both.
 """
 import os
@@ -15,13 +16,16 @@ from helpers import assert_bitwise, load_golden, write_golden_case
 FIELDS = ("id", "type", "pos", "vel", "press", "n")
 
 
-@pytest.mark.parametrize("name,variant,prec", [("expl_tank", 0, 32), ("semi_tank", 1, 64)])
+@pytest.mark.parametrize("name,variant,prec", [("expl_tank", 0, 32), ("semi_tank", 1, 64),
+                                               ("impl_tank", 1, 64)])
 def test_oracle_reproduces_reference_golden(oracle_mod, tmp_path, name, variant, prec):
     g = load_golden(name)
     d = write_golden_case(g, str(tmp_path / name))
     orc = oracle_mod.Oracle(d, variant, prec)
     if variant != 0:
         orc.set_cg(False)  # the reference's absolute r.r <= 1e-20 test
+    if name == "impl_tank":
+        orc.set_visc_implicit(True)  # MPS_CPU_IMPL: Crank-Nicolson viscosity
     sc = orc.scalars()
     assert sc["nzero"] == g["nzero"] and sc["lambda"] == g["lambda_"]
     cell_of, start, end = orc.cells()
