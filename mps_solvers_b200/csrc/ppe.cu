@@ -248,6 +248,8 @@ struct SolveArgs {
     float2* zp0;   // (z, p) per row, two buffers: current and next
     float2* zp1;
     float* q;
+    float* qp;        // the product's row sums of slice parts 1 .. PPE_MAX_SPLIT - 1
+    uint32_t cap;
     double* part;
     double* result;
     unsigned* bar;
@@ -354,6 +356,25 @@ __device__ __forceinline__ float lp_packed_row(const uint32_t* __restrict__ off,
 
 // SW: stored weights (the pack's) instead of recomputing them from the
 // positions; the two give the same matrix, the autotuner picks the faster.
+// Parts per slice of the CG product: 1 while there are at least as many
+// slices as warps (measured best at 310,912 particles), else enough parts to
+// give every warp work, at most PPE_MAX_SPLIT (33,072 particles: 0.63 ms ->
+// 0.47 ms per solve with 4).
+constexpr uint32_t PPE_MAX_SPLIT = 4;
+__device__ __forceinline__ uint32_t ppe_split(uint32_t nslices, uint32_t nwarps) {
+    if (nslices == 0 || nslices >= nwarps) return 1u;
+    const uint32_t p = (nwarps + nslices - 1) / nslices;
+    return p < PPE_MAX_SPLIT ? p : PPE_MAX_SPLIT;
+}
+
+// q_i of the last product: part 0's value plus the other parts' row sums,
+// added in part order
+__device__ __forceinline__ float q_total(const SolveArgs& S, uint32_t i, uint32_t parts) {
+    float v = S.q[i];
+    for (uint32_t p = 1; p < parts; p++) v += S.qp[(size_t)(p - 1) * S.cap + i];
+    return v;
+}
+
 template <bool EX, int PREC, bool SW>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them
@@ -365,6 +386,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     const uint32_t rsub = lane & 7, q = lane >> 3;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t parts = ppe_split(nslices, nw);
     const uint32_t* __restrict__ rowlist = S.rowlist;
     int total = 0, outers = 0;
     double relres = 0.0;
@@ -450,20 +472,27 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         double rz = tot[2];
         float beta = 0.f;
         for (int it = 0; it < S.inner_cap && total < S.max_iter; it++) {
-            // ---- q = A p_new with p_new = z + beta p (fused), p.q
+            // ---- q = A p_new with p_new = z + beta p (fused), p.q.  Work
+            // items are parts of a slice (`parts` chunk ranges), so that all
+            // warps have work when there are fewer slices than warps; part 0
+            // adds the diagonal and writes q, part p > 0 writes its row sums
+            // to qp[p - 1], and p.q adds every part's p_i * (its share of
+            // q_i), which is linear in the shares.
             double pq[1] = {0.0};
-            for (uint32_t sl = gw; sl < nslices; sl += nw) {
+            for (uint32_t u = gw; u < parts * nslices; u += nw) {
+                const uint32_t sl = u / parts, part = u % parts;
                 const uint32_t k = sl * SELL_C + rsub;
                 const uint32_t base = __ldg(S.off + sl);
                 const uint64_t pol = mat_policy(base, S.keep);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
+                const uint32_t t0 = part * T / parts, t1 = (part + 1) * T / parts;
                 const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
                 const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
 #pragma unroll 4  // measured: 4 chunks per step beat 2 (and a cp.async ring)
-                for (uint32_t t = 0; t < T; t++) {
+                for (uint32_t t = t0; t < t1; t++) {
                     const uint4 c = ld_mat(cols + 32 * t, pol);
                     const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                     const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
@@ -479,9 +508,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     const uint32_t i = __ldg(rowlist + k);
                     const float2 o = zc[i];
                     const float pn = fmaf(beta, o.y, o.x);
-                    const float qi = fmaf(S.diag32[i], pn, s);
-                    zn[i].y = pn;
-                    S.q[i] = qi;
+                    float qi = s;
+                    if (part == 0) {
+                        qi = fmaf(S.diag32[i], pn, s);
+                        zn[i].y = pn;
+                        S.q[i] = qi;
+                    } else {
+                        S.qp[(size_t)(part - 1) * S.cap + i] = s;
+                    }
                     pq[0] += (double)pn * (double)qi;
                 }
             }
@@ -497,7 +531,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     const uint32_t i = __ldg(rowlist + kk);
                     const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
-                    const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
+                    const float ri = fmaf(-alpha_f, q_total(S, i, parts), S.r[i]);
                     const float zi = ri * S.inv_diag[i];
                     S.r[i] = ri;
                     zn[i] = make_float2(zi, pn);
@@ -513,12 +547,13 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     const uint32_t i = __ldg(rowlist + kk);
                     const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
-                    const float ri = fmaf(-alpha_f, S.q[i], S.r[i]);
+                    const float ri = fmaf(-alpha_f, q_total(S, i, parts), S.r[i]);
                     rnew[i] = ri;
                     const float* r = S.r;
-                    const float* q = S.q;
-                    S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk,
-                                           [r, q, alpha_f](uint32_t j) { return fmaf(-alpha_f, q[j], r[j]); });
+                    const SolveArgs& SS = S;
+                    S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r, &SS, alpha_f, parts](uint32_t j) {
+                        return fmaf(-alpha_f, q_total(SS, j, parts), r[j]);
+                    });
                     acc2[1] += (double)ri * (double)ri;
                 }
                 double rrp[1] = {acc2[1]}, trr[1];
@@ -1373,6 +1408,7 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.zp[0], (size_t)cap * sizeof(float2));
     ok &= al((void**)&w.zp[1], (size_t)cap * sizeof(float2));
     ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
+    ok &= al((void**)&w.qp, (size_t)cap * (PPE_MAX_SPLIT - 1) * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
     ok &= al((void**)&w.y, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.ralt, (size_t)cap * sizeof(float));
@@ -1540,6 +1576,8 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.zp0 = w.zp[0];
     S.zp1 = w.zp[1];
     S.q = w.q;
+    S.qp = w.qp;
+    S.cap = cap;
     S.part = w.part;
     S.result = w.result;
     S.bar = w.bar;
@@ -1860,7 +1898,7 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.wrm, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
-                  w.r,    w.zp[0], w.zp[1], w.q,    w.part,     w.result, w.bar,
+                  w.r,    w.zp[0], w.zp[1], w.q,    w.qp,   w.part,     w.result, w.bar,
                   w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
                   w.id_snap, w.pu, w.pw, w.pz, w.pq, w.ps, w.pp, w.pm[0], w.pm[1], w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
                   w.scene_relres};

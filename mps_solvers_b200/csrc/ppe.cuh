@@ -49,7 +49,7 @@ struct PpeWork {
     float* inv_diag = nullptr;
     double* b64 = nullptr;
     double* x64 = nullptr;
-    float *r = nullptr, *q = nullptr;
+    float *r = nullptr, *q = nullptr, *qp = nullptr;
     float2* zp[2] = {nullptr, nullptr};  // (z, p) per row: current and next
     double* part = nullptr;            // blocks * PPE_PARTS
     double* result = nullptr;          // PPE_PARTS grid totals
