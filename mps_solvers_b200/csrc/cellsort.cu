@@ -81,21 +81,35 @@ __global__ void __launch_bounds__(SORT_THREADS) k_radix_upsweep(const uint32_t* 
     for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) hist[d * tiles + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of `total` counters by one block: chunks of 4096 entries,
-// each thread loading 4 consecutive counters (coalesced), a block scan of
-// the thread sums, and a running carry between chunks.
+// Exclusive scan of `total` counters by one block: chunks of 16384 entries,
+// each thread loading 16 consecutive counters as four 16-byte vectors (the
+// array starts 16-byte aligned), a block scan of the thread sums, and a
+// running carry between chunks.
 __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, uint32_t total) {
     __shared__ uint32_t warp_sums[32];
-    __shared__ uint32_t carry;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (uint32_t c0 = 0; c0 < total; c0 += 4096) {
-        const uint32_t b0 = c0 + 4 * threadIdx.x;
-        uint32_t v[4];
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < total; c0 += 16384) {
+        const uint32_t b0 = c0 + 16 * threadIdx.x;
+        const bool full = b0 + 16 <= total;
+        uint32_t v[16];
+        if (full) {
+            const uint4* p = reinterpret_cast<const uint4*>(a + b0);
 #pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = (b0 + u < total) ? a[b0 + u] : 0u;
-        const uint32_t s = v[0] + v[1] + v[2] + v[3];
+            for (int u = 0; u < 4; u++) {
+                const uint4 t = p[u];
+                v[4 * u] = t.x;
+                v[4 * u + 1] = t.y;
+                v[4 * u + 2] = t.z;
+                v[4 * u + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 16; u++) v[u] = (b0 + u < total) ? a[b0 + u] : 0u;
+        }
+        uint32_t s = 0;
+#pragma unroll
+        for (int u = 0; u < 16; u++) s += v[u];
         uint32_t x = s;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -115,14 +129,24 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ 
         }
         __syncthreads();
         uint32_t run = carry + (x - s) + (warp > 0 ? warp_sums[warp - 1] : 0u);
+        const uint32_t chunk_total = warp_sums[31];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            if (b0 + u < total) a[b0 + u] = run;
+        for (int u = 0; u < 16; u++) {
+            const uint32_t e = run;
             run += v[u];
+            v[u] = e;
         }
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = run;
-        __syncthreads();
+        if (full) {
+            uint4* p = reinterpret_cast<uint4*>(a + b0);
+#pragma unroll
+            for (int u = 0; u < 4; u++) p[u] = make_uint4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 16; u++)
+                if (b0 + u < total) a[b0 + u] = v[u];
+        }
+        carry += chunk_total;
+        __syncthreads();  // warp_sums is rewritten by the next chunk
     }
 }
 
