@@ -884,11 +884,37 @@ __device__ bool grid_reduce_scenes(double* acc, uint32_t ns, double* part, doubl
     }
     __syncthreads();
     if (last) {
+        // `per` threads share each of the m sums: thread g of a value adds
+        // blocks g, g + per, ... (eight loads in flight), and the value's
+        // first thread adds the per partial sums in order
+        __shared__ double red[PPE_THREADS];
         __threadfence();
-        for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) {
-            double v = 0.0;
-            for (uint32_t b = 0; b < gridDim.x; b++) v += __ldcg(part + (size_t)b * m + t);
-            result[t] = v;
+        const uint32_t per = blockDim.x >= m ? blockDim.x / m : 1u;
+        const uint32_t vals = blockDim.x / per;
+        const uint32_t G = gridDim.x;
+        for (uint32_t v0 = 0; v0 < m; v0 += vals) {
+            const uint32_t t = v0 + threadIdx.x / per, g = threadIdx.x % per;
+            double sum = 0.0;
+            if (threadIdx.x < vals * per && t < m) {
+                for (uint32_t b = g; b < G; b += 8 * per) {
+                    double v8[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const uint32_t bb = b + u * per;
+                        v8[u] = bb < G ? __ldcg(part + (size_t)bb * m + t) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) sum += v8[u];
+                }
+            }
+            red[threadIdx.x] = sum;
+            __syncthreads();
+            if (g == 0 && threadIdx.x < vals * per && t < m) {
+                double v = 0.0;
+                for (uint32_t k = 0; k < per; k++) v += red[threadIdx.x + k];
+                result[t] = v;
+            }
+            __syncthreads();
         }
         __threadfence();
         __syncthreads();
