@@ -252,7 +252,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dirs, accel, batch_counts = write_batch(tmpd, rank)
         n = int(sum(batch_counts))
         sim = capi.Simulation.batch(dirs, accel=accel, method=method, arith=arith, device=local_rank,
-                                    use_graph=1)
+                                    use_graph=1, precond=precond)
         nb2 = sum(sim.scene_info(s).nb2 for s in range(len(dirs)))
         nb1 = sum(sim.scene_info(s).nb1 for s in range(len(dirs)))
     else:
@@ -345,8 +345,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         scene_iters = None
     sim.close()
     compare = None
-    if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare and batch_counts is None:
-        compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)))
+    if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare:
+        if batch_counts is None:
+            compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)))
+        else:
+            compare = ppe_compare(dirs, arith, local_rank, args.warmup, max(3, min(args.steps, 5)), accel=accel)
 
     # max over ranks
     tot = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
@@ -410,16 +413,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     return line
 
 
-def ppe_compare(case_dir: str, arith: int, device: int, warm: int, steps: int):
+def ppe_compare(case_dir, arith: int, device: int, warm: int, steps: int, accel=None):
     """PPE solve milliseconds and PCG iterations per step (FP64 true residual
     to 1e-8) with diagonal scaling and with the trained learned factor, each
-    on a fresh copy of the scene after `warm` steps."""
+    on a fresh copy of the scene (or of the batch, when case_dir is a list of
+    scene directories: iterations are then the mean over scenes) after
+    `warm` steps."""
     from mps_solvers_b200 import capi, precond_weights
     out = {"tolerance": 1e-8, "steps": steps, "warmup": warm,
            "weights": os.path.relpath(precond_weights.PATH, ROOT)}
+    batch = isinstance(case_dir, (list, tuple))
     for name, pc in (("diagonal", capi.PRECOND_DIAGONAL), ("learned", capi.PRECOND_LEARNED)):
-        with capi.Simulation(case_dir, method=capi.METHOD_SEMI_IMPLICIT, arith=arith, device=device,
-                             precond=pc) as s:
+        if batch:
+            sim = capi.Simulation.batch(case_dir, accel=accel, method=capi.METHOD_SEMI_IMPLICIT, arith=arith,
+                                        device=device, precond=pc)
+        else:
+            sim = capi.Simulation(case_dir, method=capi.METHOD_SEMI_IMPLICIT, arith=arith, device=device,
+                                  precond=pc)
+        with sim as s:
             if pc == capi.PRECOND_LEARNED:
                 s.set_precond_params(precond_weights.load())
                 s.step(1)
@@ -428,7 +439,10 @@ def ppe_compare(case_dir: str, arith: int, device: int, warm: int, steps: int):
             iters, worst = 0, 0.0
             for _ in range(steps):
                 st = s.step(1)
-                iters += st.cg_iters
+                if batch:
+                    iters += float(np.mean([s.scene_info(k).cg_iters for k in range(len(case_dir))]))
+                else:
+                    iters += st.cg_iters
                 worst = max(worst, st.cg_relres)
             prof = s.profile(steps)
             out[name] = {"ppe_solve_ms": prof["ppe_solve"] / steps,

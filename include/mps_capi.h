@@ -293,7 +293,10 @@ mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t n, const mp
  * its own input.dat / GEO.dat, grid, constants, dt and time) as one particle
  * set: every stage is one launch over all scenes, and the semi-implicit PPE
  * of all scenes is one persistent launch in which each scene runs its own
- * PCG to options.cg_tol.  Each scene evolves as it would in its own handle.
+ * PCG to options.cg_tol (diagonally scaled, or with the learned factor when
+ * options.precond = MPS_PRECOND_LEARNED: mps_precond_set_params and
+ * mps_precond_tensor_cores take batch handles; training takes single scenes).
+ * Each scene evolves as it would in its own handle.
  * Particle ids of scene s are id_base(s) + its GEO.dat index;
  * mps_get_state(..., MPS_ORDER_BY_ID) returns all scenes in that order. */
 typedef struct mps_scene_spec {

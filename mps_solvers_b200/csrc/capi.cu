@@ -571,10 +571,6 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
             h->err = "every scene of a batch must have the same dimension";
             return MPS_ERR_INVALID;
         }
-    if (h->opt.precond == MPS_PRECOND_LEARNED) {
-        h->err = "the learned preconditioner is not available for batches";
-        return MPS_ERR_INVALID;
-    }
     h->prm = prms[0];
     h->nscenes = S;
     uint64_t np64 = 0;
@@ -803,6 +799,10 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
         if (e != MPS_OK) return (mps_status)e;
         e = ppe_setup_batch(h->ppe, ppe_scenes.data(), S, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
+        if (h->opt.precond == MPS_PRECOND_LEARNED) {
+            e = ppe_enable_learned(h->ppe, &h->err);
+            if (e != MPS_OK) return (mps_status)e;
+        }
     }
     Scalars sc;
     return read_status(h, &sc);
@@ -1227,10 +1227,12 @@ extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
 // ---------------------------------------------------------------- learned preconditioner
 extern "C" uint32_t mps_precond_num_params(void) { return (uint32_t)LP_NPARAM; }
 
-static mps_status need_semi(mps_handle* h) {
+// batch_ok: the call works on a batch handle (inference: parameters, the
+// tensor-core switch); training and snapshots take single scenes
+static mps_status need_semi(mps_handle* h, bool batch_ok = false) {
     if (!h) return MPS_ERR_INVALID;
-    if (h->nscenes) {
-        h->err = "the learned preconditioner is not available for batches";
+    if (h->nscenes && !batch_ok) {
+        h->err = "training the learned preconditioner takes single-scene handles";
         return MPS_ERR_INVALID;
     }
     if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) {
@@ -1241,7 +1243,7 @@ static mps_status need_semi(mps_handle* h) {
 }
 
 extern "C" mps_status mps_precond_get_params(mps_handle* h, float* w, uint32_t n) {
-    mps_status s = need_semi(h);
+    mps_status s = need_semi(h, true);
     if (s != MPS_OK) return s;
     if (!w || n != (uint32_t)LP_NPARAM) return MPS_ERR_INVALID;
     CK(cudaSetDevice(h->dev));
@@ -1255,7 +1257,7 @@ extern "C" mps_status mps_precond_get_params(mps_handle* h, float* w, uint32_t n
 }
 
 extern "C" mps_status mps_precond_set_params(mps_handle* h, const float* w, uint32_t n) {
-    mps_status s = need_semi(h);
+    mps_status s = need_semi(h, true);
     if (s != MPS_OK) return s;
     if (!w || n != (uint32_t)LP_NPARAM) return MPS_ERR_INVALID;
     CK(cudaSetDevice(h->dev));
@@ -1268,8 +1270,8 @@ extern "C" mps_status mps_precond_set_params(mps_handle* h, const float* w, uint
     return MPS_OK;
 }
 
-static mps_status need_snapshot(mps_handle* h) {
-    mps_status s = need_semi(h);
+static mps_status need_snapshot(mps_handle* h, bool batch_ok = false) {
+    mps_status s = need_semi(h, batch_ok);
     if (s != MPS_OK) return s;
     if (!h->ppe.lp.ready || !h->ppe.have_snapshot) {
         h->err = "no PPE system with the learned stencil yet: enable the learned preconditioner "
@@ -1335,7 +1337,7 @@ extern "C" mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint
 // largest entry, and use the tensor cores for inference from now on when
 // `enable` is set.
 extern "C" mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double* max_rel_diff) {
-    mps_status s = need_snapshot(h);
+    mps_status s = need_snapshot(h, true);
     if (s != MPS_OK) return s;
     CK(cudaSetDevice(h->dev));
     const LpSystem L = ppe_lp_system(h->ppe, stage_args(h));

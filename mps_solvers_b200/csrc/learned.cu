@@ -45,9 +45,18 @@ __device__ __forceinline__ float warp_sum(float v) {
 struct Feat {
     float f[LP_F];
 };
-__device__ __forceinline__ Feat edge_feat(const LpSystem& S, const float4& pi, float ni, uint32_t j) {
+// r0 and 1/n0 of row i's scene
+__device__ __forceinline__ float2 lp_consts(const LpSystem& S, uint32_t i) {
+    if (S.phys) {
+        const Phys& P = S.phys[__ldg(S.sid_of_id + __ldg(S.id + i))];
+        return make_float2(P.rzero, P.one_over_nzero);
+    }
+    return make_float2(S.P.rzero, S.P.one_over_nzero);
+}
+
+__device__ __forceinline__ Feat edge_feat(const LpSystem& S, const float4& pi, float ni, uint32_t j, float2 k) {
     const float4 pj = __ldg(S.pos + j);
-    const float inv = 1.f / S.P.rzero;
+    const float inv = 1.f / k.x;
     const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz);
     Feat e;
@@ -55,8 +64,8 @@ __device__ __forceinline__ Feat edge_feat(const LpSystem& S, const float4& pi, f
     e.f[1] = dy * inv;
     e.f[2] = dz * inv;
     e.f[3] = r * inv;
-    e.f[4] = r > 0.f ? (S.P.rzero / r - 1.f) : 0.f;
-    e.f[5] = ni * S.P.one_over_nzero;
+    e.f[4] = r > 0.f ? (k.x / r - 1.f) : 0.f;
+    e.f[5] = ni * k.y;
     e.f[6] = ptype(pj) == T_WALL ? 1.f : 0.f;
     return e;
 }
@@ -73,14 +82,22 @@ __global__ void __launch_bounds__(256) k_lp_stencil(LpSystem S, uint32_t* __rest
     if (k >= R) return;
     const uint32_t i = __ldg(S.rowlist + k);
     const float4 pi = __ldg(S.pos + i);
-    const float r02 = S.P.rzero * S.P.rzero;
+    Grid g = S.g;
+    const uint32_t* cs = S.cell_start;
+    uint32_t c = __ldg(S.cell + i);
+    if (S.grids) {  // the row's scene grid; cells are numbered from its base
+        g = S.grids[__ldg(S.sid_of_id + __ldg(S.id + i))];
+        cs = S.cell_start + g.base;
+        c -= g.base;
+    }
+    const float r0 = lp_consts(S, i).x;
+    const float r02 = r0 * r0;
     uint32_t cnt = 0, low = 0;
     uint32_t* out = scols + (size_t)i * LP_GW;
-    const uint32_t c = __ldg(S.cell + i);
-    const int rows = link_rows(S.g);
-    const CellNear nr = cell_near(S.g, c, pi.x, pi.y, pi.z, S.P.rzero);
+    const int rows = link_rows(g);
+    const CellNear nr = cell_near(g, c, pi.x, pi.y, pi.z, r0);
     for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(S.g, S.cell_start, c, row, nr);
+        const RowRange rg = link_row_near(g, cs, c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
             bool hit = false;
@@ -147,12 +164,13 @@ __global__ void __launch_bounds__(256) k_lp_edge_fwd(FwdArgs A) {
     }
     const float b0 = wbf(A.w, BB + lane), b1 = wbf(A.w, BB + lane + 32);
     const float4 pi = __ldg(S.pos + i);
+    const float2 kc = lp_consts(S, i);
     const float ni = __ldg(S.n + i);
     const uint32_t cnt = A.scnt[i];
     float acc0 = 0.f, acc1 = 0.f;
     for (uint32_t t = 0; t < cnt; t++) {
         const uint32_t j = A.scols[(size_t)i * LP_GW + t];
-        const Feat e = edge_feat(S, pi, ni, j);
+        const Feat e = edge_feat(S, pi, ni, j, kc);
         float s0 = b0, s1 = b1;
 #pragma unroll
         for (int f = 0; f < LP_F; f++) {
@@ -221,11 +239,12 @@ __global__ void __launch_bounds__(256) k_lp_readout_fwd(FwdArgs A) {
     const float ra1 = A.ra[(size_t)i * LP_H + lane + 32] + wbf(A.w, LP_BR + lane + 32);
     const float om0 = wbf(A.w, LP_OM + lane), om1 = wbf(A.w, LP_OM + lane + 32);
     const float4 pi = __ldg(S.pos + i);
+    const float2 kc = lp_consts(S, i);
     const float ni = __ldg(S.n + i);
     const uint32_t nl = A.nlow[i];
     for (uint32_t t = 0; t < nl; t++) {
         const uint32_t j = A.scols[(size_t)i * LP_GW + t];
-        const Feat e = edge_feat(S, pi, ni, j);
+        const Feat e = edge_feat(S, pi, ni, j, kc);
         float s0 = ra0 + A.rb[(size_t)j * LP_H + lane], s1 = ra1 + A.rb[(size_t)j * LP_H + lane + 32];
 #pragma unroll
         for (int f = 0; f < LP_F; f++) {
@@ -412,11 +431,12 @@ __global__ void __launch_bounds__(256) k_lp_readout_bwd_a(BwdArgs A) {
         const float ra1 = A.ra[(size_t)i * LP_H + lane + 32] + wbf(A.w, LP_BR + lane + 32);
         const float om0 = wbf(A.w, LP_OM + lane), om1 = wbf(A.w, LP_OM + lane + 32);
         const float4 pi = __ldg(S.pos + i);
+        const float2 kc = lp_consts(S, i);
         const float ni = __ldg(S.n + i);
         float dra0 = 0.f, dra1 = 0.f;
         for (uint32_t t = 0; t < A.nlow[i]; t++) {
             const uint32_t j = A.scols[(size_t)i * LP_GW + t];
-            const Feat e = edge_feat(S, pi, ni, j);
+            const Feat e = edge_feat(S, pi, ni, j, kc);
             float s0 = ra0 + A.rb[(size_t)j * LP_H + lane], s1 = ra1 + A.rb[(size_t)j * LP_H + lane + 32];
 #pragma unroll
             for (int f = 0; f < LP_F; f++) {
@@ -495,7 +515,8 @@ __global__ void __launch_bounds__(256) k_lp_readout_bwd_b(BwdArgs A) {
     for (uint32_t t = A.nlow[j]; t < cnt; t++) {
         const uint32_t i = A.scols[(size_t)j * LP_GW + t];
         const float4 pi = __ldg(S.pos + i);
-        const Feat e = edge_feat(S, pi, __ldg(S.n + i), j);
+        const float2 kc = lp_consts(S, i);
+        const Feat e = edge_feat(S, pi, __ldg(S.n + i), j, kc);
         float s0 = A.ra[(size_t)i * LP_H + lane] + br0 + rbj0;
         float s1 = A.ra[(size_t)i * LP_H + lane + 32] + br1 + rbj1;
 #pragma unroll
@@ -615,13 +636,14 @@ __global__ void __launch_bounds__(256) k_lp_edge_bwd_a(BwdArgs A) {
         }
         const float b0 = wbf(A.w, BB + lane), b1 = wbf(A.w, BB + lane + 32);
         const float4 pi = __ldg(S.pos + i);
+        const float2 kc = lp_consts(S, i);
         const float ni = __ldg(S.n + i);
         const uint32_t cnt = A.scnt[i];
         const float inv = cnt ? 1.f / (float)cnt : 0.f;
         const float da0 = A.da[(size_t)i * LP_H + lane] * inv, da1 = A.da[(size_t)i * LP_H + lane + 32] * inv;
         for (uint32_t t = 0; t < cnt; t++) {
             const uint32_t j = A.scols[(size_t)i * LP_GW + t];
-            const Feat e = edge_feat(S, pi, ni, j);
+            const Feat e = edge_feat(S, pi, ni, j, kc);
             float s0 = b0, s1 = b1;
 #pragma unroll
             for (int f = 0; f < LP_F; f++) {
@@ -680,7 +702,8 @@ __global__ void __launch_bounds__(256) k_lp_edge2_bwd_b(BwdArgs A, float* __rest
         const uint32_t ci = A.scnt[i];
         const float inv = ci ? 1.f / (float)ci : 0.f;
         const float4 pi = __ldg(S.pos + i);
-        const Feat e = edge_feat(S, pi, __ldg(S.n + i), j);
+        const float2 kc = lp_consts(S, i);
+        const Feat e = edge_feat(S, pi, __ldg(S.n + i), j, kc);
         float s0 = b0, s1 = b1;
 #pragma unroll
         for (int f = 0; f < LP_F; f++) {

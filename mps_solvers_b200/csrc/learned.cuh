@@ -124,6 +124,12 @@ struct LpSystem {            // the assembled PPE system the network works on
     Grid g;
     Phys P;
     const Scalars* sc;
+    // batch of scenes (null: one scene, g and P above): each row's scene
+    // from its particle id, and that scene's grid (with its first global
+    // cell) and constants
+    const uint32_t* sid_of_id = nullptr;
+    const Grid* grids = nullptr;
+    const Phys* phys = nullptr;
 };
 
 // neighbours within r0 of every non-Dirichlet row, and D^-1/2

@@ -840,6 +840,14 @@ struct BatchSolveArgs {
     int* iters;
     int* outers;
     double* relres;
+    // learned preconditioner: G' rows and columns (learned.cuh), y = G' r
+    const uint32_t* lo_off;
+    const uint32_t* lo_cols;
+    const float* lo_vals;
+    const uint32_t* up_off;
+    const uint32_t* up_cols;
+    const float* up_vals;
+    float* y;
     uint32_t ns;
     double tol;
     double eta_min;
@@ -952,9 +960,13 @@ __device__ __forceinline__ float batch_weight(const float4* __restrict__ pos, fl
     return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
 }
 
-template <bool EX, bool SW>
+// PREC 0: diagonal scaling; PREC 1: the learned factor, M^-1 = G'^T G'
+// (G' = G D^-1/2; neighbours of a row are rows of its own scene, so y = G'r
+// and z = G'^T y run over all rows of the scenes still iterating at once).
+template <bool EX, bool SW, int PREC>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs S) {
     __shared__ double acc[3 * PPE_MAX_SCENES];
+    __shared__ double rrn[PREC == 1 ? PPE_MAX_SCENES : 1];
     __shared__ double rz[PPE_MAX_SCENES], stop[PPE_MAX_SCENES], alpha[PPE_MAX_SCENES], rel[PPE_MAX_SCENES];
     __shared__ float beta[PPE_MAX_SCENES];
     __shared__ int its[PPE_MAX_SCENES], outs[PPE_MAX_SCENES];
@@ -1013,7 +1025,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const double bi = S.b64[ii];
                 const double ri = bi - (S.diag64[ii] * S.x64[ii] + sum);
                 const float rf = (float)ri;
-                const float zf = rf * S.inv_diag[ii];
+                const float zf = PREC == 0 ? rf * S.inv_diag[ii] : 0.f;
                 S.r[ii] = rf;
                 zc[ii] = make_float2(zf, 0.f);
                 v[0] = ri * ri;
@@ -1043,6 +1055,39 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             }
         }
         __syncthreads();
+        if (PREC == 1) {
+            // z = G'^T G' r on the rows of the scenes still open; r.z per scene
+            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += stride) {
+                if (done[__ldg(S.row_scene + kk)]) continue;
+                const uint32_t i = __ldg(rowlist + kk);
+                const float* r = S.r;
+                S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r](uint32_t j) { return r[j]; });
+            }
+            for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[t] = 0.0;
+            if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;  // barrier: y complete
+            for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[t] = 0.0;
+            __syncthreads();
+            for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
+                const uint32_t kk = k0 + lane;
+                const bool has = kk < R;
+                const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
+                const bool contrib = has && !done[s];
+                double v[1] = {0.0};
+                if (contrib) {
+                    const uint32_t i = __ldg(rowlist + kk);
+                    const float* y = S.y;
+                    const float zi =
+                        lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                    zc[i].x = zi;
+                    v[0] = (double)S.r[i] * (double)zi;
+                }
+                scene_add<1>(acc, ns, s, contrib, v);
+            }
+            if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+            for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x)
+                if (active[s]) rz[s] = acc[s];
+            __syncthreads();
+        }
         if (threadIdx.x == 0) {
             int c = 0;
             for (uint32_t s = 0; s < ns; s++) c += done[s] ? 0 : 1;
@@ -1101,28 +1146,83 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
             __syncthreads();
             for (uint32_t t = threadIdx.x; t < 2 * ns; t += blockDim.x) acc[t] = 0.0;
             __syncthreads();
-            // ---- x64 += alpha p, r -= alpha q, z = D^-1 r; r.z and r.r per scene
-            for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
-                const uint32_t kk = k0 + lane;
-                const bool has = kk < R;
-                const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
-                const bool contrib = has && active[s];
-                double v[2] = {0.0, 0.0};
-                if (contrib) {
-                    const uint32_t i = __ldg(rowlist + kk);
-                    const double al = alpha[s];
-                    const float pn = zn[i].y;
-                    S.x64[i] += al * (double)pn;
-                    const float ri = fmaf(-(float)al, S.q[i], S.r[i]);
-                    const float zi = ri * S.inv_diag[i];
-                    S.r[i] = ri;
-                    zn[i] = make_float2(zi, pn);
-                    v[0] = (double)ri * (double)zi;
-                    v[1] = (double)ri * (double)ri;
+            // ---- x64 += alpha p, r -= alpha q, z = M^-1 r; r.z and r.r per scene
+            if (PREC == 0) {
+                for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
+                    const uint32_t kk = k0 + lane;
+                    const bool has = kk < R;
+                    const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
+                    const bool contrib = has && active[s];
+                    double v[2] = {0.0, 0.0};
+                    if (contrib) {
+                        const uint32_t i = __ldg(rowlist + kk);
+                        const double al = alpha[s];
+                        const float pn = zn[i].y;
+                        S.x64[i] += al * (double)pn;
+                        const float ri = fmaf(-(float)al, S.q[i], S.r[i]);
+                        const float zi = ri * S.inv_diag[i];
+                        S.r[i] = ri;
+                        zn[i] = make_float2(zi, pn);
+                        v[0] = (double)ri * (double)zi;
+                        v[1] = (double)ri * (double)ri;
+                    }
+                    scene_add<2>(acc, ns, s, contrib, v);
                 }
-                scene_add<2>(acc, ns, s, contrib, v);
+                if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+            } else {
+                // pass A: x64 += alpha p; y = G' r_new with each neighbour's
+                // r_new = r - alpha q formed on the fly (same scene, same
+                // alpha); r_new . r_new per scene
+                for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
+                    const uint32_t kk = k0 + lane;
+                    const bool has = kk < R;
+                    const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
+                    const bool contrib = has && active[s];
+                    double v[1] = {0.0};
+                    if (contrib) {
+                        const uint32_t i = __ldg(rowlist + kk);
+                        const double al = alpha[s];
+                        const float af = (float)al;
+                        S.x64[i] += al * (double)zn[i].y;
+                        const float ri = fmaf(-af, S.q[i], S.r[i]);
+                        const float* r = S.r;
+                        const float* q = S.q;
+                        S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk,
+                                               [r, q, af](uint32_t j) { return fmaf(-af, q[j], r[j]); });
+                        v[0] = (double)ri * (double)ri;
+                    }
+                    scene_add<1>(acc, ns, s, contrib, v);
+                }
+                if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+                for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) {
+                    rrn[t] = acc[t];
+                    acc[t] = 0.0;
+                }
+                __syncthreads();
+                // pass B: r = r_new in place (no neighbour reads r now),
+                // z = G'^T y; r.z per scene
+                for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
+                    const uint32_t kk = k0 + lane;
+                    const bool has = kk < R;
+                    const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
+                    const bool contrib = has && active[s];
+                    double v[1] = {0.0};
+                    if (contrib) {
+                        const uint32_t i = __ldg(rowlist + kk);
+                        const float ri = fmaf(-(float)alpha[s], S.q[i], S.r[i]);
+                        S.r[i] = ri;
+                        const float* y = S.y;
+                        const float zi =
+                            lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                        zn[i] = make_float2(zi, zn[i].y);
+                        v[0] = (double)ri * (double)zi;
+                    }
+                    scene_add<1>(acc, ns, s, contrib, v);
+                }
+                if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+                for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[ns + t] = rrn[t];
+                __syncthreads();
             }
-            if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
             for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
                 if (!active[s]) continue;
                 beta[s] = (float)(acc[s] / rz[s]);
@@ -1404,8 +1504,10 @@ static std::vector<const void*> solve_kernels() {
             (const void*)k_ppe_solve<true, 1, true>,    (const void*)k_ppe_solve<false, 1, true>,
             (const void*)k_ppe_solve<true, 0, false>,   (const void*)k_ppe_solve<false, 0, false>,
             (const void*)k_ppe_solve<true, 1, false>,   (const void*)k_ppe_solve<false, 1, false>,
-            (const void*)k_ppe_solve_batch<true, true>, (const void*)k_ppe_solve_batch<false, true>,
-            (const void*)k_ppe_solve_batch<true, false>, (const void*)k_ppe_solve_batch<false, false>,
+            (const void*)k_ppe_solve_batch<true, true, 0>, (const void*)k_ppe_solve_batch<false, true, 0>,
+            (const void*)k_ppe_solve_batch<true, false, 0>, (const void*)k_ppe_solve_batch<false, false, 0>,
+            (const void*)k_ppe_solve_batch<true, true, 1>, (const void*)k_ppe_solve_batch<false, true, 1>,
+            (const void*)k_ppe_solve_batch<true, false, 1>, (const void*)k_ppe_solve_batch<false, false, 1>,
             (const void*)k_ppe_solve_pipe<true, true>,  (const void*)k_ppe_solve_pipe<false, true>,
             (const void*)k_ppe_solve_pipe<true, false>, (const void*)k_ppe_solve_pipe<false, false>};
 }
@@ -1581,6 +1683,11 @@ LpSystem ppe_lp_system(const PpeWork& w, const StageArgs& a) {
     L.g = a.g;
     L.P = a.P;
     L.sc = a.sc;
+    if (a.batch.n) {
+        L.sid_of_id = a.batch.sid_of_id;
+        L.grids = a.batch.grid;
+        L.phys = a.batch.phys;
+    }
     return L;
 }
 
@@ -1663,12 +1770,26 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.max_outer = S.max_outer;
         B.eta_min = S.eta_min;
         B.keep = S.keep;
+        B.lo_off = w.lp.lo_off;
+        B.lo_cols = w.lp.lo_cols;
+        B.lo_vals = w.lp.lo_vals;
+        B.up_off = w.lp.up_off;
+        B.up_cols = w.lp.up_cols;
+        B.up_vals = w.lp.up_vals;
+        B.y = w.y;
         void* bargs[] = {&B};
-        const void* bfn = w.stored_weights
-                              ? (a.exact ? (const void*)k_ppe_solve_batch<true, true>
-                                         : (const void*)k_ppe_solve_batch<false, true>)
-                              : (a.exact ? (const void*)k_ppe_solve_batch<true, false>
-                                         : (const void*)k_ppe_solve_batch<false, false>);
+        const bool blearned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+        const void* bfn;
+        if (blearned)
+            bfn = w.stored_weights ? (a.exact ? (const void*)k_ppe_solve_batch<true, true, 1>
+                                              : (const void*)k_ppe_solve_batch<false, true, 1>)
+                                   : (a.exact ? (const void*)k_ppe_solve_batch<true, false, 1>
+                                              : (const void*)k_ppe_solve_batch<false, false, 1>);
+        else
+            bfn = w.stored_weights ? (a.exact ? (const void*)k_ppe_solve_batch<true, true, 0>
+                                              : (const void*)k_ppe_solve_batch<false, true, 0>)
+                                   : (a.exact ? (const void*)k_ppe_solve_batch<true, false, 0>
+                                              : (const void*)k_ppe_solve_batch<false, false, 0>);
         w.launch_err = launch_cooperative(bfn, w.blocks, w.threads, bargs, st);
         if (!w.write_pressure) return 1;
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
