@@ -375,6 +375,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         alg_bytes = STAGE_BYTES[dom] * n
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     traffic = _traffic_from_profiles("pressure" if dom == "ppe_solve" else dom, args.workload)
+    # FP32 pipe (the secondary roofline of the stencil stages): pair
+    # evaluations of the fixed model, |{j: r_ij < re}| x FLOP per pair (PND 10
+    # over all particles at r0; viscosity 16 at rlap, collision 20 and
+    # gradient 18 at r0 over the fluid; the CG product 12 at rlap per fluid
+    # row and iteration), over the whole step's device time
+    nf = int(n - nb2 - nb1)
+    flops = n * 32 * 10 + nf * (250 * 16 + 32 * 20 + 32 * 18)
+    if method == capi.METHOD_SEMI_IMPLICIT:
+        flops += (ppe_work / 60.0) * 250 * 12 * nf / n if n else 0.0
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * 1965e6 / 1e12
+    fp32_ach = flops / (ms / args.steps / 1e3) / 1e12
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -393,6 +405,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "ms_per_launch": dom_ms,
                      "note": "stencil kernels scan the 27 reference cells and are issue/latency "
                              "bound; see profiles/ for the measured bound"},
+        "roofline_fp32": {"bound": "fp32", "achieved": fp32_ach, "peak": fp32_peak,
+                          "peak_kind": f"nominal ({sms} SMs x 128 FP32 lanes x 2 x 1965 MHz)",
+                          "unit": "TFLOP/s", "frac": fp32_ach / fp32_peak, "flops_per_step": flops,
+                          "note": "pair-evaluation model over the whole step; the stages scan ~5-50x "
+                                  "more candidates than they keep"},
+        "value_fluid_only": value * nf / n if n else None,
         "stage_ms_per_step": {k: v / prof_steps for k, v in prof.items()},
         "e2e": {"value": e2e_v, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
