@@ -200,6 +200,18 @@ def _cpu_model():
     return "unknown"
 
 
+def max_over_ranks(values, world: int, device="cpu"):
+    """Element-wise maximum of `values` over all ranks (every rank gets it):
+    the slowest replica's timings.  The process group is NCCL on the GPU box
+    and gloo in the CPU tests."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return None
@@ -351,12 +363,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         else:
             compare = ppe_compare(dirs, arith, local_rank, args.warmup, max(3, min(args.steps, 5)), accel=accel)
 
-    # max over ranks
-    tot = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    ms, e2e_s = float(tot[0]), float(tot[1])
+    ms, e2e_s = max_over_ranks([ms, e2e_s], world, dev)
     if rank != 0:
         return None
 
