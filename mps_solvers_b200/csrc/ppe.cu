@@ -183,10 +183,13 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rlap, thr = P.rlap_thr;
     const double bthr = beta * n0;
+    // n_j < bthr (double) exactly when n_j < bthr_f, the least float >= bthr
+    float bthr_f = (float)bthr;
+    if ((double)bthr_f < bthr) bthr_f = nextafterf(bthr_f, INFINITY);
     uint32_t* cols = A.cols + (size_t)i * PPE_W;
     float* wrow = A.wrm + (size_t)i * PPE_W;
     uint32_t count = 0;
-    double diag = 0.0;
+    float diag_lane = 0.f;  // this lane's few nonzero weights, then a FP64 warp sum
     const int rows = link_rows(L.g);
     const uint32_t lt = (1u << lane) - 1u;
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
@@ -203,11 +206,11 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
                     const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
                     if (rr < thr) {
                         w = weight_rr<EX>(re, rr);
-                        if (w > 0.f) app = !((double)__ldg(nn + j) < bthr);
+                        if (w > 0.f) app = !(__ldg(nn + j) < bthr_f);
                     }
                 }
             }
-            diag += (double)w;
+            diag_lane += w;
             const uint32_t m = __ballot_sync(0xffffffffu, app);
             if (app) {
                 const uint32_t k = count + __popc(m & lt);
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
             count += __popc(m);
         }
     }
-    diag = warp_sum_d(diag);
+    const double diag = warp_sum_d((double)diag_lane);
     if (lane == 0) {
         if (count > PPE_W) {
             atomicOr(&a.sc->err, ERR_CAPACITY);  // more than PPE_W neighbours
