@@ -81,6 +81,10 @@ struct mps_handle {
     uint32_t* motion_of = nullptr;   // per GEO.dat id
     float4* motion_x0 = nullptr;     // per GEO.dat id
     uint32_t* motion_count = nullptr;
+    // the device scalars as the last read_status saw them; valid until work
+    // that may change the particle count is enqueued (steps, rebuilds)
+    bool sc_valid = false;
+    Scalars sc_host{};
 };
 
 static void drop_graphs(mps_handle* h);
@@ -170,6 +174,7 @@ static void mark(mps_handle* h, int tag) {
 // The reference's divideCell: keys (after the pending update), stable sort,
 // cell table, gather into the other buffer set.
 static void rebuild(mps_handle* h, int apply) {
+    h->sc_valid = false;
     cudaStream_t st = h->stream;
     State& src = h->S[h->cur];
     State& dst = h->S[h->cur ^ 1];
@@ -191,6 +196,7 @@ static void rebuild(mps_handle* h, int apply) {
 //  explicit: MPS_GPU_EXPL::step (MPS_CAL_expl_v1.0/MPS_GPU_EXPL.cpp:277-339)
 //  semi:     MPS_CPU_EXPL::step (MPS_CAL_v4.0/MPS_CPU_EXPL.cpp:79-135)
 static void enqueue_step(mps_handle* h) {
+    h->sc_valid = false;
     cudaStream_t st = h->stream;
     const uint32_t cap = h->cap;
     h->launches = 0;
@@ -246,6 +252,8 @@ static mps_status read_status(mps_handle* h, Scalars* out) {
     Scalars s;
     CK(cudaMemcpyAsync(&s, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->sc_host = s;
+    h->sc_valid = true;
     if (out) *out = s;
     if (s.err & ERR_NAN) { h->err = "NaN in particle state"; return MPS_ERR_NAN; }
     if (s.err & ERR_DT_TOO_SMALL) { h->err = "dt below dt_min"; return MPS_ERR_DT_TOO_SMALL; }
@@ -1014,6 +1022,7 @@ static void drop_graphs(mps_handle* h) {
 }
 
 static mps_status step_async(mps_handle* h, int nsteps) {
+    h->sc_valid = false;
     CK(cudaSetDevice(h->dev));
     for (int k = 0; k < nsteps; k++) {
         if (h->opt.use_graph && !h->graph_off) {
@@ -1113,7 +1122,15 @@ extern "C" mps_status mps_phase(mps_handle* h, int phase) {
 }
 
 // ---------------------------------------------------------------- getters
-static mps_status counts(mps_handle* h, Scalars* s) { return read_status(h, s) == MPS_ERR_CUDA ? MPS_ERR_CUDA : MPS_OK; }
+// particle counts: those of the last status read while no step or rebuild
+// has been enqueued since (saves a device round trip per state transfer)
+static mps_status counts(mps_handle* h, Scalars* s) {
+    if (h->sc_valid) {
+        *s = h->sc_host;
+        return MPS_OK;
+    }
+    return read_status(h, s) == MPS_ERR_CUDA ? MPS_ERR_CUDA : MPS_OK;
+}
 
 extern "C" mps_status mps_get_counts(mps_handle* h, uint32_t* np, uint32_t* nb2, uint32_t* nb1, uint32_t* nexcl) {
     if (!h) return MPS_ERR_INVALID;
