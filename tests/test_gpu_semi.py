@@ -136,3 +136,18 @@ def test_pipelined_pcg_matches_fp64_oracle(capi, oracle_mod, tmp_path):
             assert st.cg_relres <= 1e-8 and st.cg_iters > 0
         ex, eu, ep = compare(s.state(), orc.state())
     assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
+
+
+def test_l2_residency_hints_change_no_result(capi, tmp_path):
+    """The stencil's L2 policy (evict_last head, evict_first tail, or plain
+    loads) only moves data between cache and DRAM: states agree bit for bit."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    out = []
+    for keep in (0, -1, 1):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, ppe_l2_keep_mb=keep) as s:
+            assert s.step(6).cg_relres <= 1e-8
+            out.append(s.state())
+    for o in out[1:]:
+        for f in ("pos", "vel", "press", "n"):
+            assert np.array_equal(out[0][f], o[f]), f
