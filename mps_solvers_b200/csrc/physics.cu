@@ -311,6 +311,102 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     a.tmp[i] = t;
 }
 
+// The unordered (fast) Laplacian for two fluid particles per warp: the
+// warp walks the union of both particles' culled linked cells once and
+// tests every candidate against both, so loads, index arithmetic and loop
+// control are shared.  Used when the two list entries sit in the same cell
+// (the common case: the fluid list is in sorted order within each warp of
+// the gather); otherwise each particle walks its own cells.
+template <bool BT>
+__global__ void __launch_bounds__(256) k_visc_w2(StageArgs a, const uint32_t* __restrict__ list,
+                                                 const uint32_t* __restrict__ list_n) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nl = *list_n;
+    if (2 * w >= nl) return;
+    const uint32_t i1 = list[2 * w];
+    const bool two = 2 * w + 1 < nl;
+    const uint32_t i2 = two ? list[2 * w + 1] : i1;
+    const float4* __restrict__ pos = a.cur.pos;
+    const float4* __restrict__ vel = a.cur.vel;
+    const float4 p1 = pos[i1], p2 = pos[i2];
+    const float4 u1 = vel[i1], u2 = vel[i2];
+    const Local L1 = local_of<BT>(a, i1);
+    const Local L2 = local_of<BT>(a, i2);
+    const Phys P = phys_of<BT>(a, L1.s);
+    const float re = P.rlap, thr = P.rlap_thr;
+    const bool shared = two && L1.c == L2.c && L1.s == L2.s;
+    float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2x = 0.f, a2y = 0.f, a2z = 0.f;
+    const int rows = link_rows(L1.g);
+    const CellNear n1 = cell_near(L1.g, L1.c, p1.x, p1.y, p1.z, re);
+    const CellNear n2 = cell_near(L2.g, L2.c, p2.x, p2.y, p2.z, re);
+    auto pair = [&](const float4& pi, const float4& ui, uint32_t i, uint32_t j, const float4& pj, const float4& uj,
+                    float& ax, float& ay, float& az) {
+        const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        const float rr = dx * dx + dy * dy + dz * dz;
+        if (j != i && rr < thr) {
+            const float wgt = weight_rr<false>(re, rr);
+            ax += wgt * (uj.x - ui.x);
+            ay += wgt * (uj.y - ui.y);
+            az += wgt * (uj.z - ui.z);
+        }
+    };
+    if (shared) {
+        for (int row = 0; row < rows; row++) {
+            const RowRange r1 = link_row_near(L1.g, L1.cs, L1.c, row, n1);
+            const RowRange r2 = link_row_near(L1.g, L1.cs, L1.c, row, n2);
+            const uint32_t lo = r1.hi > r1.lo ? (r2.hi > r2.lo ? min(r1.lo, r2.lo) : r1.lo) : r2.lo;
+            const uint32_t hi = r1.hi > r1.lo ? (r2.hi > r2.lo ? max(r1.hi, r2.hi) : r1.hi) : r2.hi;
+            for (uint32_t base = lo; base < hi; base += 32) {
+                const uint32_t j = base + lane;
+                if (j < hi) {
+                    const float4 pj = __ldg(pos + j), uj = __ldg(vel + j);
+                    pair(p1, u1, i1, j, pj, uj, a1x, a1y, a1z);
+                    pair(p2, u2, i2, j, pj, uj, a2x, a2y, a2z);
+                }
+            }
+        }
+    } else {
+        for (int k = 0; k < (two ? 2 : 1); k++) {
+            const Local& L = k ? L2 : L1;
+            const CellNear& nr = k ? n2 : n1;
+            const float4 pi = k ? p2 : p1, ui = k ? u2 : u1;
+            const uint32_t i = k ? i2 : i1;
+            float &ax = k ? a2x : a1x, &ay = k ? a2y : a1y, &az = k ? a2z : a1z;
+            for (int row = 0; row < rows; row++) {
+                const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
+                for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
+                    const uint32_t j = base + lane;
+                    if (j < rg.hi) pair(pi, ui, i, j, __ldg(pos + j), __ldg(vel + j), ax, ay, az);
+                }
+            }
+        }
+    }
+    a1x = warp_tree_add(a1x); a1y = warp_tree_add(a1y); a1z = warp_tree_add(a1z);
+    a2x = warp_tree_add(a2x); a2y = warp_tree_add(a2y); a2z = warp_tree_add(a2z);
+    if (lane > 1 || (lane == 1 && !two)) return;
+    const uint32_t i = lane ? i2 : i1;
+    const float4 ui = lane ? u2 : u1;
+    const Local& L = lane ? L2 : L1;
+    const Phys Pi = phys_of<BT>(a, L.s);
+    const float ax = lane ? a2x : a1x, ay = lane ? a2y : a1y, az = lane ? a2z : a1z;
+    const float dt = dt_of<BT>(a, L.s);
+    float gx, gy, gz;
+    if (BT) {
+        const float4 ge = a.batch.g_eff[L.s];
+        gx = ge.x; gy = ge.y; gz = ge.z;
+    } else {
+        gx = a.sc->g_eff[0]; gy = a.sc->g_eff[1]; gz = a.sc->g_eff[2];
+    }
+    const float lx = Pi.c_lap * ax, ly = Pi.c_lap * ay, lz = Pi.c_lap * az;
+    float4 t;
+    t.x = ui.x + dt * (Pi.niu * lx + gx);
+    t.y = ui.y + dt * (Pi.niu * ly + gy);
+    t.z = ui.z + dt * (Pi.niu * lz + gz);
+    t.w = 0.f;
+    a.tmp[i] = t;
+}
+
 template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t* __restrict__ list,
                                                      const uint32_t* __restrict__ list_n) {
@@ -497,14 +593,17 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
 //   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
 void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
+    const uint32_t nb2 = blocks_for((a.cap_fluid + 1) / 2 * 32u, (uint32_t)a.threads);  // two particles a warp
     const bool ord = a.exact && !a.semi;
     if (a.batch.n) {
         if (a.exact && ord) k_visc_w<true, true, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
         else if (a.exact) k_visc_w<true, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.list_fluid) k_visc_w2<true><<<nb2, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
         else k_visc_w<false, false, true><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
     } else {
         if (a.exact && ord) k_visc_w<true, true, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
         else if (a.exact) k_visc_w<true, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
+        else if (a.list_fluid) k_visc_w2<false><<<nb2, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
         else k_visc_w<false, false, false><<<nb, a.threads, 0, st>>>(a, a.list_fluid, a.n_fluid);
     }
 }

@@ -151,3 +151,20 @@ def test_l2_residency_hints_change_no_result(capi, tmp_path):
     for o in out[1:]:
         for f in ("pos", "vel", "press", "n"):
             assert np.array_equal(out[0][f], o[f]), f
+
+
+def test_semi_fast_arith_vs_fp64_oracle(capi, oracle_mod, tmp_path):
+    """The fast arithmetic the benchmark runs (FMA contraction, two fluid
+    particles per warp in the viscosity stage) within the same tolerances of
+    the FP64 oracle as the exact kernels."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    orc = oracle_mod.Oracle(d, oracle_mod.SEMI_JACOBI, 64)
+    orc.set_cg(True, 1e-12, 100000)
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, arith=capi.ARITH_FAST) as s:
+        for k in range(8):
+            st = s.step(1)
+            orc.step(1)
+            assert st.cg_relres <= 1e-8 and st.cg_iters > 0
+        ex, eu, ep = compare(s.state(), orc.state())
+    assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
