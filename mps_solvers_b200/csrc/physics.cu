@@ -503,6 +503,8 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     }
 }
 
+constexpr uint32_t DASH_SLOTS = 64;  // neighbours within r0 kept per particle (~32 on the lattice)
+
 template <bool EX, bool ORD, bool BT>
 __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __restrict__ list,
                                                 const uint32_t* __restrict__ list_n) {
@@ -518,37 +520,56 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const int rows = link_rows(L.g);
     const float r02 = P.rzero2;
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, P.rzero);
-    // p_hat: a minimum, independent of order
+    // p_hat: a minimum, independent of order.  The same walk keeps every
+    // candidate within r0 (any type, ascending index) in this warp's slots,
+    // so the gradient below visits only those instead of walking the cells
+    // again; more than DASH_SLOTS of them and it walks the cells again.
+    __shared__ uint32_t slots[8][DASH_SLOTS];
+    uint32_t* my = slots[(threadIdx.x >> 5) & 7u];
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t nhit = 0;
     float hat = press[i];
     for (int row = 0; row < rows; row++) {
         const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
             const uint32_t j = base + lane;
+            bool near = false;
             if (j < rg.hi) {
                 const float4 pj = __ldg(pos + j);
-                if (ptype(pj) != T_DUMMY) {
-                    const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
-                    const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
-                    if (rr <= r02) {
-                        const float pjv = __ldg(press + j);
-                        if (pjv < hat) hat = pjv;
-                    }
+                const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
+                const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
+                near = rr <= r02 || rr < P.rzero_thr;  // both passes' candidates
+                if (rr <= r02 && ptype(pj) != T_DUMMY) {
+                    const float pjv = __ldg(press + j);
+                    if (pjv < hat) hat = pjv;
                 }
             }
+            const uint32_t m = __ballot_sync(0xffffffffu, near);
+            if (near) {
+                const uint32_t k = nhit + __popc(m & lt);
+                if (k < DASH_SLOTS) my[k] = j;
+            }
+            nhit += __popc(m);
         }
     }
+    __syncwarp();
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, o));
     const float re = P.rzero, thr = P.rzero_thr;
     const bool skip_dummy = a.semi != 0;
     float gx = 0.f, gy = 0.f, gz = 0.f;
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
+    // the gradient's terms: candidates of the kept slots, in the same
+    // ascending order as the cell walk, or the cell walk itself
+    const bool slotted = nhit <= DASH_SLOTS;
+    for (int row = 0; row < (slotted ? 1 : rows); row++) {
+        RowRange rg;
+        if (slotted) rg = RowRange{0u, nhit};
+        else rg = link_row_near(L.g, L.cs, L.c, row, nr);
         for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+            const uint32_t j = slotted ? (base + lane < rg.hi ? my[base + lane] : 0xFFFFFFFFu) : base + lane;
             float tx = 0.f, ty = 0.f, tz = 0.f;
             bool hit = false;
-            if (j < rg.hi && j != i) {
+            if (base + lane < rg.hi && j != i) {
                 const float4 pj = __ldg(pos + j);
                 if (!(skip_dummy && ptype(pj) == T_DUMMY)) {
                     const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
