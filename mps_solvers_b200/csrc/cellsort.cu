@@ -159,16 +159,44 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ 
 __global__ void __launch_bounds__(SORT_THREADS) k_radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ n_dev, int shift,
-    uint32_t tiles) {
+    uint32_t tiles, int scanned) {
     constexpr int WARPS = SORT_THREADS / 32;
+    static_assert(SORT_THREADS == SORT_RADIX, "one digit per thread");
     __shared__ uint32_t warp_hist[WARPS][SORT_RADIX];
     __shared__ uint32_t tile_off[SORT_RADIX];
+    __shared__ uint32_t dsum[WARPS];
     const uint32_t n = *n_dev;
     const uint32_t base = blockIdx.x * SORT_TILE;
     if (base >= n) return;  // the whole block exits together
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = threadIdx.x; k < WARPS * SORT_RADIX; k += SORT_THREADS) (&warp_hist[0][0])[k] = 0;
-    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) tile_off[d] = hist[d * tiles + blockIdx.x];
+    if (scanned) {
+        for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) tile_off[d] = hist[d * tiles + blockIdx.x];
+    } else {
+        // the scan done here from the raw tile histograms (few tiles): the
+        // output offset of (digit d, this tile) is the count of all smaller
+        // digits plus the count of digit d in the earlier tiles
+        const int d = threadIdx.x;
+        const uint32_t* hd = hist + (size_t)d * tiles;
+        uint32_t tot = 0, pre = 0;
+#pragma unroll 8
+        for (uint32_t t = 0; t < tiles; t++) {
+            const uint32_t v = hd[t];
+            tot += v;
+            pre += t < blockIdx.x ? v : 0u;
+        }
+        uint32_t x = tot;  // inclusive scan of the digit totals: warps, then warp sums
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) dsum[warp] = x;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; w++) before += dsum[w];
+        tile_off[d] = before + x - tot + pre;
+    }
     __syncthreads();
 
     uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
@@ -274,9 +302,12 @@ int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
         k_radix_upsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], n_dev, shift, s.hist, s.tiles);
-        k_scan_exclusive<<<1, 1024, 0, st>>>(s.hist, SORT_RADIX * s.tiles);
+        // few tiles: each downsweep block scans the histograms itself (one
+        // launch less per pass); many: one scan kernel
+        const int scanned = s.tiles > SORT_FUSED_SCAN_TILES;
+        if (scanned) k_scan_exclusive<<<1, 1024, 0, st>>>(s.hist, SORT_RADIX * s.tiles);
         k_radix_downsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], s.vals[cur], s.keys[cur ^ 1],
-                                                             s.vals[cur ^ 1], s.hist, n_dev, shift, s.tiles);
+                                                             s.vals[cur ^ 1], s.hist, n_dev, shift, s.tiles, scanned);
         cur ^= 1;
     }
     return cur;
