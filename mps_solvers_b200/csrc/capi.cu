@@ -183,12 +183,10 @@ static void rebuild(mps_handle* h, int apply) {
                      src.id, h->batch);
     mark(h, ST_SORT);
     const int r = launch_radix_sort(h->sort, &h->sc->np, h->passes, h->cap, st);
-    mark(h, ST_CELLS);
-    launch_cell_start(h->sort.keys[r], h->g, h->sc, h->cell_start, h->cap, st);
-    mark(h, ST_GATHER);
+    mark(h, ST_GATHER);  // the gather also fills the cell table
     launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
-                  h->list_fluid, h->list_solid, h->batch);
-    h->launches += 3 + 3 * h->passes;
+                  h->list_fluid, h->list_solid, h->batch, h->cell_start, h->g.ncells);
+    h->launches += 2 + 3 * h->passes;
     h->cur ^= 1;
 }
 

@@ -244,30 +244,8 @@ __global__ void __launch_bounds__(SORT_THREADS) k_radix_downsweep(
 }
 
 // ---------------------------------------------------------------- cell tables
-// cell_start[c] = first sorted position whose key is >= c, for c in
-// [0, ncells]; equal to the reference's serial prefix sum of per-cell counts
-// (MPS_CAL_expl_v1.0/MPS_GPU.cpp:293-297), with cell_end[c] = cell_start[c+1]
-// and cell_start[ncells] = number of particles inside the grid.
-__device__ __forceinline__ void cell_start_fill(const uint32_t* keys, uint32_t n, uint32_t ncells, uint32_t p,
-                                                uint32_t* cell_start) {
-    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
-    long long cur = p < n ? (long long)keys[p] : (long long)ncells;
-    if (cur > (long long)ncells) cur = ncells;
-    for (long long c = prev + 1; c <= cur; c++) cell_start[c] = p;
-}
-
-__global__ void __launch_bounds__(256) k_cell_start(const uint32_t* __restrict__ keys, Grid g,
-                                                    Scalars* __restrict__ sc, uint32_t* __restrict__ cell_start) {
-    const uint32_t n = sc->np;
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > n) return;
-    cell_start_fill(keys, n, g.ncells, p, cell_start);
-    // the thread whose range reaches c = ncells knows the in-grid count
-    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
-    long long cur = p < n ? (long long)keys[p] : (long long)g.ncells;
-    if (prev < (long long)g.ncells && cur >= (long long)g.ncells) sc->np_new = p;
-}
-
+// (cell_start_fill is in cellsort.cuh; the particle steps' rebuild fills the
+// table in its gather kernel)
 __global__ void __launch_bounds__(256) k_cell_start_plain(const uint32_t* __restrict__ keys, uint32_t n, Grid g,
                                                           uint32_t* __restrict__ cell_start,
                                                           uint32_t* __restrict__ n_in_grid) {
@@ -317,10 +295,6 @@ void launch_scan_exclusive(uint32_t* a, uint32_t total, cudaStream_t st) {
     k_scan_exclusive<<<1, 1024, 0, st>>>(a, total);
 }
 
-void launch_cell_start(const uint32_t* keys_sorted, const Grid& g, Scalars* sc, uint32_t* cell_start, uint32_t cap,
-                       cudaStream_t st) {
-    k_cell_start<<<blocks_for(cap + 1, 256), 256, 0, st>>>(keys_sorted, g, sc, cell_start);
-}
 
 void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32_t* keys, uint32_t* vals,
                             cudaStream_t st) {

@@ -50,8 +50,7 @@ void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, i
 // returns the buffer index (0/1) that holds the result.
 int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st);
 // Stage 3: cell_start[0..ncells] from the sorted keys; writes sc->np_new.
-void launch_cell_start(const uint32_t* keys_sorted, const Grid& g, Scalars* sc, uint32_t* cell_start,
-                       uint32_t cap, cudaStream_t st);
+
 
 // Same pieces with n given on the host (for the device-pointer primitive).
 void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32_t* keys, uint32_t* vals,
@@ -62,5 +61,18 @@ void launch_cell_start_plain(const uint32_t* keys_sorted, uint32_t n, const Grid
 void launch_scan_exclusive(uint32_t* a, uint32_t total, cudaStream_t st);
 void launch_cell_end_from_start(const uint32_t* cell_start, uint32_t ncells, uint32_t* start_out,
                                 uint32_t* end_out, cudaStream_t st);
+
+// cell_start[c] = first sorted position whose key is >= c, for c in
+// [0, ncells]; equal to the reference's serial prefix sum of per-cell counts
+// (MPS_CAL_expl_v1.0/MPS_GPU.cpp:293-297), with cell_end[c] = cell_start[c+1]
+// and cell_start[ncells] = number of particles inside the grid.
+__device__ __forceinline__ void cell_start_fill(const uint32_t* keys, uint32_t n, uint32_t ncells, uint32_t p,
+                                                uint32_t* cell_start) {
+    long long prev = p > 0 ? (long long)keys[p - 1] : -1ll;
+    long long cur = p < n ? (long long)keys[p] : (long long)ncells;
+    if (cur > (long long)ncells) cur = ncells;
+    for (long long c = prev + 1; c <= cur; c++) cell_start[c] = p;
+}
+
 
 }  // namespace mpsb

@@ -8,6 +8,7 @@
 // gather.  With EX = true each float operation is rounded once, in the
 // reference's order, so the results equal the reference's CPU results.
 #include "physics.cuh"
+#include "cellsort.cuh"
 
 namespace mpsb {
 
@@ -23,9 +24,17 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
                                                 const float4* __restrict__ tmp, int apply,
                                                 uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc,
                                                 uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid,
-                                                BatchDev batch) {
-    const uint32_t n = sc->np, nn = sc->np_new;
+                                                BatchDev batch, uint32_t* __restrict__ cell_start, uint32_t ncells) {
+    const uint32_t n = sc->np;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    // the cell table (one thread per sorted position and one past the end)
+    // and the count of particles inside the grid, whose keys sort first
+    if (p <= n) {
+        cell_start_fill(keys_sorted, n, ncells, p, cell_start);
+        const long long prev = p > 0 ? (long long)keys_sorted[p - 1] : -1ll;
+        const long long cur = p < n ? (long long)keys_sorted[p] : (long long)ncells;
+        if (prev < (long long)ncells && cur >= (long long)ncells) sc->np_new = p;
+    }
     uint32_t ty = T_EXCL;
     if (p < n) {
         const uint32_t old = perm[p];
@@ -42,7 +51,7 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
             x.y = __fadd_rn(x.y, __fmul_rn(dt, d.y));
             x.z = __fadd_rn(x.z, __fmul_rn(dt, d.z));
         }
-        if (p >= nn) {
+        if (keys_sorted[p] >= ncells) {  // left the grid
             x.w = __uint_as_float(T_EXCL);
             u = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -78,6 +87,8 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
         __threadfence();
         const uint32_t done = atomicAdd(&sc->done_blocks, 1u);
         if (done == gridDim.x - 1) {
+            __threadfence();
+            const uint32_t nn = *(volatile uint32_t*)&sc->np_new;
             sc->nexcl += n - nn;
             sc->np = nn;
             sc->done_blocks = 0;
@@ -88,9 +99,10 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
 
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
                    const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
-                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch) {
-    k_gather<<<blocks_for(cap, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc,
-                                                    list_fluid, list_solid, batch);
+                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch, uint32_t* cell_start,
+                   uint32_t ncells) {
+    k_gather<<<blocks_for(cap + 1, 256), 256, 0, st>>>(src, dst, perm, keys_sorted, tmp, apply, index_of_id, sc,
+                                                        list_fluid, list_solid, batch, cell_start, ncells);
 }
 
 // ---------------------------------------------------------------- update_dt

@@ -87,7 +87,8 @@ __device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) {
 // reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
                    const float4* tmp, int apply, uint32_t* index_of_id, Scalars* sc, uint32_t cap, cudaStream_t st,
-                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch);
+                   uint32_t* list_fluid, uint32_t* list_solid, const BatchDev& batch, uint32_t* cell_start,
+                   uint32_t ncells);
 
 // update_dt: max |u|^2, then dt on the device
 void launch_update_dt(const StageArgs& a, uint32_t cap, cudaStream_t st);
