@@ -178,15 +178,12 @@ static void rebuild(mps_handle* h, int apply) {
     cudaStream_t st = h->stream;
     State& src = h->S[h->cur];
     State& dst = h->S[h->cur ^ 1];
-    mark(h, ST_KEYS);
-    launch_cell_keys(src.pos, src.vel, h->tmp, apply, h->g, h->sc, h->sort.keys[0], h->sort.vals[0], h->cap, st,
-                     src.id, h->batch);
-    mark(h, ST_SORT);
-    const int r = launch_radix_sort(h->sort, &h->sc->np, h->passes, h->cap, st);
+    mark(h, ST_SORT);  // the keys are computed by the first pass's upsweep
+    const int r = launch_keys_and_sort(src.pos, h->tmp, apply, h->g, h->sc, src.id, h->batch, h->sort, h->passes, st);
     mark(h, ST_GATHER);  // the gather also fills the cell table
     launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
                   h->list_fluid, h->list_solid, h->batch, h->cell_start, h->g.ncells);
-    h->launches += 2 + 3 * h->passes;
+    h->launches += 1 + h->passes * (h->sort.tiles > SORT_FUSED_SCAN_TILES ? 3 : 2);
     h->cur ^= 1;
 }
 

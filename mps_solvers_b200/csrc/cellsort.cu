@@ -13,19 +13,10 @@ namespace mpsb {
 // In a batch each particle is binned in its own scene's grid and keyed by
 // that grid's first global cell plus its cell there; outside its grid it
 // takes the sentinel of all scenes' cells.
-__global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vel,
-                                                   const float4* __restrict__ tmp, int apply, Grid g,
-                                                   Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
-                                                   uint32_t* __restrict__ vals, const uint32_t* __restrict__ id,
-                                                   BatchDev batch) {
-    const uint32_t n = sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        // the gather of this rebuild refills the particle lists
-        sc->n_fluid = 0;
-        sc->n_solid = 0;
-    }
-    if (i >= n) return;
+// key of particle i after the pending update
+__device__ __forceinline__ uint32_t cell_key(const float4* __restrict__ pos, const float4* __restrict__ tmp, int apply,
+                                             Grid g, Scalars* __restrict__ sc, const uint32_t* __restrict__ id,
+                                             const BatchDev& batch, uint32_t i) {
     float4 p = pos[i];
     uint32_t s = 0;
     if (batch.n) {
@@ -44,8 +35,58 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ po
     uint32_t k = cell_of_pos(g, p.x, p.y, p.z, &nan_flag);
     if (nan_flag) atomicOr(&sc->err, ERR_NAN);
     if (batch.n) k = k == g.ncells ? batch.ncells : g.base + k;
-    keys[i] = k;
+    return k;
+}
+
+__global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                   const float4* __restrict__ tmp, int apply, Grid g,
+                                                   Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
+                                                   uint32_t* __restrict__ vals, const uint32_t* __restrict__ id,
+                                                   BatchDev batch) {
+    const uint32_t n = sc->np;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        // the gather of this rebuild refills the particle lists
+        sc->n_fluid = 0;
+        sc->n_solid = 0;
+    }
+    if (i >= n) return;
+    keys[i] = cell_key(pos, tmp, apply, g, sc, id, batch, i);
     vals[i] = i;
+}
+
+// The keys fused with the first radix pass's upsweep: each block keys its
+// tile of 2048 particles and counts their low digits (one launch less per
+// rebuild).
+__global__ void __launch_bounds__(SORT_THREADS) k_keys_upsweep(const float4* __restrict__ pos,
+                                                               const float4* __restrict__ tmp, int apply, Grid g,
+                                                               Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
+                                                               uint32_t* __restrict__ vals,
+                                                               const uint32_t* __restrict__ id, BatchDev batch,
+                                                               uint32_t* __restrict__ hist, uint32_t tiles) {
+    __shared__ uint32_t h[SORT_RADIX];
+    const uint32_t n = sc->np;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->n_fluid = 0;  // the gather of this rebuild refills the particle lists
+        sc->n_solid = 0;
+    }
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) h[d] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * SORT_TILE;
+    if (base < n) {
+#pragma unroll
+        for (int k = 0; k < SORT_ITEMS; k++) {
+            const uint32_t idx = base + k * SORT_THREADS + threadIdx.x;
+            if (idx < n) {
+                const uint32_t key = cell_key(pos, tmp, apply, g, sc, id, batch, idx);
+                keys[idx] = key;
+                vals[idx] = idx;
+                atomicAdd(&h[key & 0xffu], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < SORT_RADIX; d += SORT_THREADS) hist[d * tiles + blockIdx.x] = h[d];
 }
 
 __global__ void __launch_bounds__(256) k_cell_keys_plain(const float4* __restrict__ pos, uint32_t n, Grid g,
@@ -274,12 +315,12 @@ void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, i
     k_cell_keys<<<blocks_for(cap, 256), 256, 0, st>>>(pos, vel, tmp, apply, g, sc, keys, vals, id, batch);
 }
 
-int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st) {
-    (void)cap;
+static int radix_passes(SortScratch& s, const uint32_t* n_dev, int passes, cudaStream_t st, bool first_counted) {
     int cur = 0;
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
-        k_radix_upsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], n_dev, shift, s.hist, s.tiles);
+        if (!(p == 0 && first_counted))
+            k_radix_upsweep<<<s.tiles, SORT_THREADS, 0, st>>>(s.keys[cur], n_dev, shift, s.hist, s.tiles);
         // few tiles: each downsweep block scans the histograms itself (one
         // launch less per pass); many: one scan kernel
         const int scanned = s.tiles > SORT_FUSED_SCAN_TILES;
@@ -289,6 +330,18 @@ int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_
         cur ^= 1;
     }
     return cur;
+}
+
+int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st) {
+    (void)cap;
+    return radix_passes(s, n_dev, passes, st, false);
+}
+
+int launch_keys_and_sort(const float4* pos, const float4* tmp, int apply, const Grid& g, Scalars* sc,
+                         const uint32_t* id, const BatchDev& batch, SortScratch& s, int passes, cudaStream_t st) {
+    k_keys_upsweep<<<s.tiles, SORT_THREADS, 0, st>>>(pos, tmp, apply, g, sc, s.keys[0], s.vals[0], id, batch, s.hist,
+                                                     s.tiles);
+    return radix_passes(s, &sc->np, passes, st, true);
 }
 
 void launch_scan_exclusive(uint32_t* a, uint32_t total, cudaStream_t st) {

@@ -49,6 +49,10 @@ void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, i
 // Stage 2: stable LSD radix sort of (keys[0], vals[0]) over sc->np keys;
 // returns the buffer index (0/1) that holds the result.
 int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st);
+// the keys of launch_cell_keys fused with the first pass of the sort; returns
+// the buffer index of the sorted keys and values, as launch_radix_sort
+int launch_keys_and_sort(const float4* pos, const float4* tmp, int apply, const Grid& g, Scalars* sc,
+                         const uint32_t* id, const BatchDev& batch, SortScratch& s, int passes, cudaStream_t st);
 // Stage 3: cell_start[0..ncells] from the sorted keys; writes sc->np_new.
 
 
