@@ -38,23 +38,6 @@ __device__ __forceinline__ uint32_t cell_key(const float4* __restrict__ pos, con
     return k;
 }
 
-__global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vel,
-                                                   const float4* __restrict__ tmp, int apply, Grid g,
-                                                   Scalars* __restrict__ sc, uint32_t* __restrict__ keys,
-                                                   uint32_t* __restrict__ vals, const uint32_t* __restrict__ id,
-                                                   BatchDev batch) {
-    const uint32_t n = sc->np;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        // the gather of this rebuild refills the particle lists
-        sc->n_fluid = 0;
-        sc->n_solid = 0;
-    }
-    if (i >= n) return;
-    keys[i] = cell_key(pos, tmp, apply, g, sc, id, batch, i);
-    vals[i] = i;
-}
-
 // The keys fused with the first radix pass's upsweep: each block keys its
 // tile of 2048 particles and counts their low digits (one launch less per
 // rebuild).
@@ -309,11 +292,6 @@ __global__ void k_start_end(const uint32_t* __restrict__ cs, uint32_t ncells, ui
 // ---------------------------------------------------------------- launchers
 static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 
-void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
-                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st, const uint32_t* id,
-                      const BatchDev& batch) {
-    k_cell_keys<<<blocks_for(cap, 256), 256, 0, st>>>(pos, vel, tmp, apply, g, sc, keys, vals, id, batch);
-}
 
 static int radix_passes(SortScratch& s, const uint32_t* n_dev, int passes, cudaStream_t st, bool first_counted) {
     int cur = 0;

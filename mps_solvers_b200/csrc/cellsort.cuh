@@ -40,20 +40,16 @@ enum ApplyMode : int {
 };
 
 // Launchers (all asynchronous on `st`).
-// Stage 1: cell key of every active particle (after the pending update);
-// with batch.n > 0 g is the whole cell space and each particle (by id) uses
-// its scene's grid.
-void launch_cell_keys(const float4* pos, const float4* vel, const float4* tmp, int apply, const Grid& g,
-                      Scalars* sc, uint32_t* keys, uint32_t* vals, uint32_t cap, cudaStream_t st, const uint32_t* id,
-                      const BatchDev& batch);
-// Stage 2: stable LSD radix sort of (keys[0], vals[0]) over sc->np keys;
-// returns the buffer index (0/1) that holds the result.
+// Stable LSD radix sort of (keys[0], vals[0]) over *n_dev keys; returns the
+// buffer index (0/1) that holds the result.
 int launch_radix_sort(SortScratch& s, const uint32_t* n_dev, int passes, uint32_t cap, cudaStream_t st);
-// the keys of launch_cell_keys fused with the first pass of the sort; returns
-// the buffer index of the sorted keys and values, as launch_radix_sort
+// The rebuild's keys and sort: the cell key of every active particle (after
+// the pending update; with batch.n > 0 g is the whole cell space and each
+// particle, by id, uses its scene's grid) computed by the first pass's
+// upsweep, then the sort over sc->np keys.  Returns the buffer index as
+// launch_radix_sort.  The cell table is filled by the gather that follows.
 int launch_keys_and_sort(const float4* pos, const float4* tmp, int apply, const Grid& g, Scalars* sc,
                          const uint32_t* id, const BatchDev& batch, SortScratch& s, int passes, cudaStream_t st);
-// Stage 3: cell_start[0..ncells] from the sorted keys; writes sc->np_new.
 
 
 // Same pieces with n given on the host (for the device-pointer primitive).
