@@ -236,14 +236,50 @@ __device__ __forceinline__ WarpTask warp_task(const StageArgs& a, const uint32_t
     return t;
 }
 
+// Ordered sums of one batch's terms (the reference adds a particle's
+// neighbour terms one after another in candidate order).  The lanes with a
+// term write it to the warp's shared buffer at its rank among them, and lane
+// 0 adds the buffer in that order, one rounding per addition: the same
+// additions as a loop over the hits, without a shuffle chain every lane runs.
+// Only lane 0's sums are the result.  buf holds 32 entries per warp.
 template <bool EX>
-__device__ __forceinline__ float warp_ordered_add(float acc, float term, uint32_t m) {
-    while (m) {
-        const int b = __ffs(m) - 1;
-        m &= m - 1u;
-        acc = fadd<EX>(acc, __shfl_sync(0xffffffffu, term, b));
+__device__ __forceinline__ void ordered_add1(float* buf, uint32_t lane, bool hit, float t, float& acc) {
+    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (m == 0u) return;
+    if (hit) buf[__popc(m & ((1u << lane) - 1u))] = t;
+    __syncwarp();
+    if (lane == 0) {
+        const int nh = __popc(m);
+#pragma unroll 4
+        for (int k = 0; k < nh; k++) acc = fadd<EX>(acc, buf[k]);
     }
-    return acc;
+    __syncwarp();
+}
+
+template <bool EX>
+__device__ __forceinline__ void ordered_add3(float4* buf, uint32_t lane, bool hit, float tx, float ty, float tz,
+                                             float& ax, float& ay, float& az) {
+    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (m == 0u) return;
+    if (hit) buf[__popc(m & ((1u << lane) - 1u))] = make_float4(tx, ty, tz, 0.f);
+    __syncwarp();
+    if (lane == 0) {
+        const int nh = __popc(m);
+#pragma unroll 4
+        for (int k = 0; k < nh; k++) {
+            const float4 t = buf[k];
+            ax = fadd<EX>(ax, t.x);
+            ay = fadd<EX>(ay, t.y);
+            az = fadd<EX>(az, t.z);
+        }
+    }
+    __syncwarp();
+}
+
+// the warp's 32-entry buffer for ordered sums (blocks of up to 256 threads)
+__device__ __forceinline__ float4* ordered_buf() {
+    __shared__ float4 ord_buf[8][32];
+    return ord_buf[(threadIdx.x >> 5) & 7u];
 }
 
 __device__ __forceinline__ float warp_tree_add(float v) {
@@ -267,6 +303,7 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rlap, thr = P.rlap_thr;
     float ax = 0.f, ay = 0.f, az = 0.f;
+    float4* obuf = ordered_buf();
     const int rows = link_rows(L.g);
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
     for (int row = 0; row < rows; row++) {
@@ -290,18 +327,8 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
                     }
                 }
             }
-            if (ORD) {
-                uint32_t m = __ballot_sync(0xffffffffu, hit);
-                while (m) {
-                    const int b = __ffs(m) - 1;
-                    m &= m - 1u;
-                    ax = __fadd_rn(ax, __shfl_sync(0xffffffffu, tx, b));
-                    ay = __fadd_rn(ay, __shfl_sync(0xffffffffu, ty, b));
-                    az = __fadd_rn(az, __shfl_sync(0xffffffffu, tz, b));
-                }
-            } else {
-                ax += tx; ay += ty; az += tz;
-            }
+            if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, ax, ay, az);
+            else { ax += tx; ay += ty; az += tz; }
         }
     }
     if (!ORD) { ax = warp_tree_add(ax); ay = warp_tree_add(ay); az = warp_tree_add(az); }
@@ -431,6 +458,7 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     if (ptype(pi) != T_FLUID) return;
     const float4 ui = vel[i];
     float cx = 0.f, cy = 0.f, cz = 0.f;
+    float4* obuf = ordered_buf();
     const Local L = local_of<BT>(a, i);
     const Phys P = phys_of<BT>(a, L.s);
     const int rows = link_rows(L.g);
@@ -463,16 +491,11 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
                     }
                 }
             }
-            uint32_t m = __ballot_sync(0xffffffffu, hit);
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1u;
-                cx = fadd<EX>(cx, __shfl_sync(0xffffffffu, tx, b));
-                cy = fadd<EX>(cy, __shfl_sync(0xffffffffu, ty, b));
-                cz = fadd<EX>(cz, __shfl_sync(0xffffffffu, tz, b));
-            }
+            if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, cx, cy, cz);
+            else { cx += tx; cy += ty; cz += tz; }
         }
     }
+    if (!ORD) { cx = warp_tree_add(cx); cy = warp_tree_add(cy); cz = warp_tree_add(cz); }
     if (lane == 0) a.tmp[i] = make_float4(cx, cy, cz, 0.f);
 }
 
@@ -489,6 +512,7 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     const Phys P = phys_of<BT>(a, L.s);
     const float re = P.rzero, thr = P.rzero_thr;
     float acc = 0.f;
+    float4* obuf = ordered_buf();
     const int rows = link_rows(L.g);
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
     for (int row = 0; row < rows; row++) {
@@ -502,7 +526,7 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
                 if (rr < thr) w = weight_rr<EX>(re, rr);
             }
-            if (ORD) acc = warp_ordered_add<true>(acc, w, __ballot_sync(0xffffffffu, w != 0.f));
+            if (ORD) ordered_add1<true>(reinterpret_cast<float*>(obuf), lane, w != 0.f, w, acc);
             else acc += w;
         }
     }
@@ -570,6 +594,7 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const float re = P.rzero, thr = P.rzero_thr;
     const bool skip_dummy = a.semi != 0;
     float gx = 0.f, gy = 0.f, gz = 0.f;
+    float4* obuf = ordered_buf();
     // the gradient's terms: candidates of the kept slots, in the same
     // ascending order as the cell walk, or the cell walk itself
     const bool slotted = nhit <= DASH_SLOTS;
@@ -598,18 +623,8 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
                     }
                 }
             }
-            if (ORD) {
-                uint32_t m = __ballot_sync(0xffffffffu, hit);
-                while (m) {
-                    const int b = __ffs(m) - 1;
-                    m &= m - 1u;
-                    gx = __fadd_rn(gx, __shfl_sync(0xffffffffu, tx, b));
-                    gy = __fadd_rn(gy, __shfl_sync(0xffffffffu, ty, b));
-                    gz = __fadd_rn(gz, __shfl_sync(0xffffffffu, tz, b));
-                }
-            } else {
-                gx += tx; gy += ty; gz += tz;
-            }
+            if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, gx, gy, gz);
+            else { gx += tx; gy += ty; gz += tz; }
         }
     }
     if (!ORD) { gx = warp_tree_add(gx); gy = warp_tree_add(gy); gz = warp_tree_add(gz); }
