@@ -101,7 +101,12 @@ typedef struct {
                             Crank-Nicolson, three PCG solves a step (the
                             reference's MPS_CPU_IMPL / MPS_GPU_IMPL step,
                             MPS_CAL_v4.0/MPS_CPU_IMPL.cpp:79-338); 0 = explicit */
-    uint32_t reserved[4];
+    int rebuild_merge;   /* cell rebuilds: 0 = merge the particles that changed
+                            cell into the sorted order when at most 8192
+                            particles can move (fluid and moving walls), else
+                            a full radix sort; -1 = always the full sort.  Both
+                            give the same stable order.                       */
+    uint32_t reserved[3];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

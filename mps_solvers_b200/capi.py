@@ -51,7 +51,7 @@ class mps_options(C.Structure):
                 ("use_graph", C.c_int), ("cg_tol", C.c_double), ("cg_max_iter", C.c_int),
                 ("cg_check_every", C.c_int), ("precond", C.c_int), ("capacity", C.c_uint32),
                 ("cg_inner_digits", C.c_int), ("ppe_pipelined", C.c_int), ("ppe_l2_keep_mb", C.c_int),
-                ("visc_implicit", C.c_int), ("reserved", C.c_uint32 * 4)]
+                ("visc_implicit", C.c_int), ("rebuild_merge", C.c_int), ("reserved", C.c_uint32 * 3)]
 
 
 class mps_params(C.Structure):

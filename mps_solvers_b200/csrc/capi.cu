@@ -39,7 +39,11 @@ struct mps_handle {
     float4* tmp = nullptr;
     uint32_t* index_of_id = nullptr;
     uint32_t* normal_id_of = nullptr;
-    uint32_t* cell_start = nullptr;
+    uint32_t* cell_tab[2] = {nullptr, nullptr};  // cell table of each state buffer's order
+    MergeScratch merge{};   // the merge rebuild's scratch (options.rebuild_merge)
+    bool merge_ready = false;
+    bool sorted = false;    // the current state buffer is sorted and its cell table valid
+    uint32_t moving = 0;    // wall and dummy particles with a motion
     uint32_t* list_fluid = nullptr;
     uint32_t* list_solid = nullptr;
     uint32_t cap_fluid = 0, cap_solid = 0;
@@ -132,7 +136,7 @@ static cudaError_t dalloc(mps_handle* h, T** p, size_t count) {
 static StageArgs stage_args(mps_handle* h) {
     StageArgs a;
     a.cur = h->S[h->cur];
-    a.cell_start = h->cell_start;
+    a.cell_start = h->cell_tab[h->cur];
     a.tmp = h->tmp;
     a.sc = h->sc;
     a.g = h->g;
@@ -173,18 +177,37 @@ static void mark(mps_handle* h, int tag) {
 
 // The reference's divideCell: keys (after the pending update), stable sort,
 // cell table, gather into the other buffer set.
+// The merge rebuild (cellsort.cuh) when at most MERGE_SMEM_CAP particles can
+// change cell between two rebuilds (fluid and moving walls) and the current
+// order is a sorted one; else the full radix sort.  Both give the same order.
+static bool use_merge(const mps_handle* h) {
+    return h->merge_ready && h->sorted && (uint64_t)h->cap_fluid + h->moving <= MERGE_SMEM_CAP;
+}
+
 static void rebuild(mps_handle* h, int apply) {
     h->sc_valid = false;
     cudaStream_t st = h->stream;
     State& src = h->S[h->cur];
     State& dst = h->S[h->cur ^ 1];
-    mark(h, ST_SORT);  // the keys are computed by the first pass's upsweep
-    const int r = launch_keys_and_sort(src.pos, h->tmp, apply, h->g, h->sc, src.id, h->batch, h->sort, h->passes, st);
-    mark(h, ST_GATHER);  // the gather also fills the cell table
-    launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
-                  h->list_fluid, h->list_solid, h->batch, h->cell_start, h->g.ncells);
-    h->launches += 1 + h->passes * (h->sort.tiles > SORT_FUSED_SCAN_TILES ? 3 : 2);
+    uint32_t* cs_new = h->cell_tab[h->cur ^ 1];
+    if (use_merge(h)) {
+        mark(h, ST_SORT);
+        launch_merge_keys_sort(src.pos, h->tmp, apply, h->g, h->sc, src.id, h->batch, src.cell, h->merge, h->cap, st);
+        mark(h, ST_GATHER);  // the merge gather also derives the cell table
+        launch_merge_gather(src, dst, h->merge, h->cell_tab[h->cur], cs_new, h->g.ncells, h->tmp, apply,
+                            h->index_of_id, h->sc, h->cap, st, h->list_fluid, h->list_solid, h->batch);
+        h->launches += 3;
+    } else {
+        mark(h, ST_SORT);  // the keys are computed by the first pass's upsweep
+        const int r =
+            launch_keys_and_sort(src.pos, h->tmp, apply, h->g, h->sc, src.id, h->batch, h->sort, h->passes, st);
+        mark(h, ST_GATHER);  // the gather also fills the cell table
+        launch_gather(src, dst, h->sort.vals[r], h->sort.keys[r], h->tmp, apply, h->index_of_id, h->sc, h->cap, st,
+                      h->list_fluid, h->list_solid, h->batch, cs_new, h->g.ncells);
+        h->launches += 1 + h->passes * (h->sort.tiles > SORT_FUSED_SCAN_TILES ? 3 : 2);
+    }
     h->cur ^= 1;
+    h->sorted = true;
 }
 
 // One step in the reference's order.
@@ -326,6 +349,23 @@ static void apply_constants(Phys& P, const HostConst& c) {
     P.one_over_dt_fixed = c.one_over_dt;
 }
 
+// The merge rebuild's scratch, unless the options turn it off or more
+// particles can move than its one-block sort takes (use_merge).
+static cudaError_t merge_setup(mps_handle* h) {
+    if (h->opt.rebuild_merge != 0 || (uint64_t)h->cap_fluid > MERGE_SMEM_CAP) return cudaSuccess;
+    size_t p2 = 1;  // the sort's global-memory case pads to a power of two
+    while (p2 < h->cap) p2 <<= 1;
+    cudaError_t e;
+    if ((e = dalloc(h, &h->merge.newkey, h->cap)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->merge.changed, h->cap)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->merge.a, p2)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->merge.b, p2)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->merge.count, 2)) != cudaSuccess) return e;
+    if ((e = merge_sort_setup()) != cudaSuccess) return e;
+    h->merge_ready = true;
+    return cudaSuccess;
+}
+
 static Grid device_grid(const HostGrid& hg, uint32_t base) {
     Grid g;
     g.left = hg.left;
@@ -395,7 +435,8 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     h->cap_solid = np - nb2;
     CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
     CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
-    CK(dalloc(h, &h->cell_start, (size_t)g.ncells + 1));
+    for (int b = 0; b < 2; b++) CK(dalloc(h, &h->cell_tab[b], (size_t)g.ncells + 1));
+    CK(merge_setup(h));
     h->sort.tiles = sort_tiles(cap);
     for (int b = 0; b < 2; b++) {
         CK(dalloc(h, &h->sort.keys[b], cap));
@@ -490,6 +531,10 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     }
     apply_constants(P, h->hc);
 
+    if (h->opt.rebuild_merge != 0 && h->opt.rebuild_merge != -1) {
+        h->err = "rebuild_merge is 0 (merge when few particles can move) or -1 (always sort)";
+        return MPS_ERR_INVALID;
+    }
     if (h->opt.visc_implicit && h->opt.method != MPS_METHOD_SEMI_IMPLICIT) {
         h->err = "Crank-Nicolson viscosity needs the semi-implicit method";
         return MPS_ERR_INVALID;
@@ -646,7 +691,8 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
     h->cap_solid = np - h->nb2;
     CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
     CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
-    CK(dalloc(h, &h->cell_start, (size_t)h->g.ncells + 1));
+    for (int b = 0; b < 2; b++) CK(dalloc(h, &h->cell_tab[b], (size_t)h->g.ncells + 1));
+    CK(merge_setup(h));
     h->sort.tiles = sort_tiles(cap);
     for (int b = 0; b < 2; b++) {
         CK(dalloc(h, &h->sort.keys[b], cap));
@@ -730,8 +776,8 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
     std::vector<uint32_t> lo(S), hi(S);
     for (uint32_t s = 0; s < S; s++) {
         const Grid& g = h->scene_grid[s];
-        CK(cudaMemcpyAsync(&lo[s], h->cell_start + g.base, 4, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(&hi[s], h->cell_start + g.base + g.ncells, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&lo[s], h->cell_tab[h->cur] + g.base, 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&hi[s], h->cell_tab[h->cur] + g.base + g.ncells, 4, cudaMemcpyDeviceToHost, h->stream));
     }
     CK(cudaStreamSynchronize(h->stream));
     std::vector<PpeScene> ppe_scenes(S);
@@ -942,6 +988,7 @@ extern "C" mps_status mps_add_wall_motion(mps_handle* h, const float lo[3], cons
     h->mot.omega[m] = 2.0 * M_PI * (double)freq;
     h->mot.phase[m] = (double)phase;
     h->mot.n = m + 1;
+    h->moving += count;
     if (selected) *selected = count;
     drop_graphs(h);  // the captured steps hold the old motion set
     return MPS_OK;
@@ -957,6 +1004,7 @@ extern "C" mps_status mps_clear_wall_motion(mps_handle* h) {
     }
     CK(cudaStreamSynchronize(h->stream));
     h->mot.n = 0;
+    h->moving = 0;
     drop_graphs(h);
     return MPS_OK;
 }
@@ -1187,7 +1235,8 @@ extern "C" mps_status mps_get_cell_tables(mps_handle* h, uint32_t* cell_of, uint
     if (counts(h, &s) != MPS_OK) return MPS_ERR_CUDA;
     const uint32_t nc = h->g.ncells;
     std::vector<uint32_t> cs(nc + 1);
-    CK(cudaMemcpyAsync(cs.data(), h->cell_start, (nc + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(cs.data(), h->cell_tab[h->cur], (nc + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       h->stream));
     if (cell_of && s.np)
         CK(cudaMemcpyAsync(cell_of, h->S[h->cur].cell, s.np * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));

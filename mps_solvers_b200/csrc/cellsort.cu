@@ -267,6 +267,104 @@ __global__ void __launch_bounds__(SORT_THREADS) k_radix_downsweep(
     }
 }
 
+// ---------------------------------------------------------------- merge rebuild
+// keys after the pending update; the changed particles (key != the cell they
+// were sorted into) appended to m.changed through one atomic per warp
+__global__ void __launch_bounds__(256) k_merge_keys(const float4* __restrict__ pos, const float4* __restrict__ tmp,
+                                                    int apply, Grid g, Scalars* __restrict__ sc,
+                                                    const uint32_t* __restrict__ id, BatchDev batch,
+                                                    const uint32_t* __restrict__ cell_old, MergeScratch m) {
+    const uint32_t n = sc->np;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->n_fluid = 0;  // the merge gather refills the particle lists
+        sc->n_solid = 0;
+    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    bool ch = false;
+    if (i < n) {
+        const uint32_t k = cell_key(pos, tmp, apply, g, sc, id, batch, i);
+        m.newkey[i] = k;
+        ch = k != cell_old[i];
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, ch);
+    uint32_t base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&m.count[0], __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (ch) m.changed[base + __popc(bal & ((1u << lane) - 1u))] = i;
+}
+
+// ascending bitonic sort of P (a power of two) entries of x in the block's
+// memory (shared or global), all threads of the block taking part
+template <class T>
+__device__ __forceinline__ void block_bitonic(T* x, uint32_t P) {
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) {
+                const uint32_t l = t ^ j;
+                if (l > t) {
+                    const T u = x[t], v = x[l];
+                    if (((t & k) == 0) == (u > v)) {
+                        x[t] = v;
+                        x[l] = u;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One block: the changed list in its two orders, padded to a power of two
+// with entries greater than any real one.  Up to MERGE_SMEM_CAP entries in
+// shared memory; more (a state set from the host that moved many particles
+// across cells) in the scratch arrays themselves, sized for every particle.
+__global__ void __launch_bounds__(MERGE_SORT_THREADS) k_merge_sort(MergeScratch m) {
+    extern __shared__ uint64_t msh[];
+    const uint32_t cnt = *(volatile uint32_t*)&m.count[0];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        m.count[1] = cnt;
+        m.count[0] = 0;  // empty for the next rebuild's keys kernel
+    }
+    if (cnt == 0) return;
+    uint32_t P = 1;
+    while (P < cnt) P <<= 1;
+    const bool in_smem = P <= MERGE_SMEM_CAP;  // else m.a and m.b hold a power of two >= cap entries
+    uint64_t* ka = in_smem ? msh : m.a;
+    uint32_t* kb = in_smem ? reinterpret_cast<uint32_t*>(msh + MERGE_SMEM_CAP) : m.b;
+    for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) {
+        if (t < cnt) {
+            const uint32_t q = m.changed[t];
+            ka[t] = ((uint64_t)m.newkey[q] << 32) | q;
+            kb[t] = q;
+        } else {
+            ka[t] = ~0ull;
+            kb[t] = ~0u;
+        }
+    }
+    __syncthreads();
+    block_bitonic(ka, P);
+    block_bitonic(kb, P);
+    if (in_smem)
+        for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+            m.a[t] = ka[t];
+            m.b[t] = kb[t];
+        }
+}
+
+cudaError_t merge_sort_setup() {
+    return cudaFuncSetAttribute(k_merge_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(MERGE_SMEM_CAP * (sizeof(uint64_t) + sizeof(uint32_t))));
+}
+
+void launch_merge_keys_sort(const float4* pos, const float4* tmp, int apply, const Grid& g, Scalars* sc,
+                            const uint32_t* id, const BatchDev& batch, const uint32_t* cell_old,
+                            const MergeScratch& m, uint32_t cap, cudaStream_t st) {
+    k_merge_keys<<<(cap + 255) / 256, 256, 0, st>>>(pos, tmp, apply, g, sc, id, batch, cell_old, m);
+    k_merge_sort<<<1, MERGE_SORT_THREADS, MERGE_SMEM_CAP * (sizeof(uint64_t) + sizeof(uint32_t)), st>>>(m);
+}
+
 // ---------------------------------------------------------------- cell tables
 // (cell_start_fill is in cellsort.cuh; the particle steps' rebuild fills the
 // table in its gather kernel)

@@ -52,6 +52,35 @@ int launch_keys_and_sort(const float4* pos, const float4* tmp, int apply, const 
                          const uint32_t* id, const BatchDev& batch, SortScratch& s, int passes, cudaStream_t st);
 
 
+// ---- merge rebuild
+// Between two rebuilds only the particles whose cell changed move in the
+// stably sorted order: the others keep their relative order (their keys are
+// unchanged and they were sorted by key, then by previous position).  The
+// new order is therefore the merge of the unchanged particles, in place,
+// with the changed ones sorted by (new key, previous position), which is
+// exactly the stable sort's result.  The keys kernel finds the changed
+// particles, one block sorts them (in shared memory up to
+// MERGE_SMEM_CAP of them, else in global memory, slowly but correctly), and
+// the merge gather (physics.cuh) moves every particle to its merged
+// position and derives the new cell table from the old one.
+constexpr uint32_t MERGE_SMEM_CAP = 8192;
+constexpr int MERGE_SORT_THREADS = 1024;
+
+struct MergeScratch {
+    uint32_t* newkey = nullptr;   // cap: each particle's key after the pending update
+    uint32_t* changed = nullptr;  // cap: positions of the changed particles, in no order
+    uint64_t* a = nullptr;        // cap: (new key << 32 | position) of the changed, ascending
+    uint32_t* b = nullptr;        // cap: positions of the changed, ascending
+    uint32_t* count = nullptr;    // [0] changed found by the keys kernel, [1] the count the merge uses
+};
+
+// The keys, the changed list and its two sorted orders (two launches).  The
+// merge gather follows (launch_merge_gather).
+void launch_merge_keys_sort(const float4* pos, const float4* tmp, int apply, const Grid& g, Scalars* sc,
+                            const uint32_t* id, const BatchDev& batch, const uint32_t* cell_old,
+                            const MergeScratch& m, uint32_t cap, cudaStream_t st);
+cudaError_t merge_sort_setup();
+
 // Same pieces with n given on the host (for the device-pointer primitive).
 void launch_cell_keys_plain(const float4* pos, uint32_t n, const Grid& g, uint32_t* keys, uint32_t* vals,
                             cudaStream_t st);

@@ -19,6 +19,77 @@ static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) /
 // exactly as k_cell_keys applied it to find its cell; particles sorted past
 // np_new (outside the grid) become type 3 with zero velocity and leave the
 // active range (MPS_CAL_expl_v1.0/MPS_GPU.cpp:268-280, 329).
+// Moves particle `old` of src to position p of dst, applying the pending
+// update of a fluid particle exactly as the keys kernel applied it to find
+// its cell; a key past the grid (left it) makes it type 3 at rest.  Returns
+// its type.
+__device__ __forceinline__ uint32_t move_particle(const State& src, const State& dst, uint32_t old, uint32_t p,
+                                                  uint32_t key, uint32_t ncells, const float4* __restrict__ tmp,
+                                                  int apply, uint32_t* __restrict__ index_of_id,
+                                                  const Scalars* __restrict__ sc, const BatchDev& batch) {
+    float4 x = src.pos[old], u = src.vel[old];
+    if (apply != 0 && ptype(x) == T_FLUID) {
+        const float dt = batch.n ? batch.dt[batch.sid_of_id[src.id[old]]] : sc->dt;
+        const float4 d = tmp[old];
+        if (apply == 1) {
+            u.x = d.x; u.y = d.y; u.z = d.z;
+        } else {
+            u.x = __fadd_rn(u.x, d.x); u.y = __fadd_rn(u.y, d.y); u.z = __fadd_rn(u.z, d.z);
+        }
+        x.x = __fadd_rn(x.x, __fmul_rn(dt, d.x));
+        x.y = __fadd_rn(x.y, __fmul_rn(dt, d.y));
+        x.z = __fadd_rn(x.z, __fmul_rn(dt, d.z));
+    }
+    if (key >= ncells) {  // left the grid
+        x.w = __uint_as_float(T_EXCL);
+        u = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    dst.pos[p] = x;
+    dst.vel[p] = u;
+    dst.press[p] = src.press[old];
+    dst.n[p] = src.n[old];
+    const uint32_t id = src.id[old];
+    dst.id[p] = id;
+    dst.cell[p] = key;
+    index_of_id[id] = p;
+    return ptype(x);
+}
+
+// The end of both gathers: this warp's particles (type ty, new position p)
+// appended to the compact lists of the active fluid and non-dummy particles
+// (order within a list does not matter: every particle's stage result is
+// independent), then the last block to finish publishes the new active count.
+__device__ __forceinline__ void gather_tail(uint32_t ty, uint32_t p, uint32_t n, Scalars* __restrict__ sc,
+                                            uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid) {
+    if (list_fluid) {
+        const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+        const bool f = ty == T_FLUID, s2 = ty == T_FLUID || ty == T_WALL;
+        const uint32_t mf = __ballot_sync(0xffffffffu, f), ms = __ballot_sync(0xffffffffu, s2);
+        uint32_t bf = 0, bs = 0;
+        if (lane == 0) {
+            if (mf) bf = atomicAdd(&sc->n_fluid, __popc(mf));
+            if (ms) bs = atomicAdd(&sc->n_solid, __popc(ms));
+        }
+        bf = __shfl_sync(0xffffffffu, bf, 0);
+        bs = __shfl_sync(0xffffffffu, bs, 0);
+        if (f) list_fluid[bf + __popc(mf & lt)] = p;
+        if (s2) list_solid[bs + __popc(ms & lt)] = p;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&sc->done_blocks, 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            const uint32_t nn = *(volatile uint32_t*)&sc->np_new;
+            sc->nexcl += n - nn;
+            sc->np = nn;
+            sc->done_blocks = 0;
+            __threadfence();
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint32_t* __restrict__ perm,
                                                 const uint32_t* __restrict__ keys_sorted,
                                                 const float4* __restrict__ tmp, int apply,
@@ -36,65 +107,70 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
         if (prev < (long long)ncells && cur >= (long long)ncells) sc->np_new = p;
     }
     uint32_t ty = T_EXCL;
-    if (p < n) {
-        const uint32_t old = perm[p];
-        float4 x = src.pos[old], u = src.vel[old];
-        if (apply != 0 && ptype(x) == T_FLUID) {
-            const float dt = batch.n ? batch.dt[batch.sid_of_id[src.id[old]]] : sc->dt;
-            const float4 d = tmp[old];
-            if (apply == 1) {
-                u.x = d.x; u.y = d.y; u.z = d.z;
-            } else {
-                u.x = __fadd_rn(u.x, d.x); u.y = __fadd_rn(u.y, d.y); u.z = __fadd_rn(u.z, d.z);
-            }
-            x.x = __fadd_rn(x.x, __fmul_rn(dt, d.x));
-            x.y = __fadd_rn(x.y, __fmul_rn(dt, d.y));
-            x.z = __fadd_rn(x.z, __fmul_rn(dt, d.z));
-        }
-        if (keys_sorted[p] >= ncells) {  // left the grid
-            x.w = __uint_as_float(T_EXCL);
-            u = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        dst.pos[p] = x;
-        dst.vel[p] = u;
-        dst.press[p] = src.press[old];
-        dst.n[p] = src.n[old];
-        const uint32_t id = src.id[old];
-        dst.id[p] = id;
-        dst.cell[p] = keys_sorted[p];
-        index_of_id[id] = p;
-        ty = ptype(x);
+    if (p < n) ty = move_particle(src, dst, perm[p], p, keys_sorted[p], ncells, tmp, apply, index_of_id, sc, batch);
+    gather_tail(ty, p, n, sc, list_fluid, list_solid);
+}
+
+// entries of the ascending x[0..m) below v
+template <class T>
+__device__ __forceinline__ uint32_t count_below(const T* __restrict__ x, uint32_t m, T v) {
+    uint32_t lo = 0, hi = m;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (x[mid] < v) lo = mid + 1;
+        else hi = mid;
     }
-    // compact lists of the active fluid and non-dummy particles (order within
-    // a list does not matter: every particle's stage result is independent)
-    if (list_fluid) {
-        const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
-        const bool f = ty == T_FLUID, s2 = ty == T_FLUID || ty == T_WALL;
-        const uint32_t mf = __ballot_sync(0xffffffffu, f), ms = __ballot_sync(0xffffffffu, s2);
-        uint32_t bf = 0, bs = 0;
-        if (lane == 0) {
-            if (mf) bf = atomicAdd(&sc->n_fluid, __popc(mf));
-            if (ms) bs = atomicAdd(&sc->n_solid, __popc(ms));
-        }
-        bf = __shfl_sync(0xffffffffu, bf, 0);
-        bs = __shfl_sync(0xffffffffu, bs, 0);
-        if (f) list_fluid[bf + __popc(mf & lt)] = p;
-        if (s2) list_solid[bs + __popc(ms & lt)] = p;
+    return lo;
+}
+
+// The merge rebuild's gather (cellsort.cuh): with B the changed particles'
+// previous positions and A their (new key, previous position), both
+// ascending, an unchanged particle at q goes to q - |B < q| + |A < (key, q)|
+// and a changed one to its rank in A plus the unchanged particles before
+// it, b - |B < b| with b = the first previous position past (key, q) in the
+// old order; the new cell table is cs_old[c] - |B < cs_old[c]| +
+// |A < (c, 0)|.  One thread per particle and per table entry.
+__global__ void __launch_bounds__(256) k_merge_gather(State src, State dst, const uint32_t* __restrict__ newkey,
+                                                      const uint64_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                                      const uint32_t* __restrict__ count,
+                                                      const uint32_t* __restrict__ cs_old, uint32_t* __restrict__ cs_new,
+                                                      uint32_t ncells, const float4* __restrict__ tmp, int apply,
+                                                      uint32_t* __restrict__ index_of_id, Scalars* __restrict__ sc,
+                                                      uint32_t* __restrict__ list_fluid,
+                                                      uint32_t* __restrict__ list_solid, BatchDev batch) {
+    const uint32_t n = sc->np;
+    const uint32_t m = count[1];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= ncells) {
+        const uint32_t c0 = cs_old[t];
+        const uint32_t v = c0 - count_below(b, m, c0) + count_below(a, m, (uint64_t)t << 32);
+        cs_new[t] = v;
+        if (t == ncells) sc->np_new = v;
     }
-    // the last block to finish publishes the new active count
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const uint32_t done = atomicAdd(&sc->done_blocks, 1u);
-        if (done == gridDim.x - 1) {
-            __threadfence();
-            const uint32_t nn = *(volatile uint32_t*)&sc->np_new;
-            sc->nexcl += n - nn;
-            sc->np = nn;
-            sc->done_blocks = 0;
-            __threadfence();
+    uint32_t ty = T_EXCL, p = 0;
+    if (t < n) {
+        const uint32_t k = newkey[t];
+        const uint32_t ra = count_below(a, m, ((uint64_t)k << 32) | t);
+        if (k != src.cell[t]) {
+            const uint32_t lo = k < ncells ? cs_old[k] : n, hi = k < ncells ? cs_old[k + 1] : n;
+            const uint32_t bnd = t < lo ? lo : (t > hi ? hi : t);
+            p = ra + bnd - count_below(b, m, bnd);
+        } else {
+            p = t - count_below(b, m, t) + ra;
         }
+        ty = move_particle(src, dst, t, p, k, ncells, tmp, apply, index_of_id, sc, batch);
     }
+    gather_tail(ty, p, n, sc, list_fluid, list_solid);
+}
+
+void launch_merge_gather(const State& src, const State& dst, const MergeScratch& m, const uint32_t* cs_old,
+                         uint32_t* cs_new, uint32_t ncells, const float4* tmp, int apply, uint32_t* index_of_id,
+                         Scalars* sc, uint32_t cap, cudaStream_t st, uint32_t* list_fluid, uint32_t* list_solid,
+                         const BatchDev& batch) {
+    const uint32_t threads = cap > ncells + 1 ? cap : ncells + 1;
+    k_merge_gather<<<blocks_for(threads, 256), 256, 0, st>>>(src, dst, m.newkey, m.a, m.b, m.count, cs_old, cs_new,
+                                                              ncells, tmp, apply, index_of_id, sc, list_fluid,
+                                                              list_solid, batch);
 }
 
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,

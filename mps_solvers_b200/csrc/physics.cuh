@@ -3,6 +3,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "cellsort.cuh"
 #include "mps_device.cuh"
 
 namespace mpsb {
@@ -83,6 +84,14 @@ __device__ __forceinline__ Local local_of(const StageArgs& a, uint32_t i) {
 __device__ __forceinline__ Phys phys_of(const StageArgs& a, uint32_t s) {
     return a.batch.n ? phys_of<true>(a, s) : phys_of<false>(a, s);
 }
+
+// the merge rebuild's reorder (cellsort.cuh: launch_merge_keys_sort first):
+// every particle moved to its merged position with the pending update
+// applied, and the new cell table cs_new from cs_old
+void launch_merge_gather(const State& src, const State& dst, const MergeScratch& m, const uint32_t* cs_old,
+                         uint32_t* cs_new, uint32_t ncells, const float4* tmp, int apply, uint32_t* index_of_id,
+                         Scalars* sc, uint32_t cap, cudaStream_t st, uint32_t* list_fluid, uint32_t* list_solid,
+                         const BatchDev& batch);
 
 // reorder after a sort: dst[p] = src[perm[p]] with the pending update applied
 void launch_gather(const State& src, const State& dst, const uint32_t* perm, const uint32_t* keys_sorted,
