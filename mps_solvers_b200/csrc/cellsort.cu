@@ -328,6 +328,32 @@ __global__ void __launch_bounds__(MERGE_SORT_THREADS) k_merge_sort(MergeScratch 
         m.count[0] = 0;  // empty for the next rebuild's keys kernel
     }
     if (cnt == 0) return;
+    if (cnt <= MERGE_SORT_THREADS) {
+        // few (the common case): every entry's rank is the count of smaller
+        // ones (the entries are distinct: they hold distinct positions)
+        uint64_t* ka = msh;
+        uint32_t* kb = reinterpret_cast<uint32_t*>(msh + MERGE_SORT_THREADS);
+        const uint32_t t = threadIdx.x;
+        uint64_t va = 0;
+        uint32_t vb = 0;
+        if (t < cnt) {
+            vb = m.changed[t];
+            va = ((uint64_t)m.newkey[vb] << 32) | vb;
+            ka[t] = va;
+            kb[t] = vb;
+        }
+        __syncthreads();
+        if (t < cnt) {
+            uint32_t ra = 0, rb = 0;
+            for (uint32_t u = 0; u < cnt; u++) {
+                ra += ka[u] < va ? 1u : 0u;
+                rb += kb[u] < vb ? 1u : 0u;
+            }
+            m.a[ra] = va;
+            m.b[rb] = vb;
+        }
+        return;
+    }
     uint32_t P = 1;
     while (P < cnt) P <<= 1;
     const bool in_smem = P <= MERGE_SMEM_CAP;  // else m.a and m.b hold a power of two >= cap entries

@@ -9,8 +9,9 @@ give the same particle order, cell tables and states bit for bit:
 
 * explicit, exact arithmetic, with and without CUDA graphs;
 * semi-implicit with a moving piston (walls change cells too);
-* a state set from the host that moves every particle one cell along x, so
-  that more particles change cell than the shared-memory sort takes (its
+* a state set from the host that moves 3,000 particles one cell along x
+  (the sort's shared-memory bitonic case; fewer take its rank sort), or
+  every particle, so that more change cell than shared memory takes (its
   global-memory case) and some leave the grid.
 """
 import numpy as np
@@ -70,7 +71,8 @@ def test_semi_merge_with_moving_piston_equals_full_sort(capi, tmp_path):
     assert_same(out[0], out[1])
 
 
-def test_merge_after_host_state_moves_every_particle(capi, tmp_path):
+@pytest.mark.parametrize("moved", [3000, None])
+def test_merge_after_host_state_moves_particles(capi, tmp_path, moved):
     d = case(tmp_path, "t", **TANK)
     out = []
     for merge in (0, -1):
@@ -79,7 +81,8 @@ def test_merge_after_host_state_moves_every_particle(capi, tmp_path):
             g = s.grid()
             st = s.state()
             pos = st["pos"].copy()
-            pos[:, 0] += np.float32(g.cell_size)  # every particle one cell along x; the last layer leaves
+            sel = slice(None) if moved is None else slice(0, moved)
+            pos[sel, 0] += np.float32(g.cell_size)  # one cell along x; the last layer leaves
             s.set_state(pos=pos)
             try:
                 s.step(1)
