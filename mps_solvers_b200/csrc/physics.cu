@@ -19,40 +19,55 @@ static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) /
 // exactly as k_cell_keys applied it to find its cell; particles sorted past
 // np_new (outside the grid) become type 3 with zero velocity and leave the
 // active range (MPS_CAL_expl_v1.0/MPS_GPU.cpp:268-280, 329).
-// Moves particle `old` of src to position p of dst, applying the pending
-// update of a fluid particle exactly as the keys kernel applied it to find
-// its cell; a key past the grid (left it) makes it type 3 at rest.  Returns
-// its type.
-__device__ __forceinline__ uint32_t move_particle(const State& src, const State& dst, uint32_t old, uint32_t p,
-                                                  uint32_t key, uint32_t ncells, const float4* __restrict__ tmp,
-                                                  int apply, uint32_t* __restrict__ index_of_id,
-                                                  const Scalars* __restrict__ sc, const BatchDev& batch) {
-    float4 x = src.pos[old], u = src.vel[old];
-    if (apply != 0 && ptype(x) == T_FLUID) {
-        const float dt = batch.n ? batch.dt[batch.sid_of_id[src.id[old]]] : sc->dt;
+// A particle as the gathers move it: read from position `old` of src with
+// the pending update of a fluid particle applied exactly as the keys kernel
+// applied it to find its cell.  store_particle writes it to position p of
+// dst; a key past the grid (left it) makes it type 3 at rest.  The merge
+// gather loads before it knows p, so the loads overlap its searches.
+struct Moved {
+    float4 x, u;
+    float press, n;
+    uint32_t id;
+};
+
+__device__ __forceinline__ Moved load_particle(const State& src, uint32_t old, const float4* __restrict__ tmp,
+                                               int apply, const Scalars* __restrict__ sc, const BatchDev& batch) {
+    Moved v;
+    v.x = src.pos[old];
+    v.u = src.vel[old];
+    v.press = src.press[old];
+    v.n = src.n[old];
+    v.id = src.id[old];
+    if (apply != 0 && ptype(v.x) == T_FLUID) {
+        const float dt = batch.n ? batch.dt[batch.sid_of_id[v.id]] : sc->dt;
         const float4 d = tmp[old];
         if (apply == 1) {
-            u.x = d.x; u.y = d.y; u.z = d.z;
+            v.u.x = d.x; v.u.y = d.y; v.u.z = d.z;
         } else {
-            u.x = __fadd_rn(u.x, d.x); u.y = __fadd_rn(u.y, d.y); u.z = __fadd_rn(u.z, d.z);
+            v.u.x = __fadd_rn(v.u.x, d.x); v.u.y = __fadd_rn(v.u.y, d.y); v.u.z = __fadd_rn(v.u.z, d.z);
         }
-        x.x = __fadd_rn(x.x, __fmul_rn(dt, d.x));
-        x.y = __fadd_rn(x.y, __fmul_rn(dt, d.y));
-        x.z = __fadd_rn(x.z, __fmul_rn(dt, d.z));
+        v.x.x = __fadd_rn(v.x.x, __fmul_rn(dt, d.x));
+        v.x.y = __fadd_rn(v.x.y, __fmul_rn(dt, d.y));
+        v.x.z = __fadd_rn(v.x.z, __fmul_rn(dt, d.z));
     }
+    return v;
+}
+
+// returns the particle's type
+__device__ __forceinline__ uint32_t store_particle(const State& dst, Moved v, uint32_t p, uint32_t key,
+                                                   uint32_t ncells, uint32_t* __restrict__ index_of_id) {
     if (key >= ncells) {  // left the grid
-        x.w = __uint_as_float(T_EXCL);
-        u = make_float4(0.f, 0.f, 0.f, 0.f);
+        v.x.w = __uint_as_float(T_EXCL);
+        v.u = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    dst.pos[p] = x;
-    dst.vel[p] = u;
-    dst.press[p] = src.press[old];
-    dst.n[p] = src.n[old];
-    const uint32_t id = src.id[old];
-    dst.id[p] = id;
+    dst.pos[p] = v.x;
+    dst.vel[p] = v.u;
+    dst.press[p] = v.press;
+    dst.n[p] = v.n;
+    dst.id[p] = v.id;
     dst.cell[p] = key;
-    index_of_id[id] = p;
-    return ptype(x);
+    index_of_id[v.id] = p;
+    return ptype(v.x);
 }
 
 // The end of both gathers: this warp's particles (type ty, new position p)
@@ -107,20 +122,33 @@ __global__ void __launch_bounds__(256) k_gather(State src, State dst, const uint
         if (prev < (long long)ncells && cur >= (long long)ncells) sc->np_new = p;
     }
     uint32_t ty = T_EXCL;
-    if (p < n) ty = move_particle(src, dst, perm[p], p, keys_sorted[p], ncells, tmp, apply, index_of_id, sc, batch);
+    if (p < n)
+        ty = store_particle(dst, load_particle(src, perm[p], tmp, apply, sc, batch), p, keys_sorted[p], ncells,
+                            index_of_id);
     gather_tail(ty, p, n, sc, list_fluid, list_solid);
 }
 
-// entries of the ascending x[0..m) below v
-template <class T>
-__device__ __forceinline__ uint32_t count_below(const T* __restrict__ x, uint32_t m, T v) {
-    uint32_t lo = 0, hi = m;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (x[mid] < v) lo = mid + 1;
-        else hi = mid;
+// The counts of entries below va in the ascending a[0..m) and below vb in
+// the ascending b[0..m), searched in one loop so that the two searches'
+// loads are in flight together
+__device__ __forceinline__ void count_below2(const uint64_t* __restrict__ a, uint64_t va,
+                                             const uint32_t* __restrict__ b, uint32_t vb, uint32_t m, uint32_t& ra,
+                                             uint32_t& rb) {
+    uint32_t alo = 0, ahi = m, blo = 0, bhi = m;
+    while (alo < ahi || blo < bhi) {
+        if (alo < ahi) {
+            const uint32_t mid = (alo + ahi) >> 1;
+            if (a[mid] < va) alo = mid + 1;
+            else ahi = mid;
+        }
+        if (blo < bhi) {
+            const uint32_t mid = (blo + bhi) >> 1;
+            if (b[mid] < vb) blo = mid + 1;
+            else bhi = mid;
+        }
     }
-    return lo;
+    ra = alo;
+    rb = blo;
 }
 
 // The merge rebuild's gather (cellsort.cuh): with B the changed particles'
@@ -143,22 +171,26 @@ __global__ void __launch_bounds__(256) k_merge_gather(State src, State dst, cons
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t <= ncells) {
         const uint32_t c0 = cs_old[t];
-        const uint32_t v = c0 - count_below(b, m, c0) + count_below(a, m, (uint64_t)t << 32);
+        uint32_t ra, rb;
+        count_below2(a, (uint64_t)t << 32, b, c0, m, ra, rb);
+        const uint32_t v = c0 - rb + ra;
         cs_new[t] = v;
         if (t == ncells) sc->np_new = v;
     }
     uint32_t ty = T_EXCL, p = 0;
     if (t < n) {
+        const Moved v = load_particle(src, t, tmp, apply, sc, batch);
         const uint32_t k = newkey[t];
-        const uint32_t ra = count_below(a, m, ((uint64_t)k << 32) | t);
-        if (k != src.cell[t]) {
+        const bool changed = k != src.cell[t];
+        uint32_t bnd = t;  // the unchanged particle's own position
+        if (changed) {
             const uint32_t lo = k < ncells ? cs_old[k] : n, hi = k < ncells ? cs_old[k + 1] : n;
-            const uint32_t bnd = t < lo ? lo : (t > hi ? hi : t);
-            p = ra + bnd - count_below(b, m, bnd);
-        } else {
-            p = t - count_below(b, m, t) + ra;
+            bnd = t < lo ? lo : (t > hi ? hi : t);
         }
-        ty = move_particle(src, dst, t, p, k, ncells, tmp, apply, index_of_id, sc, batch);
+        uint32_t ra, rb;
+        count_below2(a, ((uint64_t)k << 32) | t, b, bnd, m, ra, rb);
+        p = changed ? ra + bnd - rb : t - rb + ra;
+        ty = store_particle(dst, v, p, k, ncells, index_of_id);
     }
     gather_tail(ty, p, n, sc, list_fluid, list_solid);
 }
