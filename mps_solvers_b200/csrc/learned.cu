@@ -145,8 +145,8 @@ struct FwdArgs {
     float* dgpre;
 };
 
-// round 1 (round == 1) or round 2 messages, mean-aggregated into a_out
-template <int ROUND>
+// the first (PASS == 1) or second message pass, mean-aggregated into a_out
+template <int PASS>
 __global__ void __launch_bounds__(256) k_lp_edge_fwd(FwdArgs A) {
     const LpSystem& S = A.S;
     const uint32_t R = *S.nrows;
@@ -154,8 +154,8 @@ __global__ void __launch_bounds__(256) k_lp_edge_fwd(FwdArgs A) {
     const uint32_t lane = threadIdx.x & 31;
     if (k >= R) return;
     const uint32_t i = __ldg(S.rowlist + k);
-    const int WE = ROUND == 1 ? LP_W1E : LP_W2E;
-    const int BB = ROUND == 1 ? LP_B1 : LP_B2;
+    const int WE = PASS == 1 ? LP_W1E : LP_W2E;
+    const int BB = PASS == 1 ? LP_B1 : LP_B2;
     float w0[LP_F], w1[LP_F];
 #pragma unroll
     for (int f = 0; f < LP_F; f++) {
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(256) k_lp_edge_fwd(FwdArgs A) {
             s0 = fmaf(w0[f], e.f[f], s0);
             s1 = fmaf(w1[f], e.f[f], s1);
         }
-        if (ROUND == 2) {
+        if (PASS == 2) {
             s0 += A.uh1[(size_t)j * LP_H + lane];
             s1 += A.uh1[(size_t)j * LP_H + lane + 32];
         }
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) k_lp_edge_fwd(FwdArgs A) {
         acc1 += gelu_t(s1, nullptr);
     }
     const float inv = cnt ? 1.f / (float)cnt : 0.f;
-    float* a = ROUND == 1 ? A.a1 : A.a2;
+    float* a = PASS == 1 ? A.a1 : A.a2;
     a[(size_t)i * LP_H + lane] = acc0 * inv;
     a[(size_t)i * LP_H + lane + 32] = acc1 * inv;
 }
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(256) k_lp_copy_rows(const float* __restrict__ 
 
 // edge messages, pass A (row i): W{1,2}e and b{1,2} gradients from
 // ds_ij = (da_i / cnt_i) * GELU'(s_ij)
-template <int ROUND>
+template <int PASS>
 __global__ void __launch_bounds__(256) k_lp_edge_bwd_a(BwdArgs A) {
     __shared__ float s_we[LP_H * LP_F];
     __shared__ float s_b[LP_H];
@@ -622,8 +622,8 @@ __global__ void __launch_bounds__(256) k_lp_edge_bwd_a(BwdArgs A) {
     const uint32_t R = *S.nrows;
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
-    const int WE = ROUND == 1 ? LP_W1E : LP_W2E;
-    const int BB = ROUND == 1 ? LP_B1 : LP_B2;
+    const int WE = PASS == 1 ? LP_W1E : LP_W2E;
+    const int BB = PASS == 1 ? LP_B1 : LP_B2;
     float gw0[LP_F] = {0}, gw1[LP_F] = {0};
     float gb0 = 0.f, gb1 = 0.f;
     if (k < R) {
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(256) k_lp_edge_bwd_a(BwdArgs A) {
                 s0 = fmaf(w0[f], e.f[f], s0);
                 s1 = fmaf(w1[f], e.f[f], s1);
             }
-            if (ROUND == 2) {
+            if (PASS == 2) {
                 s0 += A.uh1[(size_t)j * LP_H + lane];
                 s1 += A.uh1[(size_t)j * LP_H + lane + 32];
             }
@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(256) k_lp_edge_bwd_a(BwdArgs A) {
     for (int t = threadIdx.x; t < LP_H; t += blockDim.x) atomicAdd(A.grad + BB + t, s_b[t]);
 }
 
-// round-2 messages, pass B (row j): duh1_j = sum over the edges (i, j) of ds_ij
+// second message pass, part B (row j): duh1_j = sum over the edges (i, j) of ds_ij
 __global__ void __launch_bounds__(256) k_lp_edge2_bwd_b(BwdArgs A, float* __restrict__ duh1) {
     const LpSystem& S = A.S;
     const uint32_t R = *S.nrows;
@@ -1248,7 +1248,7 @@ int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, u
     k_lp_readout_bwd_b<<<wb, 256, 0, st>>>(B);
     k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.dra, L.h2, L.w16, LP_RA, L.dh2, 1, L.grad, -1, S.rowlist, S.nrows);
     k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.drb, L.h2, L.w16, LP_RB, L.dh2, 1, L.grad, -1, S.rowlist, S.nrows);
-    // round 2 node: h2 = GELU(pre2) + h1
+    // second message pass, node: h2 = GELU(pre2) + h1
     const uint32_t eb = blocks_for(cap * (uint32_t)LP_H, 256);
     k_lp_copy_rows<<<eb, 256, 0, st>>>(L.dh2, L.dh1, S.rowlist, S.nrows);
     k_lp_gelu_bwd<<<eb, 256, 0, st>>>(L.dh2, L.pre2, L.dra, S.rowlist, S.nrows);  // dra reused as dpre2
@@ -1256,7 +1256,7 @@ int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, u
     k_lp_edge_bwd_a<2><<<wb, 256, 0, st>>>(B);
     k_lp_edge2_bwd_b<<<wb, 256, 0, st>>>(B, L.duh1);
     k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.duh1, L.h1, L.w16, LP_U2, L.dh1, 1, L.grad, -1, S.rowlist, S.nrows);
-    // round 1 node: h1 = GELU(pre1)
+    // first message pass, node: h1 = GELU(pre1)
     k_lp_gelu_bwd<<<eb, 256, 0, st>>>(L.dh1, L.pre1, L.dra, S.rowlist, S.nrows);  // dpre1
     k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.dra, L.a1, L.w16, LP_V1, L.da, 0, L.grad, LP_C1, S.rowlist, S.nrows);
     k_lp_edge_bwd_a<1><<<wb, 256, 0, st>>>(B);

@@ -9,9 +9,9 @@
 //
 //   edge features e_ij (7): dx/r0, dy/r0, dz/r0, |r|/r0, w(r; r0)/w_ref,
 //                           n_i/n0, [j is a wall particle]
-//   round 1: a1_i = mean_j GELU(W1e e_ij + b1)            (64)
+//   pass 1: a1_i = mean_j GELU(W1e e_ij + b1)            (64)
 //            h1_i = GELU(V1 a1_i + c1)                      (64)
-//   round 2: a2_i = mean_j GELU(W2e e_ij + U2 h1_j + b2)   (64)
+//   pass 2: a2_i = mean_j GELU(W2e e_ij + U2 h1_j + b2)   (64)
 //            h2_i = GELU(V2 a2_i + c2) + h1_i               (64)
 //   readout: G_ij = om . GELU(Re e_ij + Ra h2_i + Rb h2_j + br)   (j < i)
 //            G_ii = softplus(dl . h2_i + bd) + GMIN
