@@ -210,9 +210,12 @@ mps_status mps_phase(mps_handle* h, int phase);
  * with CUDA events between stages; stage_ms[k] (k < max_stages) receives the
  * summed milliseconds of stage k, *nstages the number of stages, and
  * mps_stage_name(k) its name (update_dt, visc, collision, pnd, pressure,
- * dash, step_end, cell_keys, radix_sort, cell_table, gather, ppe_solve;
- * pressure is the dummy copy of the explicit method or the PPE assembly of
- * the semi-implicit one).  The steps advance the simulation like mps_step. */
+ * dash, step_end, cell_keys, radix_sort, cell_table, gather, ppe_solve,
+ * motion; pressure is the dummy copy of the explicit method or the PPE
+ * assembly of the semi-implicit one; radix_sort holds the cell keys and
+ * their sort, by radix passes or, with the merge rebuild, the changed
+ * particles' sort; cell_keys and cell_table are 0, their work done inside
+ * radix_sort and gather).  The steps advance the simulation like mps_step. */
 mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int max_stages, int* nstages);
 const char* mps_stage_name(int k);
 
