@@ -253,6 +253,28 @@ mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint64_t seed, 
 mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double* max_rel_diff);
 mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
                             double* diag, uint32_t* count);
+/* The off-diagonal entries of the last assembled PPE matrix exactly as the
+ * solver stores them, i.e. the neighbour set of buildPoisson
+ * (MPS_CAL_v4.0/MPS_CPU.cpp:651-698: j of type != 2 within rlap with a
+ * nonzero weight and not a Dirichlet row) of each non-Dirichlet row i:
+ * row_start (np + 1 entries, sorted particle order) and, when cols / weights
+ * are not NULL, the columns (sorted particle indices, ascending) and their
+ * weights in cols[row_start[i] .. row_start[i + 1]).  *nnz receives the
+ * total; more than max_entries gives MPS_ERR_CAPACITY (call with cols =
+ * weights = NULL first to size the buffers).  A debug getter like
+ * mps_get_cell_tables; it allocates temporary device memory. */
+mps_status mps_ppe_stencil(mps_handle* h, uint32_t* row_start, uint32_t* cols, float* weights,
+                           uint64_t max_entries, uint64_t* nnz);
+
+/* Bounded device waits.  The persistent PPE solvers synchronise their blocks
+ * with grid-wide barriers; a barrier that is not complete after this many
+ * nanoseconds of spinning sets MPS_ERR_DEVICE_TIMEOUT, every block returns,
+ * and the next mps_step or getter reports the error (the context stays
+ * usable).  0 restores the default of 1 s.  No counterpart in the reference,
+ * which has no device-side waits (its host exit()s on errors,
+ * MPS_CAL_/MPS_GPU.cpp:1449-1455); a very small limit makes the timeout path
+ * testable without any fault. */
+mps_status mps_set_device_wait_limit(mps_handle* h, uint64_t ns);
 
 /* The handle's cudaStream_t, for callers that time or order work around it. */
 mps_status mps_get_stream(mps_handle* h, void** stream);
@@ -285,10 +307,12 @@ mps_status mps_cell_sort_dev(const float* pos4_dev, uint32_t n, const mps_grid* 
  * the device-wide synchronisation of cudaMalloc/cudaFree is not acceptable.
  * Limits: n <= MPS_NOALLOC_MAX_PARTICLES and ncells <= MPS_NOALLOC_MAX_CELLS,
  * else MPS_ERR_CAPACITY.  All calls on a device share the array, so calls
- * whose GPU work overlaps race and must be serialised.  The first call on a
- * device (with it current) looks the array's address up; make it before any
- * stream capture.  The array stays allocated on every device that loaded the
- * library until the process exits. */
+ * whose GPU work overlaps race and must be serialised.  Every call looks the
+ * array's address up for the current device and context (so it stays valid
+ * after cudaDeviceReset).  The call waits for its stream before returning and
+ * copies n from host memory, so it cannot be captured in a CUDA graph.  The
+ * array stays allocated on every device that loaded the library until the
+ * process exits. */
 #define MPS_NOALLOC_MAX_PARTICLES 524288u
 #define MPS_NOALLOC_MAX_CELLS 524288u
 mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t n, const mps_grid* g,

@@ -119,4 +119,32 @@ public:
     MPS_CPU_EXPL() : MPS_GPU_EXPL(MPS_METHOD_SEMI_IMPLICIT) {}
 };
 
+// The GL build's step class (MPS_CAL_/MPS_GPU.h:18-166), driven as
+//     mps = new mytype::MPS_GPU(); mps->Initial();   // MPS_CAL_/Renderer.h:54-56
+//     ... mps->step(); ... mps->getPos() ...         // MPS_CAL_/Renderer.h:312
+// Its step (MPS_CAL_/MPS_GPU.cpp:611-714) is the explicit equation-of-state
+// step: viscosity, collision, PND, pressure, gradient, then update_dt and
+// i_step++, the stages of MPS_GPU_EXPL::step.  Initial(), step() and the
+// getters are inherited; the two public stage members run one stage:
+class MPS_GPU : public MPS_GPU_EXPL {
+public:
+    MPS_GPU() : MPS_GPU_EXPL(MPS_METHOD_EXPLICIT) {}
+    // MPS_GPU::calVisc_expl: viscosity and gravity on the fluid, applied to
+    // velocities and positions (the library applies a stage's update while it
+    // re-sorts the cells, so this runs the stage and then that rebuild).
+    void calVisc_expl() {
+        if (!h_) Initial();
+        check(mps_phase(h_, 1));
+        check(mps_phase(h_, 2));
+        stale_ = true;
+    }
+    // MPS_GPU::calPres_expl: equation-of-state pressure from the current
+    // number density, and the dummy particles' copy of their wall pressure.
+    void calPres_expl() {
+        if (!h_) Initial();
+        check(mps_phase(h_, 5));
+        stale_ = true;
+    }
+};
+
 }  // namespace mytype

@@ -43,7 +43,7 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
            "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
            "mps_surface_case_table", "mps_precond_tensor_cores", "mps_add_wall_motion",
-           "mps_clear_wall_motion")
+           "mps_clear_wall_motion", "mps_set_device_wait_limit", "mps_ppe_stencil")
 
 
 class mps_options(C.Structure):
@@ -161,6 +161,8 @@ def lib():
             "mps_set_body_force": (C.c_int, [H, C.c_uint32, C.c_float, C.c_float]),
             "mps_add_wall_motion": (C.c_int, [H, Fp, Fp, Fp, Fp, C.c_float, C.c_float, U]),
             "mps_clear_wall_motion": (C.c_int, [H]),
+            "mps_set_device_wait_limit": (C.c_int, [H, C.c_uint64]),
+            "mps_ppe_stencil": (C.c_int, [H, U, U, Fp, C.c_uint64, C.POINTER(C.c_uint64)]),
             "mps_autotune": (C.c_int, [H, C.c_int, C.POINTER(mps_tune_report)]),
             "mps_surface_setup": (C.c_int, [H, C.POINTER(mps_surface_grid), C.c_uint32]),
             "mps_surface_extract_async": (C.c_int, [H]),
@@ -416,6 +418,24 @@ class Simulation:
                                            out["diag"].ctypes.data_as(C.POINTER(C.c_double)),
                                            C.byref(cnt)))
         return out
+
+    def ppe_stencil(self) -> Dict[str, np.ndarray]:
+        """The last assembled PPE matrix's off-diagonal entries as the solver
+        stores them: row_start (np + 1, sorted order), cols, weights."""
+        n = self.counts()["np"]
+        row_start = np.empty(n + 1, np.uint32)
+        nnz = C.c_uint64()
+        self._check(lib().mps_ppe_stencil(self.h, _p(row_start, C.c_uint32), None, None, 0, C.byref(nnz)))
+        cols = np.empty(max(nnz.value, 1), np.uint32)
+        w = np.empty(max(nnz.value, 1), np.float32)
+        self._check(lib().mps_ppe_stencil(self.h, _p(row_start, C.c_uint32), _p(cols, C.c_uint32), _p(w),
+                                          nnz.value, C.byref(nnz)))
+        return dict(row_start=row_start, cols=cols[:nnz.value], weights=w[:nnz.value])
+
+    def set_device_wait_limit(self, ns: int):
+        """Longest spin (ns) of one grid-wide wait in the PPE solvers before it
+        gives up with MPS_ERR_DEVICE_TIMEOUT (0: the default, 1 s)."""
+        self._check(lib().mps_set_device_wait_limit(self.h, int(ns)))
 
     def set_body_force(self, accel_amp: float, accel_freq: float, scene: int = 0):
         """Tank acceleration accel_amp*sin(2*pi*accel_freq*t) along x."""

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -951,6 +952,16 @@ extern "C" mps_status mps_set_body_force(mps_handle* h, uint32_t scene, float ac
     return MPS_OK;
 }
 
+extern "C" mps_status mps_set_device_wait_limit(mps_handle* h, uint64_t ns) {
+    if (!h) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    const unsigned long long v = ns;
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(h->sc) + offsetof(Scalars, wait_ns), &v, sizeof v,
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MPS_OK;
+}
+
 // ---------------------------------------------------------------- boundary motion
 extern "C" mps_status mps_add_wall_motion(mps_handle* h, const float lo[3], const float hi[3], const float vel[3],
                                           const float amp[3], float freq, float phase, uint32_t* selected) {
@@ -1455,6 +1466,22 @@ extern "C" mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uin
         for (size_t k = 0; k < np; k++) is_row[k] = is_row[k] != PPE_DIRICHLET ? 1u : 0u;
     if (count) *count = (uint32_t)np;
     return MPS_OK;
+}
+
+extern "C" mps_status mps_ppe_stencil(mps_handle* h, uint32_t* row_start, uint32_t* cols, float* weights,
+                                      uint64_t max_entries, uint64_t* nnz) {
+    mps_status s = need_semi(h, true);
+    if (s != MPS_OK) return s;
+    if (!h->ppe.have_snapshot) {
+        h->err = "no PPE system assembled yet";
+        return MPS_ERR_INVALID;
+    }
+    CK(cudaSetDevice(h->dev));
+    Scalars sc;
+    if (counts(h, &sc) != MPS_OK) return MPS_ERR_CUDA;
+    const int rc = ppe_export_stencil(h->ppe, sc.np, row_start, cols, weights, max_entries, nnz, h->stream);
+    if (rc == MPS_ERR_CAPACITY) h->err = "the stencil has more entries than max_entries";
+    return (mps_status)rc;
 }
 
 extern "C" const char* mps_stage_name(int k) { return (k >= 0 && k < ST_COUNT) ? kStageNames[k] : ""; }

@@ -48,7 +48,18 @@ struct Scalars {
     int pad_i;
     float g_eff[3];        // body force of the current step: g - a(time)
     float pad_f;
+    // longest spin of one grid-wide wait before it gives up with
+    // ERR_DEVICE_TIMEOUT (ns; 0: the default, 1 s); set by the host
+    unsigned long long wait_ns;
 };
+
+constexpr unsigned long long DEFAULT_WAIT_NS = 1000000000ull;
+
+// the wait budget of the grid-wide barriers, read once per wait
+__device__ __forceinline__ unsigned long long wait_budget_ns(const Scalars* sc) {
+    const unsigned long long w = __ldcg(&sc->wait_ns);
+    return w ? w : DEFAULT_WAIT_NS;
+}
 
 // The scenes of a batch: one particle set and one cell space made of each
 // scene's own particles and cell grid, with per-scene constants and step

@@ -24,12 +24,17 @@
 //     in the same call (keys, values, digit histograms of every tile, all
 //     ncells + 1 cell-table entries, the particle count), so nothing has to
 //     be cleared between calls.
-//   * the array's host-side name is only a stand-in for it; the device
-//     address is looked up with cudaGetSymbolAddress the first time the
-//     function runs on a device (with that device current) and cached, so
-//     make that first call on each device before any stream capture.
+//   * the array's host-side name is only a stand-in for it; every call looks
+//     the device address up with cudaGetSymbolAddress for the current device
+//     and context, so the address stays right after a cudaDeviceReset or when
+//     another context becomes current (nothing is cached);
+//   * the call cannot be captured in a CUDA graph: it copies n from host
+//     memory and ends by waiting for its stream (cudaStreamSynchronize);
+//   * errors: the launches' configurations are valid by construction for
+//     every accepted size, and the call reports the copies' return codes and
+//     the stream's result; it neither reads nor clears errors that other
+//     work left on the thread (no cudaGetLastError).
 #include <cstdint>
-#include <mutex>
 
 #include "../../include/mps_capi.h"
 #include "cellsort.cuh"
@@ -55,21 +60,13 @@ constexpr size_t kWords = kCount + 64;
 
 static __device__ __align__(256) uint32_t g_cellsort_scratch[kWords];
 
-// device address of g_cellsort_scratch, per device, looked up once
-constexpr int kMaxDevices = 64;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
+// Device address of g_cellsort_scratch in the current device's context,
+// looked up on every call (a cached address would go stale when the context
+// that loaded the module is destroyed, e.g. by cudaDeviceReset).
 mps_status scratch_for_current_device(uint32_t** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MPS_ERR_CUDA;
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_cellsort_scratch) != cudaSuccess || !p) return MPS_ERR_CUDA;
-        g_scratch_ptr[dev] = static_cast<uint32_t*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_cellsort_scratch) != cudaSuccess || !p) return MPS_ERR_CUDA;
+    *out = static_cast<uint32_t*>(p);
     return MPS_OK;
 }
 
@@ -110,12 +107,15 @@ extern "C" mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t 
     launch_cell_keys_plain((const float4*)pos4_dev, n, g, s.keys[0], s.vals[0], st);
     const int r = launch_radix_sort(s, n_dev, sort_passes(g.ncells), n, st);
     launch_cell_start_plain(s.keys[r], n, g, cs, n_in_grid_dev, st);
+    bool copies_ok = true;
     if (n) {
-        cudaMemcpyAsync(perm_dev, s.vals[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(cell_of_dev, s.keys[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+        copies_ok &= cudaMemcpyAsync(perm_dev, s.vals[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st) ==
+                     cudaSuccess;
+        copies_ok &= cudaMemcpyAsync(cell_of_dev, s.keys[r], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st) ==
+                     cudaSuccess;
     }
     launch_cell_end_from_start(cs, g.ncells, start_dev, end_dev, st);
     const cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return MPS_ERR_CUDA;
+    if (e != cudaSuccess || !copies_ok) return MPS_ERR_CUDA;
     return MPS_OK;
 }

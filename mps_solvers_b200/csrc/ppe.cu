@@ -83,13 +83,14 @@ __device__ bool grid_reduce(const double (&v)[K], double* part, double* /*result
             int ok = 1;
             unsigned cur;
             uint64_t t0;
+            const unsigned long long budget = wait_budget_ns(sc);
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             for (;;) {
                 asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
                 if ((int)(cur - target) >= 0) break;
                 uint64_t t1;
                 asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-                if (t1 - t0 > 1000000000ull) {
+                if (t1 - t0 > budget) {
                     atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
                     ok = 0;
                     break;
@@ -936,9 +937,13 @@ __device__ bool grid_reduce_scenes(double* acc, uint32_t ns, double* part, doubl
         }
     } else if (threadIdx.x == 0) {
         volatile unsigned* gen = bar + 1;
-        unsigned long long it = 0;
+        const unsigned long long budget = wait_budget_ns(sc);
+        uint64_t t0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
         while (*gen == gen0) {
-            if (++it > (1ull << 24)) {
+            uint64_t t1;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > budget) {
                 atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
                 ok = 0;
                 break;
@@ -1623,6 +1628,78 @@ static int enqueue_rows_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaS
     k_sell_pack<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.cols, w.wrm, w.rlen, w.rowlist, w.nrows,
                                                                   w.sell_off, w.sell_cols, w.sell_w);
     return launched;
+}
+
+// The stored off-diagonal entries of every row, copied out of the solver's
+// sliced layout into per-row lists (row i's entries at row_start[i] ..):
+// the operator exactly as the solver reads it, for tests.
+__global__ void __launch_bounds__(256) k_sell_export(const uint32_t* __restrict__ rlen,
+                                                     const uint32_t* __restrict__ rowlist,
+                                                     const uint32_t* __restrict__ nrows, const uint32_t* __restrict__ off,
+                                                     const uint32_t* __restrict__ scols, const float* __restrict__ sw,
+                                                     const uint32_t* __restrict__ row_start, uint32_t* __restrict__ cols,
+                                                     float* __restrict__ wts) {
+    const uint32_t R = *nrows;
+    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31, r = lane & 7, q = lane >> 3;
+    if (slice >= (R + SELL_C - 1) / SELL_C) return;
+    const uint32_t k = slice * SELL_C + r;
+    if (k >= R) return;
+    const uint32_t base = off[slice];
+    const uint32_t T = (off[slice + 1] - base) >> 7;
+    const uint32_t i = rowlist[k];
+    const uint32_t len = rlen[i];
+    const uint32_t o = row_start[i];
+    for (uint32_t t = 0; t < T; t++) {
+        for (uint32_t u = 0; u < 4; u++) {
+            const uint32_t e = 16u * t + 4u * q + u;
+            if (e < len) {
+                const size_t src = (size_t)base + 4u * (32u * t + lane) + u;
+                cols[o + e] = scols[src];
+                wts[o + e] = sw[src];
+            }
+        }
+    }
+}
+
+int ppe_export_stencil(const PpeWork& w, uint32_t np, uint32_t* row_start, uint32_t* cols, float* wts,
+                       uint64_t max_entries, uint64_t* nnz, cudaStream_t st) {
+    std::vector<uint32_t> len(np);
+    if (np && cudaMemcpyAsync(len.data(), w.rlen, (size_t)np * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return MPS_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MPS_ERR_CUDA;
+    std::vector<uint32_t> start(np + 1);
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < np; i++) {
+        start[i] = (uint32_t)t;
+        if (len[i] != PPE_DIRICHLET) t += len[i];
+    }
+    start[np] = (uint32_t)t;
+    if (t > 0xffffffffull) return MPS_ERR_CAPACITY;
+    if (nnz) *nnz = t;
+    if (row_start) memcpy(row_start, start.data(), (size_t)(np + 1) * 4);
+    if (!cols && !wts) return MPS_OK;
+    if (t > max_entries) return MPS_ERR_CAPACITY;
+    uint32_t *d_start = nullptr, *d_cols = nullptr;
+    float* d_w = nullptr;
+    int rc = MPS_OK;
+    if (cudaMalloc(&d_start, (size_t)(np + 1) * 4) != cudaSuccess || cudaMalloc(&d_cols, (t + 1) * 4) != cudaSuccess ||
+        cudaMalloc(&d_w, (t + 1) * 4) != cudaSuccess) {
+        rc = MPS_ERR_CUDA;
+    } else {
+        cudaMemcpyAsync(d_start, start.data(), (size_t)(np + 1) * 4, cudaMemcpyHostToDevice, st);
+        const uint32_t maxslices = (np + SELL_C - 1) / SELL_C;
+        if (maxslices)
+            k_sell_export<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off,
+                                                                            w.sell_cols, w.sell_w, d_start, d_cols, d_w);
+        if (cols) cudaMemcpyAsync(cols, d_cols, t * 4, cudaMemcpyDeviceToHost, st);
+        if (wts) cudaMemcpyAsync(wts, d_w, t * 4, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = MPS_ERR_CUDA;
+    }
+    cudaFree(d_start);
+    cudaFree(d_cols);
+    cudaFree(d_w);
+    return rc;
 }
 
 int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st) {

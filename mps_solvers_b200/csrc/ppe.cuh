@@ -107,6 +107,10 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
 int ppe_enqueue_cn(PpeWork& w, const StageArgs& a, const mps_options& opt, int c, double n0, double lambda,
                    uint32_t cap, cudaStream_t st);
 void ppe_free(PpeWork& w);
+// the stored off-diagonal entries of the last assembly as per-row lists in
+// particle order (host arrays; cols/wts may be NULL to size them first)
+int ppe_export_stencil(const PpeWork& w, uint32_t np, uint32_t* row_start, uint32_t* cols, float* wts,
+                       uint64_t max_entries, uint64_t* nnz, cudaStream_t st);
 // the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
 // either way); MPS_ERR_INVALID when the device cannot hold that shape
 int ppe_set_threads(PpeWork& w, int threads);

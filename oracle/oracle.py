@@ -29,6 +29,19 @@ PHASE = dict(update_dt=0, visc=1, divide_cell=2, collision=3, cal_n=4, pres_expl
 _lib = None
 
 
+def reference_dir() -> Optional[str]:
+    """The reference source tree that oracle/Makefile reads (its REF: the
+    environment variable MPS_REFERENCE_DIR, else the recipe's default), or
+    None when that directory is absent (as on a machine without the
+    reference, where only the committed fixtures are used)."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True, check=True)
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    path = r.stdout.strip().splitlines()[-1].strip() if r.stdout.strip() else ""
+    return path if path and os.path.isdir(path) else None
+
+
 def build(ref: Optional[str] = None, quiet: bool = True) -> None:
     """Build liboracle.so (and the reference binaries when the reference tree
     is present)."""

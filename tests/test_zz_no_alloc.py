@@ -67,6 +67,32 @@ def test_noalloc_matches_allocating_entry_point_twice(capi):
         assert int(b["nin"][0]) == int((key < g.ncells).sum())
 
 
+def test_noalloc_edges_of_its_fixed_regions(capi):
+    """The edges of the fixed scratch regions, each against the allocating
+    entry point bit for bit: no particles (only the cell table is written),
+    exactly MPS_NOALLOC_MAX_PARTICLES particles (every histogram tile in
+    use), and a grid of exactly MPS_NOALLOC_MAX_CELLS cells (the whole
+    cell-table region, and a third radix pass for the larger cell ids)."""
+    L = capi.lib()
+    cases = [
+        (_grid(capi), 0, 3),
+        (_grid(capi), capi.NOALLOC_MAX_PARTICLES, 4),
+        (_grid(capi, ncells_xyz=(128, 64, 64), cell=0.02), 200000, 5),
+    ]
+    assert cases[2][0].ncells == capi.NOALLOC_MAX_CELLS
+    for g, n, seed in cases:
+        ext = (g.cdx * g.cell_size, g.cdy * g.cell_size, g.cdz * g.cell_size)
+        pos = _positions(n, seed, ext)
+        st_a, a = _run(capi, L.mps_cell_sort_dev, pos, g)
+        st_b, b = _run(capi, L.mps_cell_sort_dev_noalloc, pos, g)
+        assert st_a == 0 and st_b == 0, (n, st_a, st_b)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (n, g.ncells, k)
+        assert int(b["nin"][0]) == int((b["cell"].astype(np.int64) < g.ncells).sum())
+        if n == 0:
+            assert not b["start"].any() and not b["end"].any()
+
+
 def test_noalloc_rejects_sizes_beyond_its_limits(capi):
     L = capi.lib()
     g = _grid(capi)
