@@ -106,7 +106,16 @@ typedef struct {
                             particles can move (fluid and moving walls), else
                             a full radix sort; -1 = always the full sort.  Both
                             give the same stable order.                       */
-    uint32_t reserved[3];
+    int ppe_layout;      /* PPE matrix in the solver: 0 = compact (rows
+                            numbered densely, 16-bit column codes, 6 bytes
+                            per entry) for single scenes with diagonal
+                            scaling, else the 8-byte layout; -1 = always the
+                            8-byte layout.  Same matrix either way;
+                            mps_autotune may change it.                       */
+    int ppe_smem_chunks; /* compact layout: 128-entry chunks of the matrix
+                            each warp keeps in shared memory across CG
+                            iterations (0: 8; -1: none; at most 8)           */
+    uint32_t reserved[1];
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after
@@ -193,7 +202,9 @@ mps_status mps_get_grid(mps_handle* h, mps_grid* g);
 /* n0, lambda, dt, time, c_lap = 2d/(n0 lambda), rho c^2, alpha, cg iterations,
  * cg relative residual, step, status, number of cells, kernels launched by
  * one step, FP64 residual passes of the last PPE solve, 1 when steps replay
- * a captured CUDA graph (0: direct launches), and 1 spare slot. */
+ * a captured CUDA graph (0: direct launches), and the matrix entries of the
+ * last PPE assembly whose column did not fit the compact layout's 16-bit
+ * code (-1 when the solver uses the 8-byte layout). */
 mps_status mps_get_scalars(mps_handle* h, double out16[16]);
 /* i_normal as GEO.dat indices: for each particle (by GEO index) the GEO index
  * of its wall particle (itself when it has none), np0 entries. */
@@ -414,9 +425,9 @@ mps_status mps_surface_case_table(uint8_t ntri[256], int8_t tri[256 * 16]);
  * PPE, the persistent grid's shape (1024, 512 or 256 threads per block at
  * 1024 threads per SM) and the solver's form (weights stored by the
  * assembly, weights recomputed from the positions in every product, or
- * stored weights with the pipelined single-reduction PCG), and keeps the
- * fastest of each.  The scene advances by the steps taken (call it during
- * warm-up). */
+ * stored weights with the pipelined single-reduction PCG, or the compact
+ * 16-bit layout of options.ppe_layout), and keeps the fastest of each.
+ * The scene advances by the steps taken (call it during warm-up). */
 typedef struct mps_tune_report {
     int stage_threads;         /* chosen */
     int ppe_threads;           /* chosen */
@@ -426,7 +437,9 @@ typedef struct mps_tune_report {
     /* PPE solve ms per step: [3 f + t] for form f (0 stored, 1 recomputed,
      * 2 pipelined) at 1024, 512, 256 threads per block (-1: not run) */
     float ppe_ms[9];
-    uint32_t reserved[4];
+    int ppe_compact;           /* chosen: 1 the compact 16-bit layout        */
+    float ppe_compact_ms[3];   /* its PPE solve ms per step at 1024, 512, 256
+                                  threads per block (-1: not run)            */
 } mps_tune_report;
 mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* report);
 

@@ -29,7 +29,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-co
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fno-fast-math",
             "-I/usr/local/cuda/include"]
 
-CU = ["cellsort.cu", "physics.cu", "ppe.cu", "learned.cu", "surface.cu", "capi.cu", "noalloc.cu"]
+CU = ["cellsort.cu", "physics.cu", "ppe.cu", "ppe_compact.cu", "learned.cu", "surface.cu", "capi.cu", "noalloc.cu"]
 CPP = ["host_io.cpp"]
 
 

@@ -51,7 +51,8 @@ class mps_options(C.Structure):
                 ("use_graph", C.c_int), ("cg_tol", C.c_double), ("cg_max_iter", C.c_int),
                 ("cg_check_every", C.c_int), ("precond", C.c_int), ("capacity", C.c_uint32),
                 ("cg_inner_digits", C.c_int), ("ppe_pipelined", C.c_int), ("ppe_l2_keep_mb", C.c_int),
-                ("visc_implicit", C.c_int), ("rebuild_merge", C.c_int), ("reserved", C.c_uint32 * 3)]
+                ("visc_implicit", C.c_int), ("rebuild_merge", C.c_int), ("ppe_layout", C.c_int),
+                ("ppe_smem_chunks", C.c_int), ("reserved", C.c_uint32 * 1)]
 
 
 class mps_params(C.Structure):
@@ -88,7 +89,7 @@ class mps_scene_info(C.Structure):
 class mps_tune_report(C.Structure):
     _fields_ = [("stage_threads", C.c_int), ("ppe_threads", C.c_int), ("ppe_stored_weights", C.c_int),
                 ("ppe_pipelined", C.c_int), ("stage_ms", C.c_float * 3), ("ppe_ms", C.c_float * 9),
-                ("reserved", C.c_uint32 * 4)]
+                ("ppe_compact", C.c_int), ("ppe_compact_ms", C.c_float * 3)]
 
 
 class mps_surface_grid(C.Structure):
@@ -362,7 +363,8 @@ class Simulation:
         o = (C.c_double * 16)()
         self._check(lib().mps_get_scalars(self.h, o))
         names = ("nzero", "lambda", "dt", "time", "c_lap", "one_over_alpha", "alpha", "cg_iters",
-                 "cg_relres", "step", "status", "ncells", "launches_per_step", "cg_outer", "graph")
+                 "cg_relres", "step", "status", "ncells", "launches_per_step", "cg_outer", "graph",
+                 "ppe_escaped")
         return dict(zip(names, list(o)))
 
     def normal_ids(self) -> np.ndarray:
@@ -467,7 +469,8 @@ class Simulation:
         self._check(lib().mps_autotune(self.h, steps, C.byref(r)))
         return {"stage_threads": r.stage_threads, "ppe_threads": r.ppe_threads,
                 "ppe_stored_weights": r.ppe_stored_weights, "ppe_pipelined": r.ppe_pipelined,
-                "stage_ms": list(r.stage_ms), "ppe_ms": list(r.ppe_ms)}
+                "stage_ms": list(r.stage_ms), "ppe_ms": list(r.ppe_ms), "ppe_compact": r.ppe_compact,
+                "ppe_compact_ms": list(r.ppe_compact_ms)}
 
     # ---- free surface (marching cubes)
     def surface_setup(self, shape, origin, spacing, max_triangles: int):

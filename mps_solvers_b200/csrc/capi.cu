@@ -555,6 +555,16 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
             e = ppe_enable_learned(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
         }
+        if (h->opt.ppe_layout != 0 && h->opt.ppe_layout != -1) {
+            h->err = "ppe_layout is 0 (compact where it applies) or -1 (8-byte layout)";
+            return MPS_ERR_INVALID;
+        }
+        h->ppe.c16_smem_chunks = h->opt.ppe_smem_chunks == 0 ? 8 : (h->opt.ppe_smem_chunks < 0 ? 0 : h->opt.ppe_smem_chunks);
+        if (h->opt.ppe_layout == 0 && h->opt.precond == MPS_PRECOND_DIAGONAL && !h->nscenes) {
+            e = ppe_c16_enable(h->ppe, &h->err);
+            if (e != MPS_OK) return (mps_status)e;
+            h->ppe.c16 = true;
+        }
         if (h->opt.visc_implicit) {
             e = ppe_setup(h->cn, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
             if (e != MPS_OK) return (mps_status)e;
@@ -1293,6 +1303,13 @@ extern "C" mps_status mps_get_scalars(mps_handle* h, double* o) {
     o[12] = h->launches;
     o[13] = s.cg_outer;
     o[14] = (h->opt.use_graph && !h->graph_off) ? 1.0 : 0.0;
+    o[15] = -1.0;
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT && h->ppe.c16) {
+        uint32_t esc = 0;
+        CK(cudaMemcpyAsync(&esc, h->ppe.c16_esc, sizeof esc, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        o[15] = esc;
+    }
     return MPS_OK;
 }
 
@@ -1549,17 +1566,26 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
         const int ppe_cand[3] = {1024, 512, 256};
         const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
         const int nforms = (learned || h->nscenes) ? 2 : 3;
+        // form 3: the compact layout (single scenes, diagonal scaling)
+        const bool compact_ok = h->ppe.c16_ready && !learned && !h->nscenes;
         best = 1e300;
         int best_p = h->ppe.threads;
-        bool best_sw = h->ppe.stored_weights, best_pipe = h->ppe.pipelined;
-        for (int c = 0; c < 3 * nforms; c++) {
+        bool best_sw = h->ppe.stored_weights, best_pipe = h->ppe.pipelined, best_c16 = h->ppe.c16;
+        for (int k = 0; k < 3; k++) r.ppe_compact_ms[k] = -1.f;
+        for (int c = 0; c < 12; c++) {
             const int form = c / 3;
+            if (form >= nforms && form != 3) {
+                r.ppe_ms[c] = -1.f;
+                continue;
+            }
+            if (form == 3 && !compact_ok) continue;
             if (ppe_set_threads(h->ppe, ppe_cand[c % 3]) != MPS_OK) {
-                r.ppe_ms[c] = -1.f;  // the device cannot hold this shape
+                if (form < 3) r.ppe_ms[c] = -1.f;  // the device cannot hold this shape
                 continue;
             }
             h->ppe.stored_weights = form != 1;
             h->ppe.pipelined = form == 2;
+            h->ppe.c16 = form == 3;
             drop_graphs(h);
             double tot = 0.0;
             for (int k = 0; k < steps; k++) {
@@ -1568,21 +1594,24 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
                 tot += ms[ST_PPE_SOLVE];
             }
             const double t = tot / steps;
-            r.ppe_ms[c] = (float)t;
+            if (form < 3) r.ppe_ms[c] = (float)t;
+            else r.ppe_compact_ms[c % 3] = (float)t;
             if (t < best) {
                 best = t;
                 best_p = ppe_cand[c % 3];
                 best_sw = form != 1;
                 best_pipe = form == 2;
+                best_c16 = form == 3;
             }
         }
-        for (int c = 3 * nforms; c < 9; c++) r.ppe_ms[c] = -1.f;
         ppe_set_threads(h->ppe, best_p);
         h->ppe.stored_weights = best_sw;
         h->ppe.pipelined = best_pipe;
+        h->ppe.c16 = best_c16;
         r.ppe_threads = best_p;
         r.ppe_stored_weights = best_sw ? 1 : 0;
         r.ppe_pipelined = best_pipe ? 1 : 0;
+        r.ppe_compact = best_c16 ? 1 : 0;
     }
     drop_graphs(h);
     if (rep) *rep = r;

@@ -21,111 +21,11 @@
 
 #include "cellsort.cuh"
 #include "ppe.cuh"
+#include "ppe_device.cuh"
 
 namespace mpsb {
 
 static inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
-
-// ---------------------------------------------------------------- helpers
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;  // every lane's value is used only from lane 0
-}
-__device__ __forceinline__ float warp_sum_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Grid-wide sum of K doubles fused with a grid barrier.  bar[0] counts
-// arrivals and only grows during a launch (the assembly kernel empties it
-// before every solve), so the e-th barrier of a launch completes when it
-// reaches (e + 1) * gridDim.x and a block learns e from the count it saw
-// before arriving.  Each block writes its fixed-order block sum into slot
-// [e & 1][block] (two buffers: a block can write the slot of barrier e + 1
-// only after every block has finished reading those of barrier e), arrives,
-// waits for the count, and then adds all the slots itself in block order
-// (lane-strided, then a fixed shuffle tree): the totals are identical in
-// every block and on every run, and no block waits for another to publish
-// them.  The wait is bounded: after 1 s (global timer) it sets
-// ERR_DEVICE_TIMEOUT and returns false.
-template <int K>
-__device__ bool grid_reduce(const double (&v)[K], double* part, double* /*result*/, unsigned* bar, Scalars* sc,
-                            double (&out)[K]) {
-    __shared__ double sm[K][32];
-    __shared__ double tot_s[K];
-    __shared__ unsigned ep_s;
-    __shared__ int ok_s;
-    const unsigned G = gridDim.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    unsigned seen = 0;
-    if (threadIdx.x == 0)  // the barrier's index, loaded early so the block sum hides the latency
-        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(bar) : "memory");
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const double t = warp_sum_d(v[k]);
-        if (lane == 0) sm[k][warp] = t;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        double t[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) t[k] = warp_sum_d(lane < nw ? sm[k][lane] : 0.0);
-        if (lane == 0) {
-            const unsigned e = seen / G;
-            double* slot = part + ((size_t)(e & 1u) * G + blockIdx.x) * PPE_PARTS;
-#pragma unroll
-            for (int k = 0; k < K; k++) slot[k] = t[k];
-            __threadfence();  // this block's writes (slot and vectors) before the arrival
-            atomicAdd(bar, 1u);
-            const unsigned target = (e + 1) * G;
-            int ok = 1;
-            unsigned cur;
-            uint64_t t0;
-            const unsigned long long budget = wait_budget_ns(sc);
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-            for (;;) {
-                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
-                if ((int)(cur - target) >= 0) break;
-                uint64_t t1;
-                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-                if (t1 - t0 > budget) {
-                    atomicOr(&sc->err, ERR_DEVICE_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-            __threadfence();
-            ep_s = e;
-            ok_s = ok;
-        }
-    }
-    __syncthreads();
-    if (warp == 0) {
-        const double* buf = part + (size_t)(ep_s & 1u) * G * PPE_PARTS;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            // up to 8 partials per lane loaded before adding (latency)
-            double v8[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const unsigned b = lane + 32u * u;
-                v8[u] = b < G ? __ldcg(buf + b * PPE_PARTS + k) : 0.0;
-            }
-            double t = 0.0;
-#pragma unroll
-            for (int u = 0; u < 8; u++) t += v8[u];
-            for (unsigned b = lane + 256u; b < G; b += 32) t += __ldcg(buf + b * PPE_PARTS + k);
-            t = warp_sum_d(t);
-            if (lane == 0) tot_s[k] = t;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; k++) out[k] = tot_s[k];
-    return ok_s != 0;
-}
 
 // ---------------------------------------------------------------- assembly
 struct AsmArgs {
@@ -291,41 +191,6 @@ __device__ __forceinline__ float stencil_weight(const SolveArgs& S, const float4
     const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
     const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
     return (j != i && rr < S.rlap_thr) ? weight_rr<EX>(S.rlap, rr) : 0.f;
-}
-
-// L2 residency of the stored matrix.  Every CG iteration streams the whole
-// matrix in the same order; once it is larger than L2 a plain LRU keeps none
-// of it from one iteration to the next.  The entries before `keep` (the
-// leading slices) are read as evict_last and the rest as evict_first, so the
-// streamed tail displaces itself and the head stays in L2.  The matrix is
-// read once per product, so it bypasses L1 (which keeps the gathered
-// neighbour vectors instead).  keep = 0xFFFFFFFF reads everything with the
-// default policy.
-__device__ __forceinline__ uint64_t mat_policy(uint32_t base, uint32_t keep) {
-    uint64_t p;
-    if (keep == 0xFFFFFFFFu)
-        asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
-    else if (base < keep)
-        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    else
-        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-
-__device__ __forceinline__ uint4 ld_mat(const uint4* p, uint64_t pol) {
-    uint4 v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-        : "l"(p), "l"(pol));
-    return v;
-}
-
-__device__ __forceinline__ float4 ld_mat(const float4* p, uint64_t pol) {
-    float4 v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-        : "l"(p), "l"(pol));
-    return v;
 }
 
 // The weights of one lane's 4 entries: stored, or recomputed from positions.
@@ -1621,6 +1486,7 @@ static int enqueue_rows_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaS
                                                           cap);
         launched++;
     }
+    if (w.c16 && !a.batch.n) return launched + ppe_c16_enqueue_pack(w, a, cap, st);
     // SELL-8 layout of the non-Dirichlet rows
     const uint32_t maxslices = (cap + SELL_C - 1) / SELL_C;
     k_sell_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off, maxslices);
@@ -1689,7 +1555,9 @@ int ppe_export_stencil(const PpeWork& w, uint32_t np, uint32_t* row_start, uint3
     } else {
         cudaMemcpyAsync(d_start, start.data(), (size_t)(np + 1) * 4, cudaMemcpyHostToDevice, st);
         const uint32_t maxslices = (np + SELL_C - 1) / SELL_C;
-        if (maxslices)
+        if (w.c16)
+            ppe_c16_export(w, np, d_start, d_cols, d_w, st);
+        else if (maxslices)
             k_sell_export<<<blocks_for(maxslices * 32u, 256), 256, 0, st>>>(w.rlen, w.rowlist, w.nrows, w.sell_off,
                                                                             w.sell_cols, w.sell_w, d_start, d_cols, d_w);
         if (cols) cudaMemcpyAsync(cols, d_cols, t * 4, cudaMemcpyDeviceToHost, st);
@@ -1876,6 +1744,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         return 2;
     }
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+    if (w.c16 && !learned) return ppe_c16_enqueue_solve(w, a, opt, cap, st);
     if (w.pipelined && !learned) {
         PipeArgs Pa;
         Pa.rowlist = w.rowlist;
@@ -2130,6 +1999,7 @@ void ppe_free(PpeWork& w) {
                   w.id_snap, w.pu, w.pw, w.pz, w.pq, w.ps, w.pp, w.pm[0], w.pm[1], w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
                   w.scene_relres};
     lp_free(w.lp);
+    ppe_c16_free(w);
     for (void* p : ps)
         if (p) cudaFree(p);
     w = PpeWork();

@@ -87,6 +87,22 @@ struct PpeWork {
     int* scene_iters = nullptr;
     int* scene_outer = nullptr;
     double* scene_relres = nullptr;
+    // compact layout (ppe_compact.cu): rows numbered 0..R-1 in row-list
+    // order, slices of 4 rows with 8 lanes per row, 16-bit column codes
+    // relative to the slice, FP32 weights; single scenes, diagonal scaling
+    bool c16 = false;                  // the solve uses this layout
+    bool c16_ready = false;            // its buffers exist
+    int c16_smem_chunks = 8;           // chunks per warp held in shared memory across iterations
+    size_t c16_cap_chunks = 0;
+    uint32_t* cpos = nullptr;          // compact row of each particle (rows only)
+    uint32_t* c16_width = nullptr;     // chunks per slice, then (scanned) the slices' first chunk
+    uint16_t* c16_codes = nullptr;     // 128 codes per chunk (column - 4 * slice + 32768; 65535: escaped)
+    float* c16_w = nullptr;            // 128 weights per chunk
+    uint32_t* c16_side = nullptr;      // compact column of an escaped entry (same layout)
+    uint32_t* c16_esc = nullptr;       // escaped entries of the last pack
+    double *cb64 = nullptr, *cx64 = nullptr, *cdiag64 = nullptr;
+    float *cdiag32 = nullptr, *cinv_diag = nullptr, *cr = nullptr, *cq = nullptr;
+    float2* czp[2] = {nullptr, nullptr};
 };
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
@@ -111,6 +127,15 @@ void ppe_free(PpeWork& w);
 // particle order (host arrays; cols/wts may be NULL to size them first)
 int ppe_export_stencil(const PpeWork& w, uint32_t np, uint32_t* row_start, uint32_t* cols, float* wts,
                        uint64_t max_entries, uint64_t* nnz, cudaStream_t st);
+// The compact 16-bit layout and its persistent solver (ppe_compact.cu):
+// buffers, the pack after the row list, the solve with p = max(x, 0), the
+// escaped-entry count of the last pack, and the stencil export.
+int ppe_c16_enable(PpeWork& w, std::string* err);
+int ppe_c16_enqueue_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st);
+int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, uint32_t cap, cudaStream_t st);
+int ppe_c16_export(const PpeWork& w, uint32_t np, const uint32_t* d_row_start, uint32_t* d_cols, float* d_w,
+                   cudaStream_t st);
+void ppe_c16_free(PpeWork& w);
 // the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
 // either way); MPS_ERR_INVALID when the device cannot hold that shape
 int ppe_set_threads(PpeWork& w, int threads);

@@ -168,3 +168,29 @@ def test_semi_fast_arith_vs_fp64_oracle(capi, oracle_mod, tmp_path):
             assert st.cg_relres <= 1e-8 and st.cg_iters > 0
         ex, eu, ep = compare(s.state(), orc.state())
     assert ex < X_TOL and eu < U_TOL and ep < P_TOL, (ex, eu, ep)
+
+
+def test_device_wait_timeout_is_reported_and_handle_survives(capi, tmp_path):
+    """A grid-wide wait limit of 1 ns makes the persistent PPE solver's
+    barriers give up before the other blocks arrive: every block returns, the
+    step reports MPS_ERR_DEVICE_TIMEOUT (6) instead of hanging or faulting,
+    the handle still answers its getters and is destroyed cleanly, and a new
+    handle on the same device solves normally."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    s = capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT)
+    assert s.step(2).status == 0
+    s.set_device_wait_limit(1)
+    st = s.step(1, check=False)
+    assert st.status == 6
+    with pytest.raises(capi.MPSError):
+        s.step(1)
+    c = s.counts()
+    assert c["np"] > 0
+    a = s.state()
+    assert len(a["id"]) == c["np"]
+    s.set_device_wait_limit(0)
+    s.close()
+    with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT) as s2:
+        st = s2.step(3)
+        assert st.status == 0 and st.cg_relres <= 1e-8
