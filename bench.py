@@ -161,33 +161,37 @@ def workload_name(workload: str) -> str:
             "PPE diagonally scaled CG to 1e-8 relative residual, dt=5e-4 s")
 
 
-def cpu_baseline(workload: str, case_dir: str, n_particles: int, sample_steps: int):
-    """Reference CPU step on the host cores (oracle/_ref); bounded sample."""
+def cpu_baseline(workload: str, case_dir: str, n_particles: int, warm: int, sample_steps: int):
+    """Reference CPU step on the host cores: the first `warm` steps of the
+    scene run untimed, then `sample_steps` consecutive steps are timed, so the
+    timed window is the one the GPU arm times (its steps warm+1 ..)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
+    window = f"steps {warm + 1}-{warm + sample_steps} of one run from the initial state"
     if workload == "explicit" and oracle.have_reference_build():
         out = os.path.join(case_dir, "ref_bench.bin")
-        info = oracle.run_reference("expl", case_dir, sample_steps, 0, out, threads=threads,
-                                    timeout=1800)
+        info = oracle.run_reference("expl", case_dir, warm + sample_steps, 0, out, threads=threads,
+                                    timeout=1800, untimed=warm)
         os.unlink(out)
         v = n_particles * sample_steps / info["steps_s"]
         return {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                "sample": f"{sample_steps} steps of the same scene, MPS_CAL_expl_v1.0 CPU path "
-                          f"(GPU_CUDA off) built from the reference sources, {threads} OpenMP "
-                          f"threads, step() only",
-                "cpu": _cpu_model()}
+                "sample": f"{window}, MPS_CAL_expl_v1.0 CPU path (GPU_CUDA off) built from the "
+                          f"reference sources, {threads} OpenMP threads, step() only",
+                "window": [warm + 1, warm + sample_steps], "cpu": _cpu_model()}
     # semi-implicit: the oracle's sparse restatement of the reference rules
     orc = oracle.Oracle(case_dir, oracle.SEMI_JACOBI, 64)
     orc.set_cg(True, 1e-8, 100000)
+    if warm:
+        orc.step(warm)
     t0 = time.perf_counter()
     orc.step(sample_steps)
     dt = time.perf_counter() - t0
     return {"value": n_particles * sample_steps / dt, "unit": "particle-steps/s", "cores": threads,
             "kind": "port",
-            "sample": f"{sample_steps} steps, sparse FP64 restatement of MPS_CAL_v4.0 "
-                      f"MPS_CPU_EXPL (the dense reference cannot hold this size), {threads} threads",
-            "cpu": _cpu_model()}
+            "sample": f"{window}, sparse FP64 restatement of MPS_CAL_v4.0 MPS_CPU_EXPL (the dense "
+                      f"reference cannot hold this size), {threads} threads",
+            "window": [warm + 1, warm + sample_steps], "cpu": _cpu_model()}
 
 
 def _cpu_model():
@@ -225,15 +229,16 @@ def run_reference_arm(args, rank: int, world: int):
         else:
             pos, nb2, nb1 = scene.write_case(d, make_scene(args.workload, 0))
         n = len(pos)
-        # each "step" of this arm is the bounded CPU sample
-        sample = args.ref_sample if args.ref_sample else (100 if args.workload == "explicit" else 1)
-        vals = []
-        cb = None
-        for _ in range(max(1, args.steps)):
-            cb = cpu_baseline(args.workload, d, n, sample)
-            vals.append(cb["value"])
-    v = float(np.mean(vals))
-    cb["value"] = v
+        # the GPU arm's window: `warmup` untimed steps from the initial state,
+        # then `steps` timed consecutive steps (the large scene: at most 3 of
+        # them, ~8 s each on the host)
+        k = max(1, args.steps)
+        if args.workload == "large":
+            k = min(k, 3)
+        if args.ref_sample:
+            k = args.ref_sample
+        cb = cpu_baseline(args.workload, d, n, args.warmup, k)
+    v = float(cb["value"])
     line = {
         "impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -260,23 +265,46 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tmpd = tempfile.mkdtemp(prefix=f"mpsb_{rank}_")
     precond = capi.PRECOND_LEARNED if args.precond == "learned" else capi.PRECOND_DIAGONAL
     batch_counts = None
+
+    def make_sim():
+        if args.workload == "batch":
+            return capi.Simulation.batch(dirs, accel=accel, method=method, arith=arith, device=local_rank,
+                                         use_graph=1, precond=precond)
+        return capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
+                               precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+
+    def load_learned(s):
+        from mps_solvers_b200 import precond_weights
+        s.set_precond_params(precond_weights.load())
+
     if args.workload == "batch":
         dirs, accel, batch_counts = write_batch(tmpd, rank)
         n = int(sum(batch_counts))
-        sim = capi.Simulation.batch(dirs, accel=accel, method=method, arith=arith, device=local_rank,
-                                    use_graph=1, precond=precond)
-        nb2 = sum(sim.scene_info(s).nb2 for s in range(len(dirs)))
-        nb1 = sum(sim.scene_info(s).nb1 for s in range(len(dirs)))
     else:
         pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
         n = len(pos0)
-        sim = capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
-                              precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+    learned = method == capi.METHOD_SEMI_IMPLICIT and precond == capi.PRECOND_LEARNED
+    # launch shapes picked by the library's autotuner on a scratch handle of
+    # the same scene, so that the timed handle's steps start from the initial
+    # state: warm-up steps 1..W, timed steps W+1..W+K
+    tune = None
+    if not args.no_autotune:
+        with make_sim() as scratch:
+            if learned:
+                load_learned(scratch)
+            tune = scratch.autotune(2)
+    sim = make_sim()
+    if args.workload == "batch":
+        nb2 = sum(sim.scene_info(s).nb2 for s in range(len(dirs)))
+        nb1 = sum(sim.scene_info(s).nb1 for s in range(len(dirs)))
+    if tune is not None:
+        sim.apply_tuning(tune)
     tc_diff = None
-    if method == capi.METHOD_SEMI_IMPLICIT and precond == capi.PRECOND_LEARNED:
-        from mps_solvers_b200 import precond_weights
-        sim.set_precond_params(precond_weights.load())
+    extra_warm = 0
+    if learned:
+        load_learned(sim)
         sim.step(1)  # a PPE system for the tensor-core check
+        extra_warm = 1
         tc_diff = sim.precond_tensor_cores(True)
     stream = torch.cuda.ExternalStream(sim.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -287,12 +315,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         origin, spacing = scene.surface_grid(sc_large, SURFACE_SHAPE)
         sim.surface_setup(SURFACE_SHAPE, origin, spacing, 8 << 20)
         surface = {"grid": list(SURFACE_SHAPE), "every": SURFACE_EVERY}
-    # launch shapes picked by the library's autotuner on this scene, then
     # warm-up (also captures the step graphs)
-    tune = sim.autotune(2) if not args.no_autotune else None
-    for _ in range(args.warmup):
+    for _ in range(args.warmup - extra_warm):
         sim.step_async(1)
     sim.step(0)
+    first_timed = args.warmup + 1
 
     if world > 1:
         import torch.distributed as dist
@@ -421,6 +448,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "stage_ms_per_step": {k: v / prof_steps for k, v in prof.items()},
         "e2e": {"value": e2e_v, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
+        "timed_steps": [first_timed, first_timed + args.steps - 1],
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
         "autotune": tune,
@@ -521,6 +549,9 @@ def main():
                     help="skip the diagonal-vs-learned PPE comparison (semi-implicit)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (short launch lists for profiling)")
+    ap.add_argument("--no-sub-runs", action="store_true",
+                    help="skip the short runs of the explicit, batched and large workloads that the "
+                         "default semi-implicit run adds under 'workloads'")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -555,16 +586,61 @@ def main():
             else:
                 sc = make_scene(args.workload, 0)
             pos, _, _ = scene.write_case(d, sc)
-            sample = 300 if args.workload == "explicit" else (1 if args.workload == "large" else 2)
-            line["cpu_baseline"] = cpu_baseline(args.workload, d, len(pos), sample)
+            # the GPU arm's first timed steps (all of them for the explicit
+            # scene, at most 20 for the semi-implicit ones, 2 for the large)
+            k = args.steps if args.workload == "explicit" else min(args.steps, 2 if args.workload == "large" else 20)
+            line["cpu_baseline"] = cpu_baseline(args.workload, d, len(pos), args.warmup, k)
             if args.workload == "batch":
                 line["cpu_baseline"]["sample"] += " (the batch's smallest scene)"
+    if line is not None and world == 1 and args.workload == "semi" and args.size == "full" and not args.no_sub_runs:
+        line["workloads"] = sub_runs(args, local_rank)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     if line is not None:
         print(json.dumps(line), flush=True)
+
+
+# The other configurations, measured briefly in the default run: (steps,
+# warm-up, CPU-baseline steps) each; the CPU baseline times the first of the
+# GPU arm's timed steps on the same scene.
+SUB_RUNS = (("explicit", 200, 10, 200), ("batch", 10, 3, 10), ("large", 20, 3, 1))
+SUB_KEYS = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "timed_steps", "dtype", "config",
+            "roofline", "roofline_fp32", "value_fluid_only", "stage_ms_per_step", "e2e", "gpu_launches",
+            "clocks", "autotune", "surface", "batch", "final")
+
+
+def sub_runs(args, local_rank: int):
+    """Short runs of the explicit, batched and large workloads (single GPU),
+    each with its own timing, roofline, e2e and windowed CPU baseline."""
+    import copy
+    from mps_solvers_b200 import scene
+    out = {}
+    for wl, steps, warm, cpu_steps in SUB_RUNS:
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup = wl, steps, warm
+        a.arith = "exact" if wl == "explicit" else "fast"
+        a.no_ppe_compare = True
+        a.precond = "diagonal"
+        try:
+            sub = run_ours(a, 0, 1, local_rank)
+            res = {k: sub.get(k) for k in SUB_KEYS}
+            if not args.no_cpu_baseline:
+                with tempfile.TemporaryDirectory() as d:
+                    if wl == "batch":
+                        sc = min(scene.batch_scenes(64, 0), key=lambda t: len(scene.build(t[0])[0]))[0]
+                    else:
+                        sc = make_scene(wl, 0)
+                    pos, _, _ = scene.write_case(d, sc)
+                    cb = cpu_baseline(wl, d, len(pos), warm, cpu_steps)
+                    if wl == "batch":
+                        cb["sample"] += " (the batch's smallest scene)"
+                    res["cpu_baseline"] = cb
+        except Exception as e:  # one workload failing must not lose the others
+            res = {"error": f"{type(e).__name__}: {e}"}
+        out[wl] = res
+    return out
 
 
 if __name__ == "__main__":

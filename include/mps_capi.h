@@ -442,6 +442,10 @@ typedef struct mps_tune_report {
                                   threads per block (-1: not run)            */
 } mps_tune_report;
 mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* report);
+/* Apply the choices of a report (the chosen fields: stage_threads,
+ * ppe_threads, ppe_stored_weights, ppe_pipelined, ppe_compact) to a handle,
+ * e.g. one tuned on a scratch handle of the same scene, without stepping. */
+mps_status mps_apply_tuning(mps_handle* h, const mps_tune_report* report);
 
 #ifdef __cplusplus
 }

@@ -43,7 +43,7 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
            "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
            "mps_surface_case_table", "mps_precond_tensor_cores", "mps_add_wall_motion",
-           "mps_clear_wall_motion", "mps_set_device_wait_limit", "mps_ppe_stencil")
+           "mps_clear_wall_motion", "mps_set_device_wait_limit", "mps_ppe_stencil", "mps_apply_tuning")
 
 
 class mps_options(C.Structure):
@@ -165,6 +165,7 @@ def lib():
             "mps_set_device_wait_limit": (C.c_int, [H, C.c_uint64]),
             "mps_ppe_stencil": (C.c_int, [H, U, U, Fp, C.c_uint64, C.POINTER(C.c_uint64)]),
             "mps_autotune": (C.c_int, [H, C.c_int, C.POINTER(mps_tune_report)]),
+            "mps_apply_tuning": (C.c_int, [H, C.POINTER(mps_tune_report)]),
             "mps_surface_setup": (C.c_int, [H, C.POINTER(mps_surface_grid), C.c_uint32]),
             "mps_surface_extract_async": (C.c_int, [H]),
             "mps_surface_extract": (C.c_int, [H, U]),
@@ -471,6 +472,14 @@ class Simulation:
                 "ppe_stored_weights": r.ppe_stored_weights, "ppe_pipelined": r.ppe_pipelined,
                 "stage_ms": list(r.stage_ms), "ppe_ms": list(r.ppe_ms), "ppe_compact": r.ppe_compact,
                 "ppe_compact_ms": list(r.ppe_compact_ms)}
+
+    def apply_tuning(self, tune: Dict[str, object]):
+        """Apply an autotune() result (from this or another handle of the same
+        scene) without stepping."""
+        r = mps_tune_report()
+        for k in ("stage_threads", "ppe_threads", "ppe_stored_weights", "ppe_pipelined", "ppe_compact"):
+            setattr(r, k, int(tune[k]))
+        self._check(lib().mps_apply_tuning(self.h, C.byref(r)))
 
     # ---- free surface (marching cubes)
     def surface_setup(self, shape, origin, spacing, max_triangles: int):

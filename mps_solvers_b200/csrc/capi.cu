@@ -1618,6 +1618,38 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
     return MPS_OK;
 }
 
+extern "C" mps_status mps_apply_tuning(mps_handle* h, const mps_tune_report* r) {
+    if (!h || !r) return MPS_ERR_INVALID;
+    if (r->stage_threads != 64 && r->stage_threads != 128 && r->stage_threads != 256) return MPS_ERR_INVALID;
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->stream));
+    h->stage_threads = r->stage_threads;
+    if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
+        const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
+        if (r->ppe_compact) {
+            if (learned || h->nscenes) {
+                h->err = "the compact PPE layout is for single scenes with diagonal scaling";
+                return MPS_ERR_INVALID;
+            }
+            const int e = ppe_c16_enable(h->ppe, &h->err);
+            if (e != MPS_OK) return (mps_status)e;
+        }
+        if (r->ppe_pipelined && (learned || h->nscenes)) {
+            h->err = "the pipelined PCG is for single scenes with diagonal scaling";
+            return MPS_ERR_INVALID;
+        }
+        if (ppe_set_threads(h->ppe, r->ppe_threads) != MPS_OK) {
+            h->err = "the device cannot hold that PPE block size";
+            return MPS_ERR_INVALID;
+        }
+        h->ppe.stored_weights = r->ppe_stored_weights != 0;
+        h->ppe.pipelined = r->ppe_pipelined != 0;
+        h->ppe.c16 = r->ppe_compact != 0;
+    }
+    drop_graphs(h);
+    return MPS_OK;
+}
+
 // ---------------------------------------------------------------- free surface
 extern "C" mps_status mps_surface_case_table(uint8_t* ntri, int8_t* tri) {
     if (!ntri || !tri) return MPS_ERR_INVALID;

@@ -216,10 +216,11 @@ def have_reference_build() -> bool:
 
 
 def run_reference(kind: str, case_dir: str, nsteps: int, dump_every: int, out_path: str,
-                  threads: int = 1, timeout: float = 600.0) -> dict:
-    """Run oracle/_ref/ref_{expl,semi} on case_dir; returns its timing JSON."""
+                  threads: int = 1, timeout: float = 600.0, untimed: int = 0) -> dict:
+    """Run oracle/_ref/ref_{expl,semi} on case_dir; returns its timing JSON
+    (steps_s covers the steps after the first `untimed` ones)."""
     exe = os.path.join(REF_DIR, f"ref_{kind}")
-    r = subprocess.run([exe, case_dir, str(nsteps), str(dump_every), out_path, str(threads)],
+    r = subprocess.run([exe, case_dir, str(nsteps), str(dump_every), out_path, str(threads), str(untimed)],
                        capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{exe} failed ({r.returncode}): {r.stderr[-2000:]}")

@@ -113,7 +113,7 @@ static double now_s() {
 
 int main(int argc, char** argv) {
     if (argc < 6) {
-        fprintf(stderr, "usage: %s workdir nsteps dump_every out.bin threads\n", argv[0]);
+        fprintf(stderr, "usage: %s workdir nsteps dump_every out.bin threads [untimed_first_steps]\n", argv[0]);
         return 2;
     }
     const char* workdir = argv[1];
@@ -121,6 +121,9 @@ int main(int argc, char** argv) {
     int dump_every = atoi(argv[3]);
     const char* out_path = argv[4];
     int threads = atoi(argv[5]);
+    // the first `skip` steps run untimed, so that the timed steps are a
+    // later window of the run (the one a GPU measurement times)
+    int skip = argc > 6 ? atoi(argv[6]) : 0;
 
     // Resolve the output path before changing directory.
     char out_abs[4096];
@@ -150,13 +153,13 @@ int main(int argc, char** argv) {
     for (int s = 1; s <= nsteps; s++) {
         double a = now_s();
         h->one_step();
-        t_steps += now_s() - a;
+        if (s > skip) t_steps += now_s() - a;
         if (dump_every > 0 && (s % dump_every == 0 || s == nsteps)) h->dump_state(f, (uint32_t)s);
     }
     fclose(f);
     fflush(stdout);
-    fprintf(stderr, "{\"init_s\": %.6f, \"steps\": %d, \"steps_s\": %.6f, \"threads\": %d}\n",
-            t_init, nsteps, t_steps, threads);
+    fprintf(stderr, "{\"init_s\": %.6f, \"steps\": %d, \"untimed_steps\": %d, \"steps_s\": %.6f, \"threads\": %d}\n",
+            t_init, nsteps, skip < nsteps ? skip : nsteps, t_steps, threads);
     h->finish();
     delete h;
     return 0;
