@@ -129,12 +129,12 @@ SURFACE_SHAPE = (256, 64, 128)   # vertices along x (length), y (depth), z (heig
 SURFACE_EVERY = 20
 
 
-def write_batch(d: str, seed: int):
-    """The batched workload's 64 scenes as case directories under d;
-    returns (dirs, accel, particles per scene)."""
+def write_batch(d: str, seed: int, nscenes: int = 64):
+    """The batched workload's scenes (the first nscenes of the 64) as case
+    directories under d; returns (dirs, accel, particles per scene)."""
     from mps_solvers_b200 import scene
     dirs, accel, counts = [], [], []
-    for k, (sc, amp, freq) in enumerate(scene.batch_scenes(64, seed)):
+    for k, (sc, amp, freq) in enumerate(scene.batch_scenes(nscenes, seed)):
         sd = os.path.join(d, f"scene{k:02d}")
         pos, _, _ = scene.write_case(sd, sc)
         dirs.append(sd)
@@ -271,14 +271,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             return capi.Simulation.batch(dirs, accel=accel, method=method, arith=arith, device=local_rank,
                                          use_graph=1, precond=precond)
         return capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
-                               precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL)
+                               precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL,
+                               visc_implicit=int(method == capi.METHOD_SEMI_IMPLICIT and args.visc == "implicit"))
 
     def load_learned(s):
         from mps_solvers_b200 import precond_weights
         s.set_precond_params(precond_weights.load())
 
     if args.workload == "batch":
-        dirs, accel, batch_counts = write_batch(tmpd, rank)
+        dirs, accel, batch_counts = write_batch(tmpd, rank, 8 if args.size == "small" else 64)
         n = int(sum(batch_counts))
     else:
         pos0, nb2, nb1 = scene.write_case(tmpd, make_scene(args.workload, rank, args.size))
@@ -311,7 +312,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     surface = None
     if args.workload == "large":
-        sc_large = make_scene("large", rank)
+        sc_large = make_scene("large", rank, args.size)
         origin, spacing = scene.surface_grid(sc_large, SURFACE_SHAPE)
         sim.surface_setup(SURFACE_SHAPE, origin, spacing, 8 << 20)
         surface = {"grid": list(SURFACE_SHAPE), "every": SURFACE_EVERY}
@@ -431,6 +432,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    f"{args.workload} small profiling tank", "particles": n,
                    "precond": args.precond if method == capi.METHOD_SEMI_IMPLICIT else None,
                    "fluid": int(n - nb2 - nb1), "arith": args.arith,
+                   "viscosity": ("Crank-Nicolson" if args.visc == "implicit" else "explicit")
+                   if method == capi.METHOD_SEMI_IMPLICIT else "explicit",
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
@@ -540,7 +543,11 @@ def main():
                     help="default: exact for the explicit workload (bit-identical to the "
                          "reference), fast for the semi-implicit one")
     ap.add_argument("--size", default="full", choices=["full", "small"],
-                    help="small: a ~110k-particle tank of the same kernels (profiling)")
+                    help="small (profiling): a ~110k-particle tank of the same kernels; with "
+                         "--workload batch the first 8 of the 64 scenes; with --workload large the "
+                         "small tank with the surface extraction")
+    ap.add_argument("--visc", default="explicit", choices=["explicit", "implicit"],
+                    help="semi-implicit viscosity: explicit (default) or Crank-Nicolson")
     ap.add_argument("--ref-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precond", default="diagonal", choices=["diagonal", "learned"],
@@ -557,8 +564,7 @@ def main():
         args.warmup = 3
     if args.arith is None:
         args.arith = "exact" if args.workload == "explicit" else "fast"
-    if args.workload == "batch" and args.size != "full":
-        ap.error("the batch workload has one size")
+
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
