@@ -115,7 +115,11 @@ typedef struct {
     int ppe_smem_chunks; /* compact layout: 128-entry chunks of the matrix
                             each warp keeps in shared memory across CG
                             iterations (0: 8; -1: none; at most 8)           */
-    uint32_t reserved[1];
+    int precond_every;   /* learned preconditioner on the compact layout: steps
+                            between two evaluations of the network; between
+                            them the symmetric form of the factor is kept by
+                            particle (GEO index) and re-packed for the current
+                            rows every step (0: 10; 1: every step)           */
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

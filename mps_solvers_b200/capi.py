@@ -52,7 +52,7 @@ class mps_options(C.Structure):
                 ("cg_check_every", C.c_int), ("precond", C.c_int), ("capacity", C.c_uint32),
                 ("cg_inner_digits", C.c_int), ("ppe_pipelined", C.c_int), ("ppe_l2_keep_mb", C.c_int),
                 ("visc_implicit", C.c_int), ("rebuild_merge", C.c_int), ("ppe_layout", C.c_int),
-                ("ppe_smem_chunks", C.c_int), ("reserved", C.c_uint32 * 1)]
+                ("ppe_smem_chunks", C.c_int), ("precond_every", C.c_int)]
 
 
 class mps_params(C.Structure):

@@ -56,7 +56,9 @@ struct mps_handle {
     PpeWork cn{};  // Crank-Nicolson viscosity system (options.visc_implicit)
     Staging stage{};
     // graphs, one per buffer parity
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // one graph per buffer parity, and for the learned compact preconditioner
+    // per kind of step (index parity + 2 when the step evaluates the network)
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
     int pending_apply = APPLY_NONE;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // per-stage profiling: events recorded between stages when enabled
@@ -181,6 +183,14 @@ static void mark(mps_handle* h, int tag) {
 // The merge rebuild (cellsort.cuh) when at most MERGE_SMEM_CAP particles can
 // change cell between two rebuilds (fluid and moving walls) and the current
 // order is a sorted one; else the full radix sort.  Both give the same order.
+// The compact PPE layout on or off; with the learned preconditioner it
+// carries the learned symmetric form (the factor form needs the 8-byte
+// layout).
+static void set_compact(mps_handle* h, bool on) {
+    h->ppe.c16 = on && h->ppe.c16_ready;
+    h->ppe.c16_learned = h->ppe.c16 && h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.sp_cols != nullptr;
+}
+
 static bool use_merge(const mps_handle* h) {
     return h->merge_ready && h->sorted && (uint64_t)h->cap_fluid + h->moving <= MERGE_SMEM_CAP;
 }
@@ -560,10 +570,16 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
             return MPS_ERR_INVALID;
         }
         h->ppe.c16_smem_chunks = h->opt.ppe_smem_chunks == 0 ? 8 : (h->opt.ppe_smem_chunks < 0 ? 0 : h->opt.ppe_smem_chunks);
-        if (h->opt.ppe_layout == 0 && h->opt.precond == MPS_PRECOND_DIAGONAL && !h->nscenes) {
+        h->ppe.precond_every = h->opt.precond_every > 0 ? h->opt.precond_every : 10;
+        h->ppe.index_of_id = h->index_of_id;
+        if (h->opt.ppe_layout == 0 && !h->nscenes) {
             e = ppe_c16_enable(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
-            h->ppe.c16 = true;
+            if (h->opt.precond == MPS_PRECOND_LEARNED) {
+                e = ppe_c16_learned_enable(h->ppe, &h->err);
+                if (e != MPS_OK) return (mps_status)e;
+            }
+            set_compact(h, true);
         }
         if (h->opt.visc_implicit) {
             e = ppe_setup(h->cn, h->cap, h->g, h->P, h->prm, h->stream, &h->err);
@@ -1036,6 +1052,8 @@ extern "C" void mps_destroy(mps_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (int b = 0; b < 2; b++)
         if (h->graph[b]) cudaGraphExecDestroy(h->graph[b]);
+    for (int b = 2; b < 4; b++)
+        if (h->graph[b]) cudaGraphExecDestroy(h->graph[b]);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     ppe_free(h->ppe);
     ppe_free(h->cn);
@@ -1050,7 +1068,15 @@ extern "C" void mps_destroy(mps_handle* h) {
 extern "C" const char* mps_last_error(mps_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
 // ---------------------------------------------------------------- stepping
-static mps_status capture_graph(mps_handle* h, int parity) {
+// Before every step: whether it evaluates the learned network (the learned
+// compact preconditioner re-evaluates it every precond_every steps); false
+// for every other configuration.
+static bool begin_step(mps_handle* h) {
+    if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT || !h->ppe.c16_learned) return false;
+    return ppe_begin_step(h->ppe);
+}
+
+static mps_status capture_graph(mps_handle* h, int parity, int slot) {
     cudaGraph_t g;
     const int saved = h->cur;
     h->cur = parity;
@@ -1068,7 +1094,7 @@ static mps_status capture_graph(mps_handle* h, int parity) {
         h->err = "unexpected buffer parity after a step";
         return MPS_ERR_INVALID;
     }
-    e = cudaGraphInstantiate(&h->graph[parity], g, 0);
+    e = cudaGraphInstantiate(&h->graph[slot], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         h->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
@@ -1078,7 +1104,7 @@ static mps_status capture_graph(mps_handle* h, int parity) {
 }
 
 static void drop_graphs(mps_handle* h) {
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < 4; b++)
         if (h->graph[b]) {
             cudaGraphExecDestroy(h->graph[b]);
             h->graph[b] = nullptr;
@@ -1089,10 +1115,12 @@ static mps_status step_async(mps_handle* h, int nsteps) {
     h->sc_valid = false;
     CK(cudaSetDevice(h->dev));
     for (int k = 0; k < nsteps; k++) {
+        const bool net = begin_step(h);
         if (h->opt.use_graph && !h->graph_off) {
             const int p = h->cur;
-            if (!h->graph[p]) {
-                mps_status s = capture_graph(h, p);
+            const int slot = p + (net ? 2 : 0);
+            if (!h->graph[slot]) {
+                mps_status s = capture_graph(h, p, slot);
                 if (s != MPS_OK) {
                     // a capture the driver refuses falls back to direct
                     // launches; the reason stays readable
@@ -1103,7 +1131,7 @@ static mps_status step_async(mps_handle* h, int nsteps) {
                     continue;
                 }
             }
-            CK(cudaGraphLaunch(h->graph[p], h->stream));
+            CK(cudaGraphLaunch(h->graph[slot], h->stream));
             h->cur ^= 1;
         } else {
             enqueue_step(h);
@@ -1176,6 +1204,7 @@ extern "C" mps_status mps_phase(mps_handle* h, int phase) {
         case 6: launch_dash(stage_args(h), cap, st); h->pending_apply = APPLY_ADD_VEL; break;
         case 7:
             if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT) return MPS_ERR_INVALID;
+            begin_step(h);
             ppe_enqueue_setup(h->ppe, stage_args(h), h->opt, cap, st);
             ppe_enqueue_solve(h->ppe, stage_args(h), h->opt, cap, st);
             break;
@@ -1354,6 +1383,7 @@ extern "C" mps_status mps_precond_set_params(mps_handle* h, const float* w, uint
     int e = ppe_enable_learned(h->ppe, &h->err);
     if (e != MPS_OK) return (mps_status)e;
     lp_upload_params(h->ppe.lp, w, h->stream);
+    h->ppe.lp.s_ready = false;  // the next step evaluates the new network
     CK(cudaStreamSynchronize(h->stream));
     if (!was_ready) drop_graphs(h);  // the step now also runs the network
     return MPS_OK;
@@ -1433,6 +1463,7 @@ extern "C" mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double
     const bool exact = h->opt.arith == MPS_ARITH_EXACT;
     const size_t ng = (size_t)h->cap * LP_GW, nd = h->cap;
     std::vector<float> g0(ng), d0(nd), g1(ng), d1(nd);
+    lp_build_stencil(h->ppe.lp, L, h->cap, h->stream);  // this system's stencil
     for (int pass = 0; pass < 2; pass++) {
         lp_forward(h->ppe.lp, L, exact, h->cap, h->stream, pass == 1);
         CK(cudaMemcpyAsync(pass ? g1.data() : g0.data(), h->ppe.lp.gval, ng * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -1453,6 +1484,7 @@ extern "C" mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double
     h->ppe.lp.tensor_cores = enable != 0;
     lp_forward(h->ppe.lp, L, exact, h->cap, h->stream, h->ppe.lp.tensor_cores);
     CK(cudaStreamSynchronize(h->stream));
+    h->ppe.lp.s_ready = false;  // the next step evaluates the network with the chosen layers
     drop_graphs(h);
     Scalars sc;
     return read_status(h, &sc);
@@ -1512,6 +1544,7 @@ extern "C" mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage
     for (int s = 0; s < nsteps; s++) {
         h->prof_on = true;
         h->prof_used = 0;
+        begin_step(h);
         enqueue_step(h);
         mark(h, -1);
         h->prof_on = false;
@@ -1567,7 +1600,7 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
         const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
         const int nforms = (learned || h->nscenes) ? 2 : 3;
         // form 3: the compact layout (single scenes, diagonal scaling)
-        const bool compact_ok = h->ppe.c16_ready && !learned && !h->nscenes;
+        const bool compact_ok = h->ppe.c16_ready && !h->nscenes && (!learned || h->ppe.sp_cols != nullptr);
         best = 1e300;
         int best_p = h->ppe.threads;
         bool best_sw = h->ppe.stored_weights, best_pipe = h->ppe.pipelined, best_c16 = h->ppe.c16;
@@ -1585,7 +1618,7 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
             }
             h->ppe.stored_weights = form != 1;
             h->ppe.pipelined = form == 2;
-            h->ppe.c16 = form == 3;
+            set_compact(h, form == 3);
             drop_graphs(h);
             double tot = 0.0;
             for (int k = 0; k < steps; k++) {
@@ -1607,7 +1640,7 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
         ppe_set_threads(h->ppe, best_p);
         h->ppe.stored_weights = best_sw;
         h->ppe.pipelined = best_pipe;
-        h->ppe.c16 = best_c16;
+        set_compact(h, best_c16);
         r.ppe_threads = best_p;
         r.ppe_stored_weights = best_sw ? 1 : 0;
         r.ppe_pipelined = best_pipe ? 1 : 0;
@@ -1627,11 +1660,12 @@ extern "C" mps_status mps_apply_tuning(mps_handle* h, const mps_tune_report* r) 
     if (h->opt.method == MPS_METHOD_SEMI_IMPLICIT) {
         const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
         if (r->ppe_compact) {
-            if (learned || h->nscenes) {
-                h->err = "the compact PPE layout is for single scenes with diagonal scaling";
+            if (h->nscenes) {
+                h->err = "the compact PPE layout is for single scenes";
                 return MPS_ERR_INVALID;
             }
-            const int e = ppe_c16_enable(h->ppe, &h->err);
+            int e = ppe_c16_enable(h->ppe, &h->err);
+            if (e == MPS_OK && h->opt.precond == MPS_PRECOND_LEARNED) e = ppe_c16_learned_enable(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
         }
         if (r->ppe_pipelined && (learned || h->nscenes)) {
@@ -1644,7 +1678,7 @@ extern "C" mps_status mps_apply_tuning(mps_handle* h, const mps_tune_report* r) 
         }
         h->ppe.stored_weights = r->ppe_stored_weights != 0;
         h->ppe.pipelined = r->ppe_pipelined != 0;
-        h->ppe.c16 = r->ppe_compact != 0;
+        set_compact(h, r->ppe_compact != 0);
     }
     drop_graphs(h);
     return MPS_OK;

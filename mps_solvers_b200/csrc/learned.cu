@@ -1087,7 +1087,8 @@ static int lp_setup_training(LearnedWork& L) {
 }
 
 void lp_free(LearnedWork& L) {
-    void* ps[] = {L.w32, L.w16, L.grad, L.adam_m, L.adam_v, L.scols, L.scnt, L.nlow, L.gdiag, L.gval,
+    void* ps[] = {L.s_cnt, L.s_col, L.s_val, L.s_diag,
+                  L.w32, L.w16, L.grad, L.adam_m, L.adam_v, L.scols, L.scnt, L.nlow, L.gdiag, L.gval,
                   L.a1,  L.pre1, L.h1,  L.uh1,  L.a2,  L.pre2, L.h2,  L.ra,   L.rb,  L.dgpre, L.dinv,
                   L.lo_off, L.up_off, L.lo_cols, L.up_cols, L.lo_vals, L.up_vals,
                   L.dh1, L.dh2, L.dra,  L.drb,  L.duh1, L.da,  L.dgval, L.dgdiag, L.z, L.v1, L.v2,
@@ -1158,7 +1159,8 @@ void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStrea
                                                              const_cast<Scalars*>(S.sc));
 }
 
-void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores) {
+void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
+                bool pack_factor) {
     (void)exact;
     const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
     const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
@@ -1192,6 +1194,7 @@ void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cud
     dense(L.h2, LP_RB, -1, nullptr, nullptr, L.rb, 0);
     k_lp_readout_fwd<<<wb, 256, 0, st>>>(A);
     k_lp_transpose<<<blocks_for(cap, 256), 256, 0, st>>>(L.scols, L.scnt, L.nlow, L.gval, S.rowlist, S.nrows);
+    if (!pack_factor) return;
     // the solve layout
     const uint32_t maxslices = (cap + LP_SLICE - 1) / LP_SLICE;
     k_lp_slice_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(L.scnt, L.nlow, S.rowlist, S.nrows, L.lo_off,
@@ -1203,8 +1206,67 @@ void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cud
                                                                     L.lo_vals, L.up_cols, L.up_vals);
 }
 
+// ---------------------------------------------------------------- symmetric form
+__global__ void k_lp_sym_reset(uint32_t* __restrict__ s_cnt, float* __restrict__ s_diag, uint32_t n) {
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    s_cnt[id] = 0;
+    s_diag[id] = 1.f;
+}
+
+// Row i (thread per row): S_ij = G_ii G_ij for its j < i entries and
+// G_ji G_jj for its j > i ones (k_lp_transpose left G_ji there); the two
+// products of one pair are the same two factors, so S is symmetric bit for
+// bit.  S_ii = max(G_ii^2, (1 + 1e-3) sum_j |S_ij|).
+__global__ void __launch_bounds__(256) k_lp_sym_build(LpSystem S, const uint32_t* __restrict__ scols,
+                                                      const uint32_t* __restrict__ scnt,
+                                                      const uint32_t* __restrict__ nlow, const float* __restrict__ gval,
+                                                      const float* __restrict__ gdiag, uint32_t* __restrict__ s_cnt,
+                                                      uint32_t* __restrict__ s_col, float* __restrict__ s_val,
+                                                      float* __restrict__ s_diag) {
+    const uint32_t R = *S.nrows;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= R) return;
+    const uint32_t i = __ldg(S.rowlist + k);
+    const uint32_t id = __ldg(S.id + i);
+    const float gi = gdiag[i];
+    const uint32_t n = scnt[i], nl = nlow[i];
+    float sum = 0.f;
+    for (uint32_t t = 0; t < n; t++) {
+        const uint32_t j = scols[(size_t)i * LP_GW + t];
+        const float g = gval[(size_t)i * LP_GW + t];
+        const float v = t < nl ? gi * g : g * gdiag[j];
+        s_col[(size_t)id * LP_GW + t] = __ldg(S.id + j);
+        s_val[(size_t)id * LP_GW + t] = v;
+        sum += fabsf(v);
+    }
+    s_cnt[id] = n;
+    s_diag[id] = fmaxf(gi * gi, 1.001f * sum);
+}
+
+int lp_alloc_symmetric(LearnedWork& L) {
+    if (L.s_cnt) return MPS_OK;
+    const size_t N = L.cap, NG = (size_t)L.cap * LP_GW;
+    if (cudaMalloc(&L.s_cnt, N * 4 + 64) != cudaSuccess || cudaMalloc(&L.s_col, NG * 4 + 64) != cudaSuccess ||
+        cudaMalloc(&L.s_val, NG * 4 + 64) != cudaSuccess || cudaMalloc(&L.s_diag, N * 4 + 64) != cudaSuccess)
+        return MPS_ERR_CUDA;
+    return MPS_OK;
+}
+
+int lp_build_symmetric(LearnedWork& L, const LpSystem& S, uint32_t np0, cudaStream_t st) {
+    if (!L.s_cnt) return MPS_ERR_INVALID;
+    k_lp_sym_reset<<<blocks_for(np0, 256), 256, 0, st>>>(L.s_cnt, L.s_diag, np0);
+    k_lp_sym_build<<<blocks_for(L.cap, 256), 256, 0, st>>>(S, L.scols, L.scnt, L.nlow, L.gval, L.gdiag, L.s_cnt,
+                                                           L.s_col, L.s_val, L.s_diag);
+    L.s_ready = true;
+    return MPS_OK;
+}
+
 int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, uint32_t cap, cudaStream_t st) {
     if (lp_setup_training(L) != MPS_OK) return MPS_ERR_CUDA;
+    // the stencil of this system (a step may have kept an older one between
+    // network evaluations)
+    lp_build_stencil(L, S, cap, st);
     lp_forward(L, S, exact, cap, st, false);  // training: FP32 activations (the oracle's network)
     const uint32_t tb = blocks_for(cap, 256), wb = blocks_for(cap * 32u, 256);
     const uint32_t db = blocks_for(cap, 4);

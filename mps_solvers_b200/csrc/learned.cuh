@@ -100,6 +100,16 @@ struct LearnedWork {
     uint32_t *lo_off = nullptr, *up_off = nullptr;
     uint32_t *lo_cols = nullptr, *up_cols = nullptr;
     float *lo_vals = nullptr, *up_vals = nullptr;
+    // The symmetric first-order form of G^T G on G's own pattern (both
+    // triangles), S = G_d^2 + G_d G_L + G_L^T G_d (G_d the diagonal, G_L the
+    // strict lower part), with the diagonal raised where needed so that S is
+    // diagonally dominant and therefore SPD.  Kept by GEO index (particle id)
+    // so that it stays valid across re-sorts between network evaluations.
+    uint32_t* s_cnt = nullptr;       // cap: stored entries of the row (0: none, S_ii = 1)
+    uint32_t* s_col = nullptr;       // cap * LP_GW: the neighbour's GEO index
+    float* s_val = nullptr;          // cap * LP_GW: S_ij
+    float* s_diag = nullptr;         // cap: S_ii
+    bool s_ready = false;            // built at least once
 };
 
 constexpr uint32_t LP_SLICE = 32;
@@ -137,12 +147,17 @@ void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStrea
 // network forward on the built stencil -> gdiag, gval (G and G^T values);
 // tensor_cores: the 64 -> 64 layers on tcgen05 with BF16 activations
 // (inference), else in FP32 on the CUDA cores (training)
-void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores);
+void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
+                bool pack_factor = true);
 // loss sums (L.loss = {z^T M z, sum log G_ii}) and the parameter gradient
 // (L.grad) for a probe seed; the loss is lp_loss_value of those sums
 int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, uint32_t cap, cudaStream_t st);
 double lp_loss_value(const double* sums, uint32_t nrows);
 // one Adam step on the FP32 master weights, then refresh the BF16 copy
 void lp_adam(LearnedWork& L, float lr, cudaStream_t st);
+// The symmetric form S by particle id (s_* arrays): allocate them, and
+// build them after lp_forward (for np0 GEO indices)
+int lp_alloc_symmetric(LearnedWork& L);
+int lp_build_symmetric(LearnedWork& L, const LpSystem& S, uint32_t np0, cudaStream_t st);
 
 }  // namespace mpsb

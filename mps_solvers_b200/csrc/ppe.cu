@@ -1607,7 +1607,18 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.id_snap, a.cur.id, (size_t)cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
     w.have_snapshot = true;
-    if (w.lp.ready) {
+    if (w.lp.ready && w.c16_learned && !a.batch.n) {
+        // the symmetric form by GEO index, rebuilt every precond_every steps;
+        // S' of the current rows every step
+        if (w.build_net) {
+            const LpSystem L = ppe_lp_system(w, a);
+            lp_build_stencil(w.lp, L, cap, st);
+            lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores, false);
+            lp_build_symmetric(w.lp, L, cap, st);
+            launched += 12;
+        }
+        launched += ppe_c16_enqueue_learned_pack(w, a, cap, st);
+    } else if (w.lp.ready) {
         const LpSystem L = ppe_lp_system(w, a);
         lp_build_stencil(w.lp, L, cap, st);
         lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores);
@@ -1744,7 +1755,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         return 2;
     }
     const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
-    if (w.c16 && !learned) return ppe_c16_enqueue_solve(w, a, opt, cap, st);
+    if (w.c16 && (!learned || w.c16_learned)) return ppe_c16_enqueue_solve(w, a, opt, cap, st);
     if (w.pipelined && !learned) {
         PipeArgs Pa;
         Pa.rowlist = w.rowlist;

@@ -103,7 +103,29 @@ struct PpeWork {
     double *cb64 = nullptr, *cx64 = nullptr, *cdiag64 = nullptr;
     float *cdiag32 = nullptr, *cinv_diag = nullptr, *cr = nullptr, *cq = nullptr;
     float2* czp[2] = {nullptr, nullptr};
+    // the learned preconditioner on the compact layout: S' = D^-1/2 S D^-1/2
+    // (S the symmetric form in LearnedWork, kept by GEO index) in 4-row
+    // slices, one product fused into the residual update of every iteration
+    bool c16_learned = false;          // the compact solve applies S'
+    int precond_every = 10;            // steps between network evaluations
+    uint32_t* sp_off = nullptr;        // first chunk of every slice (widths, then scanned)
+    uint32_t* sp_cols = nullptr;       // 128 compact columns per chunk
+    float* sp_vals = nullptr;          // 128 values per chunk
+    float* cr2 = nullptr;              // second residual buffer of the fused update
+    size_t sp_cap_chunks = 0;
+    const uint32_t* index_of_id = nullptr;  // the handle's GEO index -> sorted position
+    bool build_net = true;             // this step evaluates the network (c16_learned)
+    uint64_t net_steps = 0;            // steps since the handle was created
 };
+
+// The learned compact form re-evaluates its network every precond_every
+// steps (and whenever its form has not been built): decide for the next
+// step, count it, and return the decision.
+inline bool ppe_begin_step(PpeWork& w) {
+    w.build_net = !w.lp.s_ready || w.precond_every <= 1 || (w.net_steps % (uint64_t)w.precond_every) == 0;
+    w.net_steps++;
+    return w.build_net;
+}
 
 int ppe_setup(PpeWork& w, uint32_t cap, const Grid& g, const Phys& P, const mps_params& prm, cudaStream_t st,
               std::string* err);
@@ -136,6 +158,10 @@ int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt
 int ppe_c16_export(const PpeWork& w, uint32_t np, const uint32_t* d_row_start, uint32_t* d_cols, float* d_w,
                    cudaStream_t st);
 void ppe_c16_free(PpeWork& w);
+// the learned S' on the compact layout: buffers, and its per-step pack from
+// the symmetric form kept by GEO index (after ppe_c16_enqueue_pack)
+int ppe_c16_learned_enable(PpeWork& w, std::string* err);
+int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st);
 // the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
 // either way); MPS_ERR_INVALID when the device cannot hold that shape
 int ppe_set_threads(PpeWork& w, int threads);

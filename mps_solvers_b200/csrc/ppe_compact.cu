@@ -174,6 +174,115 @@ __global__ void __launch_bounds__(256) k_c16_export(const uint32_t* __restrict__
         }
 }
 
+// ---------------------------------------------------------------- learned S'
+// S' = D^-1/2 S D^-1/2 on the compact rows, S the symmetric form of the
+// learned factor kept by GEO index (learned.cuh): row k holds its diagonal
+// (first) and the stored neighbours that are rows now, in 4-row slices of
+// 32-entry chunks (lane 8 r + l: entries 32 t + 4 l .. + 3 of row r), 32-bit
+// compact columns, padding = the row itself with value 0.
+constexpr uint32_t SP_MAXW = (LP_GW + 1 + 31) / 32;  // chunks a row can need
+
+struct SpArgs {
+    const uint32_t* rowlist;
+    const uint32_t* nrows;
+    const uint32_t* idv;       // GEO index of each particle
+    const uint32_t* index_of_id;
+    const uint32_t* rlen;
+    const uint32_t* cpos;
+    const double* diag64;      // particle-indexed diagonal of A
+    const uint32_t* s_cnt;
+    const uint32_t* s_col;
+    const float* s_val;
+    const float* s_diag;
+    const Scalars* sc;
+    uint32_t* off;             // widths, then the scanned first chunks
+    uint32_t* cols;
+    float* vals;
+    uint32_t maxslices;
+};
+
+__device__ __forceinline__ bool sp_row_now(const SpArgs& A, uint32_t jd, uint32_t np, uint32_t* j) {
+    const uint32_t jj = __ldg(A.index_of_id + jd);
+    *j = jj;
+    return jj < np && __ldg(A.rlen + jj) != PPE_DIRICHLET;
+}
+
+// chunks per slice: one warp per slice, 8 lanes per row
+__global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
+    const uint32_t R = *A.nrows, np = A.sc->np;
+    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31, r = lane >> 3, l = lane & 7;
+    if (slice > A.maxslices) return;
+    const uint32_t k = slice * C16_ROWS + r;
+    uint32_t cnt = 0;
+    if (k < R) {
+        const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
+        const uint32_t n = __ldg(A.s_cnt + id);
+        for (uint32_t t = l; t < n; t += 8) {
+            uint32_t j;
+            cnt += sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, &j) ? 1u : 0u;
+        }
+        if (l == 0) cnt += 1;  // the diagonal
+    }
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, 2);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, 4);
+    cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, 8));
+    cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, 16));
+    if (lane == 0) A.off[slice] = (cnt + 31u) / 32u;
+}
+
+__global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
+    const uint32_t R = *A.nrows, np = A.sc->np;
+    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31, r = lane >> 3, l = lane & 7;
+    if (slice >= (R + C16_ROWS - 1) / C16_ROWS) return;
+    const uint32_t g0 = A.off[slice], T = A.off[slice + 1] - g0;
+    const uint32_t k = slice * C16_ROWS + r;
+    const bool has = k < R;
+    // padding first: every slot of the row is the row itself with value 0
+    for (uint32_t t = 0; t < T; t++) {
+        const size_t at = (size_t)(g0 + t) * C16_CHUNK + 32u * r + 4u * l;
+        *reinterpret_cast<uint4*>(A.cols + at) = make_uint4(k, k, k, k);
+        *reinterpret_cast<float4*>(A.vals + at) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncwarp();
+    uint32_t id = 0, n = 0, i = 0;
+    float di = 0.f;
+    if (has) {
+        i = __ldg(A.rowlist + k);
+        id = __ldg(A.idv + i);
+        n = __ldg(A.s_cnt + id);
+        di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
+        if (l == 0) {
+            const size_t at = (size_t)g0 * C16_CHUNK + 32u * r;
+            A.cols[at] = k;
+            A.vals[at] = __ldg(A.s_diag + id) * (di * di);
+        }
+    }
+    uint32_t nmax = n;
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 1));
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 2));
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 4));
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 8));
+    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 16));
+    uint32_t pos = 1;  // after the diagonal
+    for (uint32_t t0 = 0; t0 < nmax; t0 += 8) {
+        const uint32_t t = t0 + l;
+        uint32_t j = 0;
+        const bool ok = has && t < n && sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, &j);
+        const uint32_t m = (__ballot_sync(0xffffffffu, ok) >> (8u * r)) & 0xffu;
+        if (ok) {
+            const uint32_t q = pos + __popc(m & ((1u << l) - 1u));
+            const size_t at = (size_t)(g0 + q / 32u) * C16_CHUNK + 32u * r + (q % 32u);
+            const float dj = (float)(1.0 / sqrt(-__ldg(A.diag64 + j)));
+            A.cols[at] = __ldg(A.cpos + j);
+            A.vals[at] = __ldg(A.s_val + (size_t)id * LP_GW + t) * (di * dj);
+        }
+        pos += __popc(m);
+    }
+}
+
 // ---------------------------------------------------------------- solve
 struct C16Args {
     const uint32_t* nrows;
@@ -198,7 +307,33 @@ struct C16Args {
     uint32_t keep;             // chunks read as evict_last
     int max_iter, inner_cap, max_outer;
     int smem_chunks;           // chunks per warp held in shared memory
+    // learned S' (LRN): slices of the same 4 rows, the second residual buffer
+    const uint32_t* sp_off;
+    const uint32_t* sp_cols;
+    const float* sp_vals;
+    float* r2;
 };
+
+// Row sums of S' x over a slice: lanes 8 r .. 8 r + 7 return row r's sum
+// (x_j given by a functor of the compact column).
+template <class X>
+__device__ __forceinline__ float sp_slice_sum(const C16Args& S, uint32_t sl, uint32_t lane, X x) {
+    const uint32_t g0 = __ldg(S.sp_off + sl), T = __ldg(S.sp_off + sl + 1) - g0;
+    float s = 0.f;
+    for (uint32_t t = 0; t < T; t++) {
+        const size_t at = (size_t)(g0 + t) * C16_CHUNK + 4u * lane;
+        const uint4 c = __ldg(reinterpret_cast<const uint4*>(S.sp_cols + at));
+        const float4 v = __ldg(reinterpret_cast<const float4*>(S.sp_vals + at));
+        s = fmaf(v.x, x(c.x), s);
+        s = fmaf(v.y, x(c.y), s);
+        s = fmaf(v.z, x(c.z), s);
+        s = fmaf(v.w, x(c.w), s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    return s;
+}
 
 // The four columns of a lane's chunk entries.
 __device__ __forceinline__ void c16_cols(const uint2 cw, int base, const uint32_t* __restrict__ side, size_t at,
@@ -225,7 +360,10 @@ __device__ __forceinline__ uint2 ld_codes(const uint2* p, uint64_t pol) {
 
 __device__ __forceinline__ uint64_t c16_policy(uint32_t chunk, uint32_t keep) { return mat_policy(chunk, keep); }
 
-template <bool EX>
+// LRN: the learned preconditioner z = S' r instead of z = D^-1 r; S' is
+// applied in the residual update (the neighbours' new residuals formed from
+// r and q on the fly), so an iteration keeps two grid-wide reductions.
+template <bool EX, bool LRN>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
     extern __shared__ __align__(16) unsigned char c16_sm[];
     const uint32_t R = *S.nrows;
@@ -264,6 +402,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
     bool converged = false;
     float2* zc = S.zp0;
     float2* zn = S.zp1;
+    float* rc = S.r;   // residual read by this iteration
+    float* ra = S.r2;  // and the buffer its update writes (LRN)
     for (int outer = 0; outer < S.max_outer; outer++) {
         // ---- true residual r64 = b - A x64 (FP64); z = D^-1 r, p = 0
         double acc[3] = {0.0, 0.0, 0.0};
@@ -298,12 +438,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
                 const double bi = S.b64[k];
                 const double ri = bi - (S.diag64[k] * S.x64[k] + s);
                 const float rf = (float)ri;
-                const float zf = rf * S.inv_diag[k];
-                S.r[k] = rf;
-                zc[k] = make_float2(zf, 0.f);
+                rc[k] = rf;
+                if (!LRN) {
+                    const float zf = rf * S.inv_diag[k];
+                    zc[k] = make_float2(zf, 0.f);
+                    acc[2] += (double)rf * (double)zf;
+                }
                 acc[0] += ri * ri;
                 acc[1] += bi * bi;
-                acc[2] += (double)rf * (double)zf;
             }
         }
         double tot[3];
@@ -316,6 +458,22 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
             break;
         }
         if (total >= S.max_iter) break;
+        if (LRN) {
+            // z = S' r of the new residual, r.z
+            double rz0[1] = {0.0};
+            for (uint32_t sl = gw; sl < nsl; sl += nw) {
+                const float* rr_ = rc;
+                const float zs = sp_slice_sum(S, sl, lane, [rr_](uint32_t j) { return rr_[j]; });
+                const uint32_t k = sl * C16_ROWS + rr;
+                if (l == 0 && k < R) {
+                    zc[k] = make_float2(zs, 0.f);
+                    rz0[0] += (double)rc[k] * (double)zs;
+                }
+            }
+            double trz[1];
+            if (!grid_reduce<1>(rz0, S.part, S.result, S.bar, S.sc, trz)) return;
+            tot[2] = trz[0];
+        }
         double eta = 0.3 * S.tol / relres;
         if (eta < S.eta_min) eta = S.eta_min;
         if (eta > 0.5) eta = 0.5;
@@ -375,20 +533,46 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
             if (!grid_reduce<1>(pq, S.part, S.result, S.bar, S.sc, totp)) return;
             const double alpha = rz / totp[0];
             const float alpha_f = (float)alpha;
-            // ---- x64 += alpha p, r -= alpha q, z = D^-1 r, r.z, r.r
+            // ---- x64 += alpha p, r -= alpha q, z = M^-1 r, r.z, r.r
             double acc2[2] = {0.0, 0.0};
-            for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < R; k += gridDim.x * blockDim.x) {
-                const float pn = zn[k].y;
-                S.x64[k] += alpha * (double)pn;
-                const float ri = fmaf(-alpha_f, S.q[k], S.r[k]);
-                const float zi = ri * S.inv_diag[k];
-                S.r[k] = ri;
-                zn[k] = make_float2(zi, pn);
-                acc2[0] += (double)ri * (double)zi;
-                acc2[1] += (double)ri * (double)ri;
+            if (LRN) {
+                // z_k = sum_j S'_kj (r_j - alpha q_j), the new residual into
+                // the other buffer (the neighbours read the old one)
+                for (uint32_t sl = gw; sl < nsl; sl += nw) {
+                    const float* rr_ = rc;
+                    const float* qq_ = S.q;
+                    const float zs = sp_slice_sum(S, sl, lane,
+                                                  [rr_, qq_, alpha_f](uint32_t j) { return fmaf(-alpha_f, qq_[j], rr_[j]); });
+                    const uint32_t k = sl * C16_ROWS + rr;
+                    if (l == 0 && k < R) {
+                        const float pn = zn[k].y;
+                        S.x64[k] += alpha * (double)pn;
+                        const float ri = fmaf(-alpha_f, S.q[k], rc[k]);
+                        ra[k] = ri;
+                        zn[k] = make_float2(zs, pn);
+                        acc2[0] += (double)ri * (double)zs;
+                        acc2[1] += (double)ri * (double)ri;
+                    }
+                }
+            } else {
+                for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < R; k += gridDim.x * blockDim.x) {
+                    const float pn = zn[k].y;
+                    S.x64[k] += alpha * (double)pn;
+                    const float ri = fmaf(-alpha_f, S.q[k], rc[k]);
+                    const float zi = ri * S.inv_diag[k];
+                    rc[k] = ri;
+                    zn[k] = make_float2(zi, pn);
+                    acc2[0] += (double)ri * (double)zi;
+                    acc2[1] += (double)ri * (double)ri;
+                }
             }
             double tot2[2];
             if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
+            if (LRN) {
+                float* t_ = rc;
+                rc = ra;
+                ra = t_;
+            }
             total++;
             beta = (float)(tot2[0] / rz);
             rz = tot2[0];
@@ -450,9 +634,13 @@ int ppe_c16_enable(PpeWork& w, std::string* err) {
     cudaMemset(w.czp[0], 0, vec * sizeof(float2));
     cudaMemset(w.czp[1], 0, vec * sizeof(float2));
     const size_t most = c16_smem_bytes(PPE_THREADS, 8);
-    if (cudaFuncSetAttribute(k_ppe_solve_c16<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
+    if (cudaFuncSetAttribute(k_ppe_solve_c16<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(k_ppe_solve_c16<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
+        cudaFuncSetAttribute(k_ppe_solve_c16<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_ppe_solve_c16<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_ppe_solve_c16<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) !=
             cudaSuccess) {
         ppe_c16_free(w);
         if (err) *err = "the compact PPE solver cannot have its shared memory";
@@ -464,7 +652,7 @@ int ppe_c16_enable(PpeWork& w, std::string* err) {
 
 void ppe_c16_free(PpeWork& w) {
     void* ps[] = {w.cpos, w.c16_width, w.c16_codes, w.c16_w, w.c16_side, w.c16_esc, w.cb64, w.cx64, w.cdiag64,
-                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1]};
+                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1], w.sp_off, w.sp_cols, w.sp_vals, w.cr2};
     for (void* p : ps)
         if (p) cudaFree(p);
     w.cpos = w.c16_width = w.c16_esc = nullptr;
@@ -474,8 +662,13 @@ void ppe_c16_free(PpeWork& w) {
     w.cb64 = w.cx64 = w.cdiag64 = nullptr;
     w.cdiag32 = w.cinv_diag = w.cr = w.cq = nullptr;
     w.czp[0] = w.czp[1] = nullptr;
+    w.sp_off = nullptr;
+    w.sp_cols = nullptr;
+    w.sp_vals = nullptr;
+    w.cr2 = nullptr;
     w.c16_ready = false;
     w.c16 = false;
+    w.c16_learned = false;
 }
 
 int ppe_c16_enqueue_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st) {
@@ -526,12 +719,63 @@ int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt
     if (chunks > 8) chunks = 8;
     S.smem_chunks = chunks;
     const size_t smem = c16_smem_bytes(w.threads, chunks);
+    S.sp_off = w.sp_off;
+    S.sp_cols = w.sp_cols;
+    S.sp_vals = w.sp_vals;
+    S.r2 = w.cr2;
     void* args[] = {&S};
-    const void* fn = a.exact ? (const void*)k_ppe_solve_c16<true> : (const void*)k_ppe_solve_c16<false>;
+    const bool lrn = w.c16_learned;
+    const void* fn = a.exact ? (lrn ? (const void*)k_ppe_solve_c16<true, true> : (const void*)k_ppe_solve_c16<true, false>)
+                             : (lrn ? (const void*)k_ppe_solve_c16<false, true> : (const void*)k_ppe_solve_c16<false, false>);
     w.launch_err = launch_cooperative_smem(fn, w.blocks, w.threads, smem, args, st);
     if (!w.write_pressure) return 1;
     k_c16_finish<<<cblocks(cap, 256), 256, 0, st>>>(w.cx64, w.rlen, w.cpos, a.cur.press, a.sc);
     return 2;
+}
+
+int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
+    if (lp_alloc_symmetric(w.lp) != MPS_OK) {
+        if (err) *err = "cudaMalloc failed for the learned symmetric form";
+        return MPS_ERR_CUDA;
+    }
+    if (w.sp_cols) return MPS_OK;
+    const size_t slices = (w.cap + C16_ROWS - 1) / C16_ROWS + 2;
+    w.sp_cap_chunks = slices * SP_MAXW;
+    bool ok = c16_alloc(&w.sp_off, slices + 2);
+    ok &= c16_alloc(&w.sp_cols, w.sp_cap_chunks * C16_CHUNK);
+    ok &= c16_alloc(&w.sp_vals, w.sp_cap_chunks * C16_CHUNK);
+    ok &= c16_alloc(&w.cr2, (size_t)w.cap + 8);
+    if (!ok) {
+        if (err) *err = "cudaMalloc failed for the learned compact preconditioner";
+        return MPS_ERR_CUDA;
+    }
+    cudaMemset(w.cr2, 0, ((size_t)w.cap + 8) * sizeof(float));
+    return MPS_OK;
+}
+
+int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st) {
+    SpArgs A;
+    A.rowlist = w.rowlist;
+    A.nrows = w.nrows;
+    A.idv = a.cur.id;
+    A.index_of_id = w.index_of_id;
+    A.rlen = w.rlen;
+    A.cpos = w.cpos;
+    A.diag64 = w.diag64;
+    A.s_cnt = w.lp.s_cnt;
+    A.s_col = w.lp.s_col;
+    A.s_val = w.lp.s_val;
+    A.s_diag = w.lp.s_diag;
+    A.sc = a.sc;
+    A.off = w.sp_off;
+    A.cols = w.sp_cols;
+    A.vals = w.sp_vals;
+    const uint32_t maxslices = (cap + C16_ROWS - 1) / C16_ROWS;
+    A.maxslices = maxslices;
+    k_sp_width<<<cblocks((maxslices + 1) * 32u, 256), 256, 0, st>>>(A);
+    launch_scan_exclusive(w.sp_off, maxslices + 1, st);
+    k_sp_pack<<<cblocks(maxslices * 32u, 256), 256, 0, st>>>(A);
+    return 3;
 }
 
 int ppe_c16_export(const PpeWork& w, uint32_t np, const uint32_t* d_row_start, uint32_t* d_cols, float* d_w,
