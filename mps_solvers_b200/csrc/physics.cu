@@ -8,6 +8,7 @@
 // gather.  With EX = true each float operation is rounded once, in the
 // reference's order, so the results equal the reference's CPU results.
 #include "physics.cuh"
+#include "cellblock.cuh"
 #include "cellsort.cuh"
 
 namespace mpsb {
@@ -647,6 +648,62 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     }
 }
 
+// Fast-arithmetic PND of a single scene by cell blocks (cellblock.cuh): one
+// block per coarse cell, half a warp per particle of type != 2 in it, the
+// candidates within r0 walked by sub-cell rows from shared memory.
+__device__ __forceinline__ float half_sum(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;
+}
+
+__global__ void __launch_bounds__(CB_THREADS) k_pnd_cb(StageArgs a) {
+    extern __shared__ __align__(16) unsigned char cb_raw[];
+    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
+    const uint32_t c = blockIdx.x;
+    const uint32_t t_lo = __ldg(a.cell_start + c), t_hi = __ldg(a.cell_start + c + 1);
+    if (t_lo == t_hi) return;
+    const float4* __restrict__ pos = a.cur.pos;
+    // a block of dummy particles only needs no number density
+    bool want = false;
+    for (uint32_t i = t_lo + threadIdx.x; i < t_hi; i += blockDim.x) want |= ptype(__ldg(pos + i)) != T_DUMMY;
+    if (!__syncthreads_or(want)) return;
+    const bool staged = cb_stage(S, a.g, a.cell_start, c, pos);
+    const float re = a.P.rzero, thr = a.P.rzero_thr;
+    const uint32_t lane = threadIdx.x & 31, hl = lane & 15, warp = threadIdx.x >> 5;
+    for (uint32_t b = t_lo + 2 * warp; b < t_hi; b += 2 * CB_WARPS) {
+        const uint32_t i = b + (lane >> 4);
+        const bool active = i < t_hi;
+        const float4 pi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool go = active && ptype(pi) != T_DUMMY;
+        float acc = 0.f;
+        if (go && staged) {
+            const CbWindow w = cb_window(S, pi, re);
+            cb_walk(S, pi, w, hl, [&](uint32_t e) {
+                const float4 pj = S.pos[e];
+                const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                const float rr = dx * dx + dy * dy + dz * dz;
+                if (rr < thr && S.idx[e] != i) acc += weight_rr<false>(re, rr);
+            });
+        } else if (go) {  // too many particles to stage: the coarse cells from global memory
+            const CellNear nr = cell_near(a.g, c, pi.x, pi.y, pi.z, re);
+            for (int row = 0; row < link_rows(a.g); row++) {
+                const RowRange rg = link_row_near(a.g, a.cell_start, c, row, nr);
+                for (uint32_t j = rg.lo + hl; j < rg.hi; j += 16) {
+                    const float4 pj = __ldg(pos + j);
+                    const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                    const float rr = dx * dx + dy * dy + dz * dz;
+                    if (rr < thr && j != i) acc += weight_rr<false>(re, rr);
+                }
+            }
+        }
+        acc = half_sum(acc);
+        if (go && hl == 0) a.cur.n[i] = acc;
+    }
+}
+
 constexpr uint32_t DASH_SLOTS = 64;  // neighbours within r0 kept per particle (~32 on the lattice)
 
 template <bool EX, bool ORD, bool BT>
@@ -788,6 +845,15 @@ void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // equation of state of calPres_expl (MPS_GPU_EXPL.cpp:391-415):
 //   p = max(0, rho c^2 (n - n0) / n0).
 void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
+    if (!a.exact && !a.batch.n && !eos && !all_types && a.cell_blocks) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_pnd_cb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_SMEM);
+            attr = true;
+        }
+        k_pnd_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(a);
+        return;
+    }
     const bool use_list = a.list_solid && !all_types;
     const uint32_t* list = use_list ? a.list_solid : nullptr;
     const uint32_t nb = blocks_for((use_list ? a.cap_solid : cap) * 32u, (uint32_t)a.threads);

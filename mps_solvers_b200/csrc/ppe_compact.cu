@@ -177,10 +177,13 @@ __global__ void __launch_bounds__(256) k_c16_export(const uint32_t* __restrict__
 // ---------------------------------------------------------------- learned S'
 // S' = D^-1/2 S D^-1/2 on the compact rows, S the symmetric form of the
 // learned factor kept by GEO index (learned.cuh): row k holds its diagonal
-// (first) and the stored neighbours that are rows now, in 4-row slices of
-// 32-entry chunks (lane 8 r + l: entries 32 t + 4 l .. + 3 of row r), 32-bit
-// compact columns, padding = the row itself with value 0.
-constexpr uint32_t SP_MAXW = (LP_GW + 1 + 31) / 32;  // chunks a row can need
+// (first) and the stored neighbours that are rows now.  Sliced ELL with a
+// thread per row: slices of 32 consecutive rows, width = the longest row of
+// the slice, entry t of row k at off[k / 32] + 32 t + k % 32 (a warp's loads
+// of one entry index are one 128-byte line), padding = the row itself with
+// value 0.  Applied by the thread that updates the row, so the product needs
+// no more parallelism than the elementwise update.
+constexpr uint32_t SP_SLICE = 32;
 
 struct SpArgs {
     const uint32_t* rowlist;
@@ -195,7 +198,7 @@ struct SpArgs {
     const float* s_val;
     const float* s_diag;
     const Scalars* sc;
-    uint32_t* off;             // widths, then the scanned first chunks
+    uint32_t* off;             // widths (entries), then the scanned first entries
     uint32_t* cols;
     float* vals;
     uint32_t maxslices;
@@ -207,79 +210,53 @@ __device__ __forceinline__ bool sp_row_now(const SpArgs& A, uint32_t jd, uint32_
     return jj < np && __ldg(A.rlen + jj) != PPE_DIRICHLET;
 }
 
-// chunks per slice: one warp per slice, 8 lanes per row
+// entries of every 32-row slice (thread per row, warp per slice)
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31, r = lane >> 3, l = lane & 7;
-    if (slice > A.maxslices) return;
-    const uint32_t k = slice * C16_ROWS + r;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = k / SP_SLICE;
     uint32_t cnt = 0;
     if (k < R) {
         const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
         const uint32_t n = __ldg(A.s_cnt + id);
-        for (uint32_t t = l; t < n; t += 8) {
+        cnt = 1;  // the diagonal
+        for (uint32_t t = 0; t < n; t++) {
             uint32_t j;
             cnt += sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, &j) ? 1u : 0u;
         }
-        if (l == 0) cnt += 1;  // the diagonal
     }
-    cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
-    cnt += __shfl_xor_sync(0xffffffffu, cnt, 2);
-    cnt += __shfl_xor_sync(0xffffffffu, cnt, 4);
-    cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, 8));
-    cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, 16));
-    if (lane == 0) A.off[slice] = (cnt + 31u) / 32u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
+    if ((threadIdx.x & 31) == 0 && s <= A.maxslices) A.off[s] = cnt * SP_SLICE;
 }
 
 __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t slice = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31, r = lane >> 3, l = lane & 7;
-    if (slice >= (R + C16_ROWS - 1) / C16_ROWS) return;
-    const uint32_t g0 = A.off[slice], T = A.off[slice + 1] - g0;
-    const uint32_t k = slice * C16_ROWS + r;
-    const bool has = k < R;
-    // padding first: every slot of the row is the row itself with value 0
-    for (uint32_t t = 0; t < T; t++) {
-        const size_t at = (size_t)(g0 + t) * C16_CHUNK + 32u * r + 4u * l;
-        *reinterpret_cast<uint4*>(A.cols + at) = make_uint4(k, k, k, k);
-        *reinterpret_cast<float4*>(A.vals + at) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    __syncwarp();
-    uint32_t id = 0, n = 0, i = 0;
-    float di = 0.f;
-    if (has) {
-        i = __ldg(A.rowlist + k);
-        id = __ldg(A.idv + i);
-        n = __ldg(A.s_cnt + id);
-        di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
-        if (l == 0) {
-            const size_t at = (size_t)g0 * C16_CHUNK + 32u * r;
-            A.cols[at] = k;
-            A.vals[at] = __ldg(A.s_diag + id) * (di * di);
-        }
-    }
-    uint32_t nmax = n;
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 1));
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 2));
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 4));
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 8));
-    nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, 16));
-    uint32_t pos = 1;  // after the diagonal
-    for (uint32_t t0 = 0; t0 < nmax; t0 += 8) {
-        const uint32_t t = t0 + l;
-        uint32_t j = 0;
-        const bool ok = has && t < n && sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, &j);
-        const uint32_t m = (__ballot_sync(0xffffffffu, ok) >> (8u * r)) & 0xffu;
-        if (ok) {
-            const uint32_t q = pos + __popc(m & ((1u << l) - 1u));
-            const size_t at = (size_t)(g0 + q / 32u) * C16_CHUNK + 32u * r + (q % 32u);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
+    if (s >= (R + SP_SLICE - 1) / SP_SLICE) return;
+    const uint32_t base = A.off[s], W = (A.off[s + 1] - base) / SP_SLICE;
+    uint32_t t = 0;
+    if (k < R) {
+        const uint32_t i = __ldg(A.rowlist + k);
+        const uint32_t id = __ldg(A.idv + i);
+        const uint32_t n = __ldg(A.s_cnt + id);
+        const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
+        A.cols[base + lane] = k;
+        A.vals[base + lane] = __ldg(A.s_diag + id) * (di * di);
+        t = 1;
+        for (uint32_t u = 0; u < n; u++) {
+            uint32_t j;
+            if (!sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, &j)) continue;
             const float dj = (float)(1.0 / sqrt(-__ldg(A.diag64 + j)));
-            A.cols[at] = __ldg(A.cpos + j);
-            A.vals[at] = __ldg(A.s_val + (size_t)id * LP_GW + t) * (di * dj);
+            A.cols[base + SP_SLICE * t + lane] = __ldg(A.cpos + j);
+            A.vals[base + SP_SLICE * t + lane] = __ldg(A.s_val + (size_t)id * LP_GW + u) * (di * dj);
+            t++;
         }
-        pos += __popc(m);
+    }
+    for (; t < W; t++) {
+        A.cols[base + SP_SLICE * t + lane] = k < R ? k : 0u;
+        A.vals[base + SP_SLICE * t + lane] = 0.f;
     }
 }
 
@@ -314,25 +291,23 @@ struct C16Args {
     float* r2;
 };
 
-// Row sums of S' x over a slice: lanes 8 r .. 8 r + 7 return row r's sum
-// (x_j given by a functor of the compact column).
+// Row k of S' x (thread per row; x_j given by a functor of the compact column)
 template <class X>
-__device__ __forceinline__ float sp_slice_sum(const C16Args& S, uint32_t sl, uint32_t lane, X x) {
-    const uint32_t g0 = __ldg(S.sp_off + sl), T = __ldg(S.sp_off + sl + 1) - g0;
-    float s = 0.f;
-    for (uint32_t t = 0; t < T; t++) {
-        const size_t at = (size_t)(g0 + t) * C16_CHUNK + 4u * lane;
-        const uint4 c = __ldg(reinterpret_cast<const uint4*>(S.sp_cols + at));
-        const float4 v = __ldg(reinterpret_cast<const float4*>(S.sp_vals + at));
-        s = fmaf(v.x, x(c.x), s);
-        s = fmaf(v.y, x(c.y), s);
-        s = fmaf(v.z, x(c.z), s);
-        s = fmaf(v.w, x(c.w), s);
+__device__ __forceinline__ float sp_row(const C16Args& S, uint32_t k, X x) {
+    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
+    const uint32_t base = __ldg(S.sp_off + s), W = (__ldg(S.sp_off + s + 1) - base) / SP_SLICE;
+    float a0 = 0.f, a1 = 0.f;
+    uint32_t t = 0;
+    for (; t + 1 < W; t += 2) {
+        const uint32_t c0 = __ldg(S.sp_cols + base + SP_SLICE * t + lane);
+        const uint32_t c1 = __ldg(S.sp_cols + base + SP_SLICE * (t + 1) + lane);
+        const float v0 = __ldg(S.sp_vals + base + SP_SLICE * t + lane);
+        const float v1 = __ldg(S.sp_vals + base + SP_SLICE * (t + 1) + lane);
+        a0 = fmaf(v0, x(c0), a0);
+        a1 = fmaf(v1, x(c1), a1);
     }
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    s += __shfl_xor_sync(0xffffffffu, s, 4);
-    return s;
+    if (t < W) a0 = fmaf(__ldg(S.sp_vals + base + SP_SLICE * t + lane), x(__ldg(S.sp_cols + base + SP_SLICE * t + lane)), a0);
+    return a0 + a1;
 }
 
 // The four columns of a lane's chunk entries.
@@ -461,14 +436,11 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
         if (LRN) {
             // z = S' r of the new residual, r.z
             double rz0[1] = {0.0};
-            for (uint32_t sl = gw; sl < nsl; sl += nw) {
+            for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < R; k += gridDim.x * blockDim.x) {
                 const float* rr_ = rc;
-                const float zs = sp_slice_sum(S, sl, lane, [rr_](uint32_t j) { return rr_[j]; });
-                const uint32_t k = sl * C16_ROWS + rr;
-                if (l == 0 && k < R) {
-                    zc[k] = make_float2(zs, 0.f);
-                    rz0[0] += (double)rc[k] * (double)zs;
-                }
+                const float zs = sp_row(S, k, [rr_](uint32_t j) { return rr_[j]; });
+                zc[k] = make_float2(zs, 0.f);
+                rz0[0] += (double)rc[k] * (double)zs;
             }
             double trz[1];
             if (!grid_reduce<1>(rz0, S.part, S.result, S.bar, S.sc, trz)) return;
@@ -538,21 +510,18 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_c16(C16Args S) {
             if (LRN) {
                 // z_k = sum_j S'_kj (r_j - alpha q_j), the new residual into
                 // the other buffer (the neighbours read the old one)
-                for (uint32_t sl = gw; sl < nsl; sl += nw) {
+                for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < R; k += gridDim.x * blockDim.x) {
                     const float* rr_ = rc;
                     const float* qq_ = S.q;
-                    const float zs = sp_slice_sum(S, sl, lane,
-                                                  [rr_, qq_, alpha_f](uint32_t j) { return fmaf(-alpha_f, qq_[j], rr_[j]); });
-                    const uint32_t k = sl * C16_ROWS + rr;
-                    if (l == 0 && k < R) {
-                        const float pn = zn[k].y;
-                        S.x64[k] += alpha * (double)pn;
-                        const float ri = fmaf(-alpha_f, S.q[k], rc[k]);
-                        ra[k] = ri;
-                        zn[k] = make_float2(zs, pn);
-                        acc2[0] += (double)ri * (double)zs;
-                        acc2[1] += (double)ri * (double)ri;
-                    }
+                    const float zs =
+                        sp_row(S, k, [rr_, qq_, alpha_f](uint32_t j) { return fmaf(-alpha_f, qq_[j], rr_[j]); });
+                    const float pn = zn[k].y;
+                    S.x64[k] += alpha * (double)pn;
+                    const float ri = fmaf(-alpha_f, S.q[k], rc[k]);
+                    ra[k] = ri;
+                    zn[k] = make_float2(zs, pn);
+                    acc2[0] += (double)ri * (double)zs;
+                    acc2[1] += (double)ri * (double)ri;
                 }
             } else {
                 for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < R; k += gridDim.x * blockDim.x) {
@@ -739,11 +708,11 @@ int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
         return MPS_ERR_CUDA;
     }
     if (w.sp_cols) return MPS_OK;
-    const size_t slices = (w.cap + C16_ROWS - 1) / C16_ROWS + 2;
-    w.sp_cap_chunks = slices * SP_MAXW;
+    const size_t slices = (w.cap + SP_SLICE - 1) / SP_SLICE + 2;
+    w.sp_cap_chunks = slices * (LP_GW + 1);  // entries per lane position: 32-row slices of up to LP_GW + 1
     bool ok = c16_alloc(&w.sp_off, slices + 2);
-    ok &= c16_alloc(&w.sp_cols, w.sp_cap_chunks * C16_CHUNK);
-    ok &= c16_alloc(&w.sp_vals, w.sp_cap_chunks * C16_CHUNK);
+    ok &= c16_alloc(&w.sp_cols, w.sp_cap_chunks * SP_SLICE);
+    ok &= c16_alloc(&w.sp_vals, w.sp_cap_chunks * SP_SLICE);
     ok &= c16_alloc(&w.cr2, (size_t)w.cap + 8);
     if (!ok) {
         if (err) *err = "cudaMalloc failed for the learned compact preconditioner";
@@ -770,11 +739,11 @@ int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, c
     A.off = w.sp_off;
     A.cols = w.sp_cols;
     A.vals = w.sp_vals;
-    const uint32_t maxslices = (cap + C16_ROWS - 1) / C16_ROWS;
+    const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
-    k_sp_width<<<cblocks((maxslices + 1) * 32u, 256), 256, 0, st>>>(A);
+    k_sp_width<<<cblocks((maxslices + 1) * SP_SLICE, 256), 256, 0, st>>>(A);
     launch_scan_exclusive(w.sp_off, maxslices + 1, st);
-    k_sp_pack<<<cblocks(maxslices * 32u, 256), 256, 0, st>>>(A);
+    k_sp_pack<<<cblocks(maxslices * SP_SLICE, 256), 256, 0, st>>>(A);
     return 3;
 }
 
