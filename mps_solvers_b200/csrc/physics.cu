@@ -8,7 +8,6 @@
 // gather.  With EX = true each float operation is rounded once, in the
 // reference's order, so the results equal the reference's CPU results.
 #include "physics.cuh"
-#include "cellblock.cuh"
 #include "cellsort.cuh"
 
 namespace mpsb {
@@ -648,228 +647,6 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     }
 }
 
-// Fast-arithmetic PND of a single scene by cell blocks (cellblock.cuh): one
-// block per coarse cell, half a warp per particle of type != 2 in it, the
-// candidates within r0 walked by sub-cell rows from shared memory.
-__device__ __forceinline__ float half_sum(float v) {
-    v += __shfl_xor_sync(0xffffffffu, v, 8);
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    return v;
-}
-
-__global__ void __launch_bounds__(CB_THREADS) k_pnd_cb(StageArgs a) {
-    extern __shared__ __align__(16) unsigned char cb_raw[];
-    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
-    const uint32_t c = blockIdx.x;
-    const uint32_t t_lo = __ldg(a.cell_start + c), t_hi = __ldg(a.cell_start + c + 1);
-    if (t_lo == t_hi) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    // a block of dummy particles only needs no number density
-    bool want = false;
-    for (uint32_t i = t_lo + threadIdx.x; i < t_hi; i += blockDim.x) want |= ptype(__ldg(pos + i)) != T_DUMMY;
-    if (!__syncthreads_or(want)) return;
-    const bool staged = cb_stage(S, a.g, a.cell_start, c, pos);
-    const float re = a.P.rzero, thr = a.P.rzero_thr;
-    const uint32_t lane = threadIdx.x & 31, hl = lane & 15, warp = threadIdx.x >> 5;
-    for (uint32_t b = t_lo + 2 * warp; b < t_hi; b += 2 * CB_WARPS) {
-        const uint32_t i = b + (lane >> 4);
-        const bool active = i < t_hi;
-        const float4 pi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const bool go = active && ptype(pi) != T_DUMMY;
-        float acc = 0.f;
-        if (go && staged) {
-            const CbWindow w = cb_window(S, pi, re);
-            cb_walk(S, pi, w, hl, [&](uint32_t e) {
-                const float4 pj = S.pos[e];
-                const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                const float rr = dx * dx + dy * dy + dz * dz;
-                if (rr < thr && S.idx[e] != i) acc += weight_rr<false>(re, rr);
-            });
-        } else if (go) {  // too many particles to stage: the coarse cells from global memory
-            const CellNear nr = cell_near(a.g, c, pi.x, pi.y, pi.z, re);
-            for (int row = 0; row < link_rows(a.g); row++) {
-                const RowRange rg = link_row_near(a.g, a.cell_start, c, row, nr);
-                for (uint32_t j = rg.lo + hl; j < rg.hi; j += 16) {
-                    const float4 pj = __ldg(pos + j);
-                    const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                    const float rr = dx * dx + dy * dy + dz * dz;
-                    if (rr < thr && j != i) acc += weight_rr<false>(re, rr);
-                }
-            }
-        }
-        acc = half_sum(acc);
-        if (go && hl == 0) a.cur.n[i] = acc;
-    }
-}
-
-// The fluid particles of coarse cell c, two a warp (half a warp each),
-// after the block's candidates are staged: f(i, pi, hl, staged) for each,
-// with every lane of the warp taking the same number of turns.
-template <class F>
-__device__ __forceinline__ void cb_fluid_targets(const StageArgs& a, CbShared& S, uint32_t c, F f) {
-    const uint32_t t_lo = __ldg(a.cell_start + c), t_hi = __ldg(a.cell_start + c + 1);
-    if (t_lo == t_hi) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    bool want = false;
-    for (uint32_t i = t_lo + threadIdx.x; i < t_hi; i += blockDim.x) want |= ptype(__ldg(pos + i)) == T_FLUID;
-    if (!__syncthreads_or(want)) return;
-    const bool staged = cb_stage(S, a.g, a.cell_start, c, pos);
-    const uint32_t lane = threadIdx.x & 31, hl = lane & 15, warp = threadIdx.x >> 5;
-    for (uint32_t b = t_lo + 2 * warp; b < t_hi; b += 2 * CB_WARPS) {
-        const uint32_t i = b + (lane >> 4);
-        const bool active = i < t_hi;
-        const float4 pi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        f(i, pi, hl, staged, active && ptype(pi) == T_FLUID);
-    }
-}
-
-// Candidates of particle i within re: from the staged block, or (a block too
-// dense to stage) from the coarse cells in global memory; g(j, pj) for each,
-// lanes of the half stepping alike.
-template <class G>
-__device__ __forceinline__ void cb_candidates(const StageArgs& a, const CbShared& S, uint32_t c, const float4& pi,
-                                              float re, uint32_t hl, bool staged, bool go, G g) {
-    if (!go) return;
-    if (staged) {
-        const CbWindow w = cb_window(S, pi, re);
-        cb_walk(S, pi, w, hl, [&](uint32_t e) { g(S.idx[e], S.pos[e]); });
-    } else {
-        const CellNear nr = cell_near(a.g, c, pi.x, pi.y, pi.z, re);
-        for (int row = 0; row < link_rows(a.g); row++) {
-            const RowRange rg = link_row_near(a.g, a.cell_start, c, row, nr);
-            for (uint32_t j = rg.lo + hl; j < rg.hi; j += 16) g(j, __ldg(a.cur.pos + j));
-        }
-    }
-}
-
-// Fast viscosity (the Laplacian of u within rlap, plus the body force) by
-// cell blocks, as k_visc_w2 computes it.
-__global__ void __launch_bounds__(CB_THREADS) k_visc_cb(StageArgs a) {
-    extern __shared__ __align__(16) unsigned char cb_raw[];
-    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
-    const uint32_t c = blockIdx.x;
-    const Phys& P = a.P;
-    const float re = P.rlap, thr = P.rlap_thr;
-    const float4* __restrict__ vel = a.cur.vel;
-    cb_fluid_targets(a, S, c, [&](uint32_t i, const float4& pi, uint32_t hl, bool staged, bool go) {
-        const float4 ui = go ? __ldg(vel + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        float ax = 0.f, ay = 0.f, az = 0.f;
-        cb_candidates(a, S, c, pi, re, hl, staged, go, [&](uint32_t j, const float4& pj) {
-            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            const float rr = dx * dx + dy * dy + dz * dz;
-            if (j != i && rr < thr) {
-                const float wgt = weight_rr<false>(re, rr);
-                const float4 uj = __ldg(vel + j);
-                ax += wgt * (uj.x - ui.x);
-                ay += wgt * (uj.y - ui.y);
-                az += wgt * (uj.z - ui.z);
-            }
-        });
-        ax = half_sum(ax);
-        ay = half_sum(ay);
-        az = half_sum(az);
-        if (go && hl == 0) {
-            const float dt = a.sc->dt;
-            const float gx = a.sc->g_eff[0], gy = a.sc->g_eff[1], gz = a.sc->g_eff[2];
-            float4 t;
-            t.x = ui.x + dt * (P.niu * (P.c_lap * ax) + gx);
-            t.y = ui.y + dt * (P.niu * (P.c_lap * ay) + gy);
-            t.z = ui.z + dt * (P.niu * (P.c_lap * az) + gz);
-            t.w = 0.f;
-            a.tmp[i] = t;
-        }
-    });
-}
-
-// Fast collision by cell blocks, as k_collision_w<false, ...> computes it.
-__global__ void __launch_bounds__(CB_THREADS) k_collision_cb(StageArgs a) {
-    extern __shared__ __align__(16) unsigned char cb_raw[];
-    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
-    const uint32_t c = blockIdx.x;
-    const Phys& P = a.P;
-    const float4* __restrict__ vel = a.cur.vel;
-    cb_fluid_targets(a, S, c, [&](uint32_t i, const float4& pi, uint32_t hl, bool staged, bool go) {
-        const float4 ui = go ? __ldg(vel + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        float cx = 0.f, cy = 0.f, cz = 0.f;
-        cb_candidates(a, S, c, pi, P.col_dis, hl, staged, go, [&](uint32_t j, const float4& pj) {
-            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            const float rr = dx * dx + dy * dy + dz * dz;
-            if (j != i && rr < P.col_thr) {
-                const float ood = rsqrtf(rr), ds = rr * ood;
-                const float4 uj = __ldg(vel + j);
-                const float hx = 0.5f * (uj.x - ui.x), hy = 0.5f * (uj.y - ui.y), hz = 0.5f * (uj.z - ui.z);
-                const float vabs = (hx * dx + hy * dy + hz * dz) * ood;
-                if (ds <= P.col_dis && vabs <= 0.f) {
-                    const float k = P.col_rate * vabs * ood;
-                    cx += k * dx;
-                    cy += k * dy;
-                    cz += k * dz;
-                }
-            }
-        });
-        cx = half_sum(cx);
-        cy = half_sum(cy);
-        cz = half_sum(cz);
-        if (go && hl == 0) a.tmp[i] = make_float4(cx, cy, cz, 0.f);
-    });
-}
-
-// Fast pressure gradient by cell blocks, as k_dash_w<false, ...> computes
-// it: p_hat = the least pressure within r0 (type != 2), then the gradient
-// over the r0 neighbours (type 2 left out in the semi-implicit method).
-__global__ void __launch_bounds__(CB_THREADS) k_dash_cb(StageArgs a) {
-    extern __shared__ __align__(16) unsigned char cb_raw[];
-    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
-    const uint32_t c = blockIdx.x;
-    const Phys& P = a.P;
-    const float* __restrict__ press = a.cur.press;
-    const float re = P.rzero, thr = P.rzero_thr, r02 = P.rzero2;
-    const bool skip_dummy = a.semi != 0;
-    cb_fluid_targets(a, S, c, [&](uint32_t i, const float4& pi, uint32_t hl, bool staged, bool go) {
-        float hat = go ? __ldg(press + i) : 0.f;
-        // r02 >= the threshold's square root radius: walk with the larger of the two
-        const float rw = re * 1.0001f;
-        cb_candidates(a, S, c, pi, rw, hl, staged, go, [&](uint32_t j, const float4& pj) {
-            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            const float rr = dx * dx + dy * dy + dz * dz;
-            if (rr <= r02 && ptype(pj) != T_DUMMY) hat = fminf(hat, __ldg(press + j));
-        });
-        hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, 8));
-        hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, 4));
-        hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, 2));
-        hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, 1));
-        float gx = 0.f, gy = 0.f, gz = 0.f;
-        cb_candidates(a, S, c, pi, re, hl, staged, go, [&](uint32_t j, const float4& pj) {
-            if (j == i || (skip_dummy && ptype(pj) == T_DUMMY)) return;
-            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            const float rr = dx * dx + dy * dy + dz * dz;
-            if (rr < thr) {
-                const float w = weight_rr<false>(re, rr);
-                if (w != 0.f) {
-                    const float k = __fdividef(__ldg(press + j) - hat, rr) * w;
-                    gx += k * dx;
-                    gy += k * dy;
-                    gz += k * dz;
-                }
-            }
-        });
-        gx = half_sum(gx);
-        gy = half_sum(gy);
-        gz = half_sum(gz);
-        if (go && hl == 0) {
-            const float cg = P.dim_f * P.one_over_nzero;
-            const float kk = -a.sc->dt * P.one_over_rho;
-            a.tmp[i] = make_float4(kk * (cg * gx), kk * (cg * gy), kk * (cg * gz), 0.f);
-        }
-    });
-}
-
-static void cb_attr(const void* fn) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_SMEM);
-}
-
 constexpr uint32_t DASH_SLOTS = 64;  // neighbours within r0 kept per particle (~32 on the lattice)
 
 template <bool EX, bool ORD, bool BT>
@@ -971,12 +748,6 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
 // MPS_GPU.cpp:683-717): for a fluid particle,
 //   tmp = u + dt*(nu * c_lap * sum_j w(r; rlap) (u_j - u_i) + g).
 void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (!a.exact && !a.batch.n && a.cell_blocks) {
-        static bool attr = false;
-        if (!attr) { cb_attr((const void*)k_visc_cb); attr = true; }
-        k_visc_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(a);
-        return;
-    }
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const uint32_t nb2 = blocks_for((a.cap_fluid + 1) / 2 * 32u, (uint32_t)a.threads);  // two particles a warp
     const bool ord = a.exact && !a.semi;
@@ -998,12 +769,6 @@ void launch_visc(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // particle, over neighbours of any type with ds <= col_dis that approach
 // (vabs = (0.5 du).dr / ds <= 0): crt += col_rate * vabs / ds * dr.
 void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (!a.exact && !a.batch.n && a.cell_blocks) {
-        static bool attr = false;
-        if (!attr) { cb_attr((const void*)k_collision_cb); attr = true; }
-        k_collision_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(a);
-        return;
-    }
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
     if (a.batch.n) {
@@ -1023,15 +788,6 @@ void launch_collision(const StageArgs& a, uint32_t cap, cudaStream_t st) {
 // equation of state of calPres_expl (MPS_GPU_EXPL.cpp:391-415):
 //   p = max(0, rho c^2 (n - n0) / n0).
 void launch_pnd(const StageArgs& a, int eos, int all_types, uint32_t cap, cudaStream_t st) {
-    if (!a.exact && !a.batch.n && !eos && !all_types && a.cell_blocks) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_pnd_cb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_SMEM);
-            attr = true;
-        }
-        k_pnd_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(a);
-        return;
-    }
     const bool use_list = a.list_solid && !all_types;
     const uint32_t* list = use_list ? a.list_solid : nullptr;
     const uint32_t nb = blocks_for((use_list ? a.cap_solid : cap) * 32u, (uint32_t)a.threads);
@@ -1072,12 +828,6 @@ void launch_dummy_press(const StageArgs& a, const uint32_t* normal_id_of, const 
 // over every type (semi-implicit: type 2 excluded, MPS_CAL_v4.0/MPS_CPU.cpp:384-445),
 // tmp = -dt/rho * grad.
 void launch_dash(const StageArgs& a, uint32_t cap, cudaStream_t st) {
-    if (!a.exact && !a.batch.n && a.cell_blocks) {
-        static bool attr = false;
-        if (!attr) { cb_attr((const void*)k_dash_cb); attr = true; }
-        k_dash_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(a);
-        return;
-    }
     const uint32_t nb = blocks_for((a.list_fluid ? a.cap_fluid : cap) * 32u, (uint32_t)a.threads);
     const bool ord = a.exact && !a.semi;
     if (a.batch.n) {

@@ -36,7 +36,6 @@ struct StageArgs {
     uint32_t cap_solid = 0;
     BatchDev batch;            // scenes of a batch (n == 0: one scene, g and P)
     int threads = 256;         // block size of the particle-stage kernels (autotuned: 64, 128, 256)
-    bool cell_blocks = true;   // fast arithmetic, single scene: the cell-block stencil kernels
 };
 
 // Scene-local view of particle i: its scene, its grid, its cell table (the

@@ -22,7 +22,6 @@
 #include "cellsort.cuh"
 #include "ppe.cuh"
 #include "ppe_device.cuh"
-#include "cellblock.cuh"
 
 namespace mpsb {
 
@@ -137,120 +136,6 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
         A.inv_diag[i] = (float)(1.0 / dg);
         A.b64[i] = b_tmp * (n0 - ni);
         A.x64[i] = (double)a.cur.press[i];
-    }
-}
-
-// The same assembly for the fast arithmetic of a single scene, by cell
-// blocks (cellblock.cuh): one block per coarse cell, half a warp per
-// particle; a row's entries come in sub-cell order instead of ascending
-// index (the fast sums are not in the reference's order anyway).
-__device__ __forceinline__ double half_sum_d(double v) {
-    v += __shfl_xor_sync(0xffffffffu, v, 8);
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    return v;
-}
-
-__global__ void __launch_bounds__(CB_THREADS) k_ppe_assemble_cb(AsmArgs A) {
-    extern __shared__ __align__(16) unsigned char cb_raw[];
-    CbShared& S = *reinterpret_cast<CbShared*>(cb_raw);
-    const StageArgs& a = A.a;
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.bar[0] = 0u;  // the solver's barrier starts empty
-    const uint32_t c = blockIdx.x;
-    const uint32_t t_lo = __ldg(a.cell_start + c), t_hi = __ldg(a.cell_start + c + 1);
-    if (t_lo == t_hi) return;
-    const float4* __restrict__ pos = a.cur.pos;
-    const float* __restrict__ nn = a.cur.n;
-    const double bthr = A.beta * A.n0;
-    float bthr_f = (float)bthr;  // n_j < bthr (double) exactly when n_j < bthr_f
-    if ((double)bthr_f < bthr) bthr_f = nextafterf(bthr_f, INFINITY);
-    // Dirichlet rows (type 2, or n < beta n0) are identity rows
-    bool want = false;
-    for (uint32_t i = t_lo + threadIdx.x; i < t_hi; i += blockDim.x) {
-        const bool dir = ptype(__ldg(pos + i)) == T_DUMMY || (double)__ldg(nn + i) < bthr;
-        if (dir) {
-            A.rlen[i] = PPE_DIRICHLET;
-            A.diag64[i] = 1.0;
-            A.diag32[i] = 1.0f;
-            A.inv_diag[i] = 1.0f;
-            A.b64[i] = 0.0;
-            A.x64[i] = 0.0;
-        }
-        want |= !dir;
-    }
-    if (!__syncthreads_or(want)) return;
-    const bool staged = cb_stage(S, a.g, a.cell_start, c, pos);
-    const double dt = (double)a.sc->dt;
-    const double Aii = A.rho_lambda_alpha_n0 / (A.dim2 * dt * dt);
-    const float re = a.P.rlap, thr = a.P.rlap_thr;
-    const uint32_t lane = threadIdx.x & 31, hl = lane & 15, warp = threadIdx.x >> 5;
-    const uint32_t hmask = 0xffffu << (lane & 16u), lt = ((1u << lane) - 1u) & hmask;
-    for (uint32_t b = t_lo + 2 * warp; b < t_hi; b += 2 * CB_WARPS) {
-        const uint32_t i = b + (lane >> 4);
-        const bool active = i < t_hi;
-        const float4 pi = active ? __ldg(pos + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const double ni = active ? (double)__ldg(nn + i) : 0.0;
-        const bool go = active && ptype(pi) != T_DUMMY && !(ni < bthr);
-        uint32_t count = 0;
-        float diag_lane = 0.f;
-        if (go) {
-            uint32_t* cols = A.cols + (size_t)i * PPE_W;
-            float* wrow = A.wrm + (size_t)i * PPE_W;
-            auto visit = [&](uint32_t j, const float4& pj, bool valid) {
-                bool app = false;
-                float w = 0.f;
-                if (valid && j != i && ptype(pj) != T_DUMMY) {
-                    const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                    const float rr = dx * dx + dy * dy + dz * dz;
-                    if (rr < thr) {
-                        w = weight_rr<false>(re, rr);
-                        if (w > 0.f) app = !(__ldg(nn + j) < bthr_f);
-                    }
-                }
-                diag_lane += w;
-                const uint32_t m = __ballot_sync(hmask, app);
-                if (app) {
-                    const uint32_t k = count + __popc(m & lt);
-                    if (k < PPE_W) {
-                        cols[k] = j;
-                        wrow[k] = w;
-                    }
-                }
-                count += __popc(m);
-            };
-            if (staged) {
-                const CbWindow w = cb_window(S, pi, re);
-                cb_walk_uniform(S, pi, w, hl, [&](uint32_t e, bool valid) {
-                    const uint32_t ee = valid ? e : 0u;
-                    visit(S.idx[ee], S.pos[ee], valid);
-                });
-            } else {
-                const CellNear nr = cell_near(a.g, c, pi.x, pi.y, pi.z, re);
-                for (int row = 0; row < link_rows(a.g); row++) {
-                    const RowRange rg = link_row_near(a.g, a.cell_start, c, row, nr);
-                    for (uint32_t j0 = rg.lo; j0 < rg.hi; j0 += 16) {
-                        const uint32_t j = j0 + hl;
-                        const bool valid = j < rg.hi;
-                        visit(j, valid ? __ldg(pos + j) : pi, valid);
-                    }
-                }
-            }
-        }
-        const double diag = half_sum_d((double)diag_lane);
-        if (go && hl == 0) {
-            if (count > PPE_W) {
-                atomicOr(&a.sc->err, ERR_CAPACITY);
-                count = PPE_W;
-            }
-            const double dg = -diag - Aii;
-            A.rlen[i] = count;
-            A.diag64[i] = dg;
-            A.diag32[i] = (float)dg;
-            A.inv_diag[i] = (float)(1.0 / dg);
-            A.b64[i] = A.b_tmp * (A.n0 - ni);
-            A.x64[i] = (double)a.cur.press[i];
-        }
     }
 }
 
@@ -1712,13 +1597,6 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     if (a.batch.n) {
         if (a.exact) k_ppe_assemble<true, true><<<warps_blocks, 256, 0, st>>>(A);
         else k_ppe_assemble<false, true><<<warps_blocks, 256, 0, st>>>(A);
-    } else if (!a.exact && a.cell_blocks) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_ppe_assemble_cb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_SMEM);
-            attr = true;
-        }
-        k_ppe_assemble_cb<<<a.g.ncells, CB_THREADS, CB_SMEM, st>>>(A);
     } else {
         if (a.exact) k_ppe_assemble<true, false><<<warps_blocks, 256, 0, st>>>(A);
         else k_ppe_assemble<false, false><<<warps_blocks, 256, 0, st>>>(A);

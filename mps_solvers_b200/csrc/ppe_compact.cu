@@ -291,23 +291,32 @@ struct C16Args {
     float* r2;
 };
 
-// Row k of S' x (thread per row; x_j given by a functor of the compact column)
+// Row k of S' x (thread per row; x_j given by a functor of the compact
+// column).  Eight entries at a time: their columns and values are loaded
+// first, then the eight x_j, so a row of ~25 entries costs four rounds of
+// dependent loads instead of one per entry.
 template <class X>
 __device__ __forceinline__ float sp_row(const C16Args& S, uint32_t k, X x) {
     const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
     const uint32_t base = __ldg(S.sp_off + s), W = (__ldg(S.sp_off + s + 1) - base) / SP_SLICE;
-    float a0 = 0.f, a1 = 0.f;
-    uint32_t t = 0;
-    for (; t + 1 < W; t += 2) {
-        const uint32_t c0 = __ldg(S.sp_cols + base + SP_SLICE * t + lane);
-        const uint32_t c1 = __ldg(S.sp_cols + base + SP_SLICE * (t + 1) + lane);
-        const float v0 = __ldg(S.sp_vals + base + SP_SLICE * t + lane);
-        const float v1 = __ldg(S.sp_vals + base + SP_SLICE * (t + 1) + lane);
-        a0 = fmaf(v0, x(c0), a0);
-        a1 = fmaf(v1, x(c1), a1);
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (uint32_t t0 = 0; t0 < W; t0 += 8) {
+        uint32_t c[8];
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const bool ok = t0 + u < W;
+            const size_t at = base + SP_SLICE * (size_t)(t0 + u) + lane;
+            c[u] = ok ? __ldg(S.sp_cols + at) : k;
+            v[u] = ok ? __ldg(S.sp_vals + at) : 0.f;
+        }
+        float xv[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) xv[u] = x(c[u]);
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[u] = fmaf(v[u], xv[u], acc[u]);
     }
-    if (t < W) a0 = fmaf(__ldg(S.sp_vals + base + SP_SLICE * t + lane), x(__ldg(S.sp_cols + base + SP_SLICE * t + lane)), a0);
-    return a0 + a1;
+    return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 }
 
 // The four columns of a lane's chunk entries.

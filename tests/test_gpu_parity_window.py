@@ -146,7 +146,7 @@ def gpu_ppe_pairs(sim):
     return codes, st
 
 
-def _check_pairs(sim, case_dir, tag, ordered=True):
+def _check_pairs(sim, case_dir, tag):
     snap = sim.ppe_snapshot()
     iv = _input_values(case_dir)
     n0 = sim.scalars()["nzero"]
@@ -160,8 +160,6 @@ def _check_pairs(sim, case_dir, tag, ordered=True):
                                  "missing": int(len(missing))})
     assert len(extra) == 0 and len(missing) == 0, (tag, len(extra), len(missing), extra[:5], missing[:5])
     assert np.array_equal(got, want)
-    if not ordered:  # the fast assembly stores a row by sub-cell, not by index
-        return
     # every row's columns ascend (the reference's summation order)
     rs = st["row_start"].astype(np.int64)
     c = st["cols"].astype(np.int64)
@@ -179,7 +177,7 @@ def test_ppe_neighbour_sets_bit_exact_golden(capi, tmp_path, arith):
     with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, arith=mode) as s:
         for k in range(3):
             s.step(2)
-            _check_pairs(s, d, f"golden_{arith}_step{2 * k + 2}", ordered=arith == "exact")
+            _check_pairs(s, d, f"golden_{arith}_step{2 * k + 2}")
 
 
 @pytest.mark.parametrize("arith", ["exact", "fast"])
@@ -191,9 +189,9 @@ def test_ppe_neighbour_sets_bit_exact_full_size(capi, tmp_path, arith):
     mode = capi.ARITH_EXACT if arith == "exact" else capi.ARITH_FAST
     with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, arith=mode) as s:
         s.step(1)
-        _check_pairs(s, d, f"c2_{arith}_step1", ordered=arith == "exact")
+        _check_pairs(s, d, f"c2_{arith}_step1")
         s.step(19)
-        _check_pairs(s, d, f"c2_{arith}_step20", ordered=arith == "exact")
+        _check_pairs(s, d, f"c2_{arith}_step20")
 
 
 def test_semi_dam_break_100_steps_vs_fp64_oracle(capi, oracle_mod, tmp_path):
