@@ -188,7 +188,7 @@ static void mark(mps_handle* h, int tag) {
 // layout).
 static void set_compact(mps_handle* h, bool on) {
     h->ppe.c16 = on && h->ppe.c16_ready;
-    h->ppe.c16_learned = h->ppe.c16 && h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.sp_cols != nullptr;
+    h->ppe.c16_learned = h->ppe.c16 && h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.sp_ent != nullptr;
 }
 
 static bool use_merge(const mps_handle* h) {
@@ -1600,7 +1600,7 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
         const bool learned = h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.lp.ready;
         const int nforms = (learned || h->nscenes) ? 2 : 3;
         // form 3: the compact layout (single scenes, diagonal scaling)
-        const bool compact_ok = h->ppe.c16_ready && !h->nscenes && (!learned || h->ppe.sp_cols != nullptr);
+        const bool compact_ok = h->ppe.c16_ready && !h->nscenes && (!learned || h->ppe.sp_ent != nullptr);
         best = 1e300;
         int best_p = h->ppe.threads;
         bool best_sw = h->ppe.stored_weights, best_pipe = h->ppe.pipelined, best_c16 = h->ppe.c16;

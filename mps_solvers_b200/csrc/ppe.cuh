@@ -108,9 +108,9 @@ struct PpeWork {
     // slices, one product fused into the residual update of every iteration
     bool c16_learned = false;          // the compact solve applies S'
     int precond_every = 10;            // steps between network evaluations
-    uint32_t* sp_off = nullptr;        // first chunk of every slice (widths, then scanned)
-    uint32_t* sp_cols = nullptr;       // 128 compact columns per chunk
-    float* sp_vals = nullptr;          // 128 values per chunk
+    uint32_t* sp_off = nullptr;        // first entry of every 32-row slice (widths, then scanned)
+    uint32_t* sp_ent = nullptr;        // off-diagonal entries: column - row (16 bits) << 16 | BF16 value
+    float* sp_diag = nullptr;          // the diagonal, per compact row
     float* cr2 = nullptr;              // second residual buffer of the fused update
     size_t sp_cap_chunks = 0;
     const uint32_t* index_of_id = nullptr;  // the handle's GEO index -> sorted position

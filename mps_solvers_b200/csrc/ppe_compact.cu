@@ -25,6 +25,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "cellsort.cuh"
 #include "ppe.cuh"
 #include "ppe_device.cuh"
@@ -176,13 +178,15 @@ __global__ void __launch_bounds__(256) k_c16_export(const uint32_t* __restrict__
 
 // ---------------------------------------------------------------- learned S'
 // S' = D^-1/2 S D^-1/2 on the compact rows, S the symmetric form of the
-// learned factor kept by GEO index (learned.cuh): row k holds its diagonal
-// (first) and the stored neighbours that are rows now.  Sliced ELL with a
-// thread per row: slices of 32 consecutive rows, width = the longest row of
-// the slice, entry t of row k at off[k / 32] + 32 t + k % 32 (a warp's loads
-// of one entry index are one 128-byte line), padding = the row itself with
-// value 0.  Applied by the thread that updates the row, so the product needs
-// no more parallelism than the elementwise update.
+// learned factor kept by GEO index (learned.cuh).  Row k: its diagonal in
+// FP32 (sp_diag) and its stored neighbours that are rows now, each as one
+// 32-bit word, (column - k) in the upper 16 bits and the value in BF16 in the
+// lower 16 (S is built diagonally dominant with a 1 % margin, more than BF16
+// rounding takes away, so S' stays SPD).  A pair farther apart than 32,767
+// rows is left out from both its rows, which keeps S' symmetric and
+// dominant.  Sliced ELL with a thread per row: slices of 32 consecutive rows,
+// width = the longest row of the slice, entry t of row k at
+// off[k / 32] + 32 t + k % 32, padding = 0 (the row itself, value 0).
 constexpr uint32_t SP_SLICE = 32;
 
 struct SpArgs {
@@ -199,18 +203,23 @@ struct SpArgs {
     const float* s_diag;
     const Scalars* sc;
     uint32_t* off;             // widths (entries), then the scanned first entries
-    uint32_t* cols;
-    float* vals;
+    uint32_t* ent;
+    float* diag;
     uint32_t maxslices;
 };
 
-__device__ __forceinline__ bool sp_row_now(const SpArgs& A, uint32_t jd, uint32_t np, uint32_t* j) {
+// the stored neighbour jd of compact row k: a row now, close enough to code
+__device__ __forceinline__ bool sp_entry(const SpArgs& A, uint32_t jd, uint32_t np, uint32_t k, uint32_t* j,
+                                         int* delta) {
     const uint32_t jj = __ldg(A.index_of_id + jd);
     *j = jj;
-    return jj < np && __ldg(A.rlen + jj) != PPE_DIRICHLET;
+    if (jj >= np || __ldg(A.rlen + jj) == PPE_DIRICHLET) return false;
+    const int d = (int)__ldg(A.cpos + jj) - (int)k;
+    *delta = d;
+    return d >= -32767 && d <= 32767;
 }
 
-// entries of every 32-row slice (thread per row, warp per slice)
+// off-diagonal entries of every 32-row slice (thread per row, warp per slice)
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,15 +228,19 @@ __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     if (k < R) {
         const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
         const uint32_t n = __ldg(A.s_cnt + id);
-        cnt = 1;  // the diagonal
         for (uint32_t t = 0; t < n; t++) {
             uint32_t j;
-            cnt += sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, &j) ? 1u : 0u;
+            int d;
+            cnt += sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, k, &j, &d) ? 1u : 0u;
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
     if ((threadIdx.x & 31) == 0 && s <= A.maxslices) A.off[s] = cnt * SP_SLICE;
+}
+
+__device__ __forceinline__ uint32_t sp_bf16_bits(float v) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v));
 }
 
 __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
@@ -242,22 +255,18 @@ __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
         const uint32_t id = __ldg(A.idv + i);
         const uint32_t n = __ldg(A.s_cnt + id);
         const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
-        A.cols[base + lane] = k;
-        A.vals[base + lane] = __ldg(A.s_diag + id) * (di * di);
-        t = 1;
+        A.diag[k] = __ldg(A.s_diag + id) * (di * di);
         for (uint32_t u = 0; u < n; u++) {
             uint32_t j;
-            if (!sp_row_now(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, &j)) continue;
+            int d;
+            if (!sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, k, &j, &d)) continue;
             const float dj = (float)(1.0 / sqrt(-__ldg(A.diag64 + j)));
-            A.cols[base + SP_SLICE * t + lane] = __ldg(A.cpos + j);
-            A.vals[base + SP_SLICE * t + lane] = __ldg(A.s_val + (size_t)id * LP_GW + u) * (di * dj);
+            const float v = __ldg(A.s_val + (size_t)id * LP_GW + u) * (di * dj);
+            A.ent[base + SP_SLICE * t + lane] = ((uint32_t)(d & 0xffff) << 16) | sp_bf16_bits(v);
             t++;
         }
     }
-    for (; t < W; t++) {
-        A.cols[base + SP_SLICE * t + lane] = k < R ? k : 0u;
-        A.vals[base + SP_SLICE * t + lane] = 0.f;
-    }
+    for (; t < W; t++) A.ent[base + SP_SLICE * t + lane] = 0u;
 }
 
 // ---------------------------------------------------------------- solve
@@ -286,37 +295,41 @@ struct C16Args {
     int smem_chunks;           // chunks per warp held in shared memory
     // learned S' (LRN): slices of the same 4 rows, the second residual buffer
     const uint32_t* sp_off;
-    const uint32_t* sp_cols;
-    const float* sp_vals;
+    const uint32_t* sp_ent;
+    const float* sp_diag;
     float* r2;
 };
 
 // Row k of S' x (thread per row; x_j given by a functor of the compact
-// column).  Eight entries at a time: their columns and values are loaded
-// first, then the eight x_j, so a row of ~25 entries costs four rounds of
-// dependent loads instead of one per entry.
+// column).  Eight entries a round: their words first, then the eight x_j,
+// so a row of ~25 entries costs four rounds of dependent loads.
+// S' is read every iteration and is small next to the matrix: keep it in L2
+__device__ __forceinline__ uint32_t sp_load(const uint32_t* p, uint64_t pol) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 template <class X>
 __device__ __forceinline__ float sp_row(const C16Args& S, uint32_t k, X x) {
     const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
     const uint32_t base = __ldg(S.sp_off + s), W = (__ldg(S.sp_off + s + 1) - base) / SP_SLICE;
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (uint32_t t0 = 0; t0 < W; t0 += 8) {
-        uint32_t c[8];
-        float v[8];
+        uint32_t e[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const bool ok = t0 + u < W;
-            const size_t at = base + SP_SLICE * (size_t)(t0 + u) + lane;
-            c[u] = ok ? __ldg(S.sp_cols + at) : k;
-            v[u] = ok ? __ldg(S.sp_vals + at) : 0.f;
-        }
+        for (int u = 0; u < 8; u++)
+            e[u] = t0 + u < W ? sp_load(S.sp_ent + base + SP_SLICE * (size_t)(t0 + u) + lane, pol) : 0u;
         float xv[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) xv[u] = x(c[u]);
+        for (int u = 0; u < 8; u++) xv[u] = x((uint32_t)((int)k + ((int)e[u] >> 16)));
 #pragma unroll
-        for (int u = 0; u < 8; u++) acc[u] = fmaf(v[u], xv[u], acc[u]);
+        for (int u = 0; u < 8; u++) acc[u] = fmaf(__uint_as_float(e[u] << 16), xv[u], acc[u]);
     }
-    return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    const float off = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    return fmaf(__ldg(S.sp_diag + k), x(k), off);
 }
 
 // The four columns of a lane's chunk entries.
@@ -630,7 +643,7 @@ int ppe_c16_enable(PpeWork& w, std::string* err) {
 
 void ppe_c16_free(PpeWork& w) {
     void* ps[] = {w.cpos, w.c16_width, w.c16_codes, w.c16_w, w.c16_side, w.c16_esc, w.cb64, w.cx64, w.cdiag64,
-                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1], w.sp_off, w.sp_cols, w.sp_vals, w.cr2};
+                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1], w.sp_off, w.sp_ent, w.sp_diag, w.cr2};
     for (void* p : ps)
         if (p) cudaFree(p);
     w.cpos = w.c16_width = w.c16_esc = nullptr;
@@ -641,8 +654,8 @@ void ppe_c16_free(PpeWork& w) {
     w.cdiag32 = w.cinv_diag = w.cr = w.cq = nullptr;
     w.czp[0] = w.czp[1] = nullptr;
     w.sp_off = nullptr;
-    w.sp_cols = nullptr;
-    w.sp_vals = nullptr;
+    w.sp_ent = nullptr;
+    w.sp_diag = nullptr;
     w.cr2 = nullptr;
     w.c16_ready = false;
     w.c16 = false;
@@ -698,8 +711,8 @@ int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt
     S.smem_chunks = chunks;
     const size_t smem = c16_smem_bytes(w.threads, chunks);
     S.sp_off = w.sp_off;
-    S.sp_cols = w.sp_cols;
-    S.sp_vals = w.sp_vals;
+    S.sp_ent = w.sp_ent;
+    S.sp_diag = w.sp_diag;
     S.r2 = w.cr2;
     void* args[] = {&S};
     const bool lrn = w.c16_learned;
@@ -716,12 +729,12 @@ int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
         if (err) *err = "cudaMalloc failed for the learned symmetric form";
         return MPS_ERR_CUDA;
     }
-    if (w.sp_cols) return MPS_OK;
+    if (w.sp_ent) return MPS_OK;
     const size_t slices = (w.cap + SP_SLICE - 1) / SP_SLICE + 2;
     w.sp_cap_chunks = slices * (LP_GW + 1);  // entries per lane position: 32-row slices of up to LP_GW + 1
     bool ok = c16_alloc(&w.sp_off, slices + 2);
-    ok &= c16_alloc(&w.sp_cols, w.sp_cap_chunks * SP_SLICE);
-    ok &= c16_alloc(&w.sp_vals, w.sp_cap_chunks * SP_SLICE);
+    ok &= c16_alloc(&w.sp_ent, w.sp_cap_chunks * SP_SLICE);
+    ok &= c16_alloc(&w.sp_diag, (size_t)w.cap + 8);
     ok &= c16_alloc(&w.cr2, (size_t)w.cap + 8);
     if (!ok) {
         if (err) *err = "cudaMalloc failed for the learned compact preconditioner";
@@ -746,8 +759,8 @@ int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, c
     A.s_diag = w.lp.s_diag;
     A.sc = a.sc;
     A.off = w.sp_off;
-    A.cols = w.sp_cols;
-    A.vals = w.sp_vals;
+    A.ent = w.sp_ent;
+    A.diag = w.sp_diag;
     const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
     k_sp_width<<<cblocks((maxslices + 1) * SP_SLICE, 256), 256, 0, st>>>(A);

@@ -42,12 +42,36 @@ def test_headline_kernels_have_traffic():
     assert bench._traffic_from_profiles("visc", "explicit") > 0
 
 
+def _ncu_commands(text):
+    # a command continued with backslashes is one line
+    return [ln.strip() for ln in text.replace("\\\n", " ").splitlines() if ln.strip().startswith("ncu ")]
+
+
 def test_every_summary_gives_its_ncu_command():
     files = _summaries()
     assert files
     for f in files:
         text = open(f).read()
         assert "ncu " in text, f
-        for line in text.replace("\\\n", " ").splitlines():  # a command continued with backslashes
-            if line.strip().startswith("ncu "):
-                assert "--clock-control none" in line, (f, line)
+        for line in _ncu_commands(text):
+            assert "--clock-control none" in line, (f, line)
+
+
+def test_multi_pass_captures_are_one_kernel_on_a_small_case():
+    """A capture that collects more than gpu__time_duration.sum replays each
+    launch many times: it must select one kernel (-k without alternatives),
+    at most three launches (-c), and a small case (the ~110k-particle tank,
+    the 70,912-particle explicit scene, or the 8-scene batch)."""
+    import re
+    for f in _summaries():
+        for line in _ncu_commands(open(f).read()):
+            metrics = re.findall(r"--metrics\s+(\S+)", line)
+            one_pass = not re.search(r"--set|--section", line) and all(
+                m == "gpu__time_duration.sum" for m in metrics)
+            if one_pass:
+                continue
+            k = re.search(r"-k\s+(\S+)", line)
+            assert k and "|" not in k.group(1), (f, "one kernel per capture", line)
+            c = re.search(r"-c\s+(\d+)", line)
+            assert c and int(c.group(1)) <= 3, (f, "at most three launches", line)
+            assert "--size small" in line or "--workload explicit" in line, (f, "a small case", line)
