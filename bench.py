@@ -409,7 +409,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     else:
         alg_bytes = STAGE_BYTES[dom] * n
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
-    traffic = _traffic_from_profiles("pressure" if dom == "ppe_solve" else dom, args.workload)
+    # the committed traffic figures are for the full-size workloads
+    traffic = (_traffic_from_profiles("pressure" if dom == "ppe_solve" else dom, args.workload)
+               if args.size == "full" else None)
     # FP32 pipe (the secondary roofline of the stencil stages): pair
     # evaluations of the fixed model, |{j: r_ij < re}| x FLOP per pair (PND 10
     # over all particles at r0; viscosity 16 at rlap, collision 20 and
