@@ -148,11 +148,18 @@ typedef struct {
 typedef struct mps_handle mps_handle;
 
 /* Grid of the reference's cell list (MPS::allocateCellList,
- * MPS_CAL_expl_v1.0/MPS.cpp:567-642). */
+ * MPS_CAL_expl_v1.0/MPS.cpp:567-642).  cell_yz is the cell edge along y and
+ * z; 0 (or cell_size) is the reference's cubic cell.  A handle created with
+ * MPS_ARITH_FAST in 3-D sorts by the reference's grid with its cells halved
+ * along y and z (cell_yz = cell_size / 2, cdy and cdz doubled), which its
+ * stencil walks scan with fewer candidates; mps_get_grid and
+ * mps_get_cell_tables report that grid.  Exact arithmetic keeps the
+ * reference's grid. */
 typedef struct {
     float left, back, bottom, cell_size;
     uint32_t cdx, cdy, cdz, ncells;
     int dim;
+    float cell_yz;
 } mps_grid;
 
 const char* mps_status_string(mps_status s);

@@ -71,7 +71,7 @@ class mps_step_stats(C.Structure):
 class mps_grid(C.Structure):
     _fields_ = [("left", C.c_float), ("back", C.c_float), ("bottom", C.c_float),
                 ("cell_size", C.c_float), ("cdx", C.c_uint32), ("cdy", C.c_uint32),
-                ("cdz", C.c_uint32), ("ncells", C.c_uint32), ("dim", C.c_int)]
+                ("cdz", C.c_uint32), ("ncells", C.c_uint32), ("dim", C.c_int), ("cell_yz", C.c_float)]
 
 
 class mps_scene_spec(C.Structure):

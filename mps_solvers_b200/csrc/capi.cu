@@ -33,7 +33,7 @@ struct mps_handle {
     Phys P{};
     uint32_t np0 = 0, nb2 = 0, nb1 = 0, cap = 0;
     int passes = 1;
-    int normal_reach = 1;
+    int normal_reach = 1, normal_reach_yz = 1;
     // device memory
     State S[2]{};
     int cur = 0;
@@ -377,6 +377,11 @@ static cudaError_t merge_setup(mps_handle* h) {
     return cudaSuccess;
 }
 
+// cell rows on each side along y and z that cover one cell_size
+static int walk_reach(float cell_size, float cell_yz) {
+    return cell_yz < cell_size ? (int)std::ceil((double)cell_size / (double)cell_yz - 1e-9) : 1;
+}
+
 static Grid device_grid(const HostGrid& hg, uint32_t base) {
     Grid g;
     g.left = hg.left;
@@ -390,7 +395,18 @@ static Grid device_grid(const HostGrid& hg, uint32_t base) {
     g.ncells = hg.ncells;
     g.dim = hg.dim;
     g.base = base;
+    g.cell_yz = hg.cell_yz;
+    g.reach = walk_reach(hg.cell_size, hg.cell_yz);
     return g;
+}
+
+// cells along x and along y/z that cover sqrt(2) r0 (the dummy-to-wall search)
+static void normal_reaches(double rzero, const HostGrid& hg, int* rx, int* ryz) {
+    const double need = std::sqrt(2.0) * rzero;
+    const int a = (int)std::ceil(need / (double)hg.cell_size - 1e-12);
+    const int b = (int)std::ceil(need / (double)hg.cell_yz - 1e-12);
+    *rx = a > *rx ? a : *rx;
+    *ryz = b > *ryz ? b : *ryz;
 }
 
 static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint32_t nb2, uint32_t nb1,
@@ -407,25 +423,12 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     CK(cudaEventCreate(&h->ev1));
     int st = make_grid(prm, pos3, np, &h->hg, &h->err);
     if (st != MPS_OK) return (mps_status)st;
-    Grid& g = h->g;
-    g.left = h->hg.left;
-    g.back = h->hg.back;
-    g.bottom = h->hg.bottom;
-    g.cell_size = h->hg.cell_size;
-    g.cdx = h->hg.cdx;
-    g.cdy = h->hg.cdy;
-    g.cdz = h->hg.cdz;
-    g.sheet = h->hg.sheet;
-    g.ncells = h->hg.ncells;
-    g.dim = h->hg.dim;
-    g.base = 0;
+    if (h->opt.arith == MPS_ARITH_FAST) refine_grid_yz(&h->hg);
+    h->g = device_grid(h->hg, 0);
+    const Grid& g = h->g;
     h->passes = sort_passes(g.ncells);
-    // reach (in cells) that covers sqrt(2) r0 for the dummy-to-wall search
-    {
-        double need = std::sqrt(2.0) * (double)prm.rzero;
-        int r = (int)std::ceil(need / (double)g.cell_size - 1e-12);
-        h->normal_reach = r < 1 ? 1 : r;
-    }
+    h->normal_reach = h->normal_reach_yz = 1;
+    normal_reaches(prm.rzero, h->hg, &h->normal_reach, &h->normal_reach_yz);
 
     const uint32_t cap = h->cap;
     for (int b = 0; b < 2; b++) {
@@ -507,7 +510,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         StageArgs a = stage_args(h);
         launch_pnd64(a, n64, h->cap, h->stream);
         launch_n0_lambda64(a, n64, res, h->stream);
-        launch_normals(a, h->normal_reach, h->normal_id_of, h->cap, h->stream);
+        launch_normals(a, h->normal_reach, h->normal_reach_yz, h->normal_id_of, h->cap, h->stream);
         double hr[2] = {0, 0};
         CK(cudaMemcpyAsync(hr, res, sizeof hr, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -524,7 +527,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         launch_pnd(a, 0, 1, h->cap, h->stream);  // n of every particle
         launch_nzero(h->S[h->cur].n, h->sc, h->best, h->cap, h->stream);
         launch_lambda(a, h->best, h->lambda_dev, h->stream);
-        launch_normals(a, h->normal_reach, h->normal_id_of, h->cap, h->stream);
+        launch_normals(a, h->normal_reach, h->normal_reach_yz, h->normal_id_of, h->cap, h->stream);
         unsigned long long best = 0;
         float lam = 0.f;
         CK(cudaMemcpyAsync(&best, h->best, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -676,7 +679,7 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
     CK(cudaEventCreate(&h->ev1));
     // per-scene grids in one cell space
     uint64_t cells = 0;
-    int reach = 1;
+    int reach = 1, reach_yz = 1;
     for (uint32_t s = 0; s < S; s++) {
         HostGrid hg;
         int st = make_grid(prms[s], geos[s].pos.data(), geos[s].np, &hg, &h->err);
@@ -684,12 +687,11 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
             h->err = "scene " + std::to_string(s) + ": " + h->err;
             return (mps_status)st;
         }
+        if (h->opt.arith == MPS_ARITH_FAST) refine_grid_yz(&hg);
         if (s == 0) h->hg = hg;
         h->scene_grid.push_back(device_grid(hg, (uint32_t)cells));
         cells += hg.ncells;
-        const double need = std::sqrt(2.0) * (double)prms[s].rzero;
-        const int r = (int)std::ceil(need / (double)hg.cell_size - 1e-12);
-        reach = r > reach ? r : reach;
+        normal_reaches(prms[s].rzero, hg, &reach, &reach_yz);
     }
     if (cells >= 0xffffffffull) {
         h->err = "too many cells in the batch";
@@ -700,6 +702,7 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
     h->g.base = 0;
     h->passes = sort_passes(h->g.ncells);
     h->normal_reach = reach;
+    h->normal_reach_yz = reach_yz;
 
     const uint32_t cap = h->cap;
     for (int b = 0; b < 2; b++) {
@@ -865,7 +868,7 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
             apply_constants(h->scene_phys[s], c);
         }
     }
-    launch_normals(a, h->normal_reach, h->normal_id_of, cap, h->stream);
+    launch_normals(a, h->normal_reach, h->normal_reach_yz, h->normal_id_of, cap, h->stream);
     CK(cudaMemcpyAsync(h->phys_dev, h->scene_phys.data(), S * sizeof(Phys), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->P = h->scene_phys[0];
@@ -1308,6 +1311,7 @@ extern "C" mps_status mps_get_grid(mps_handle* h, mps_grid* g) {
     g->cdz = h->g.cdz;
     g->ncells = h->g.ncells;
     g->dim = h->g.dim;
+    g->cell_yz = h->g.cell_yz;
     return MPS_OK;
 }
 
@@ -1886,6 +1890,9 @@ extern "C" mps_status mps_cell_sort_dev(const float* pos4_dev, uint32_t n, const
     g.sheet = gg->cdx * gg->cdy;
     g.ncells = gg->ncells;
     g.dim = gg->dim;
+    g.cell_yz = gg->cell_yz > 0.f ? gg->cell_yz : gg->cell_size;
+    g.reach = walk_reach(g.cell_size, g.cell_yz);
+    g.base = 0;
     const uint32_t tiles = sort_tiles(n > 0 ? n : 1);
     SortScratch s;
     s.tiles = tiles;

@@ -142,7 +142,21 @@ int make_grid(const mps_params& p, const float* pos3, uint32_t np, HostGrid* out
     out->sheet = cdx * cdy;
     out->ncells = (uint32_t)ncells;
     out->dim = p.dim;
+    out->cell_yz = cell_size;
     return MPS_OK;
+}
+
+bool refine_grid_yz(HostGrid* g) {
+    if (g->dim != 3) return false;
+    const uint64_t cdy = 2ull * g->cdy, cdz = 2ull * g->cdz;
+    const uint64_t ncells = (uint64_t)g->cdx * cdy * cdz;
+    if (ncells >= 0x7fffffffull) return false;
+    g->cell_yz = 0.5f * g->cell_size;  // exact: same faces as the reference's cells, plus the midplanes
+    g->cdy = (uint32_t)cdy;
+    g->cdz = (uint32_t)cdz;
+    g->sheet = g->cdx * g->cdy;
+    g->ncells = (uint32_t)ncells;
+    return true;
 }
 
 // MPS::calOnce constants (MPS_CAL_expl_v1.0/MPS.cpp:515-529) from n0, lambda.

@@ -94,14 +94,11 @@ __global__ void __launch_bounds__(256) k_lp_stencil(LpSystem S, uint32_t* __rest
     const float r02 = r0 * r0;
     uint32_t cnt = 0, low = 0;
     uint32_t* out = scols + (size_t)i * LP_GW;
-    const int rows = link_rows(g);
     const CellNear nr = cell_near(g, c, pi.x, pi.y, pi.z, r0);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(g, cs, c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    auto visit = [&](uint32_t j, bool in) {
+        {
             bool hit = false;
-            if (j < rg.hi && j != i && __ldg(S.rlen + j) != PPE_DIRICHLET) {
+            if (in && j != i && __ldg(S.rlen + j) != PPE_DIRICHLET) {
                 const float4 pj = __ldg(S.pos + j);
                 const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
                 hit = dx * dx + dy * dy + dz * dz < r02;
@@ -114,7 +111,9 @@ __global__ void __launch_bounds__(256) k_lp_stencil(LpSystem S, uint32_t* __rest
             cnt += __popc(m);
             low += __popc(__ballot_sync(0xffffffffu, hit && j < i));
         }
-    }
+    };
+    if (g.reach > 1) walk_cells<true>(g, cs, c, nr, lane, visit);
+    else walk_cells<false>(g, cs, c, nr, lane, visit);
     if (lane == 0) {
         if (cnt > LP_GW) {
             atomicOr(&sc->err, ERR_CAPACITY);

@@ -6,11 +6,19 @@
 namespace mpsb {
 
 // Cell grid of the reference's cell list (MPS_CAL_expl_v1.0/MPS.cpp:567-642).
+// The fast-arithmetic 3-D path halves the cells along y and z (cell_yz =
+// cell_size / 2, twice the cells along y and z, reach 2): a walk then visits
+// up to 25 rows of 3 half-height cells instead of 9 rows of 3 cells, and on
+// a dam-break state the culled walk holds about 35 % fewer candidates for the
+// rlap stencil and half as many for r0.  The reference's grid has cell_yz =
+// cell_size and reach 1.
 struct Grid {
     float left, back, bottom, cell_size;
     uint32_t cdx, cdy, cdz, sheet, ncells;
     int dim;
     uint32_t base;  // first global cell id of this grid (scenes of a batch; 0 otherwise)
+    float cell_yz;  // cell edge along y and z (cell_size along x)
+    int reach;      // cell rows walked on each side along y and z to cover cell_size
 };
 
 // Per-scene constants, fixed after initialisation.
@@ -133,8 +141,8 @@ __device__ __forceinline__ uint32_t cell_of_pos(const Grid& g, float x, float y,
         return g.ncells;
     }
     uint32_t cx = (uint32_t)(long long)__fdiv_rn(__fsub_rn(x, g.left), g.cell_size);
-    uint32_t cy = (uint32_t)(long long)__fdiv_rn(__fsub_rn(y, g.back), g.cell_size);
-    uint32_t cz = (uint32_t)(long long)__fdiv_rn(__fsub_rn(z, g.bottom), g.cell_size);
+    uint32_t cy = (uint32_t)(long long)__fdiv_rn(__fsub_rn(y, g.back), g.cell_yz);
+    uint32_t cz = (uint32_t)(long long)__fdiv_rn(__fsub_rn(z, g.bottom), g.cell_yz);
     if (cx >= g.cdx || cy >= g.cdy || cz >= g.cdz) return g.ncells;
     return cz * g.sheet + cy * g.cdx + cx;
 }
@@ -145,14 +153,21 @@ __device__ __forceinline__ uint32_t cell_of_pos(const Grid& g, float x, float y,
 // its id (with unsigned wrap) is below ncells, exactly the reference's test.
 // The kept cells are consecutive, so their particles are one index range;
 // rows come in the reference's order, so visiting rows in order and indices
-// ascending reproduces the reference's summation order.
+// ascending reproduces the reference's summation order.  On a grid with
+// reach 2 the rows run over dz, dy in [-2, 2] in the same order (25 rows),
+// and the candidates still come in ascending index order.
 struct RowRange { uint32_t lo, hi; };
+
+__device__ __forceinline__ void row_offsets(const Grid& g, int row, int* dz, int* dy) {
+    const int w = 2 * g.reach + 1;
+    if (g.dim == 3) { *dz = row / w - g.reach; *dy = row % w - g.reach; }
+    else { *dz = 0; *dy = row - g.reach; }
+}
 
 __device__ __forceinline__ RowRange link_row(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
                                              int row) {
     int dz, dy;
-    if (g.dim == 3) { dz = row / 3 - 1; dy = row % 3 - 1; }
-    else { dz = 0; dy = row - 1; }
+    row_offsets(g, row, &dz, &dy);
     uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
     uint32_t a = c0 - 1u, b = c0 + 1u;
     bool va = a < g.ncells, v0 = c0 < g.ncells, vb = b < g.ncells;
@@ -165,7 +180,10 @@ __device__ __forceinline__ RowRange link_row(const Grid& g, const uint32_t* __re
     return r;
 }
 
-__device__ __forceinline__ int link_rows(const Grid& g) { return g.dim == 3 ? 9 : 3; }
+__device__ __forceinline__ int link_rows(const Grid& g) {
+    const int w = 2 * g.reach + 1;
+    return g.dim == 3 ? w * w : w;
+}
 
 // Culling of the linked cells: the distances from a particle to the faces of
 // its own cell bound the distance to any particle of a neighbouring cell.  A
@@ -177,37 +195,38 @@ __device__ __forceinline__ int link_rows(const Grid& g) { return g.dim == 3 ? 9 
 struct CellNear {
     float xl, xr, yl, yr, zl, zr;  // to the low / high face along each axis
     float re2;                     // (re + margin)^2
+    float hyz;                     // cell edge along y and z (rows beyond the first)
 };
 
 __device__ __forceinline__ CellNear cell_near(const Grid& g, uint32_t c, float x, float y, float z, float re) {
     const uint32_t cz = c / g.sheet, rem = c - cz * g.sheet;
     const uint32_t cy = rem / g.cdx, cx = rem - cy * g.cdx;
     const float x0 = g.left + g.cell_size * (float)cx;
-    const float y0 = g.back + g.cell_size * (float)cy;
-    const float z0 = g.bottom + g.cell_size * (float)cz;
+    const float y0 = g.back + g.cell_yz * (float)cy;
+    const float z0 = g.bottom + g.cell_yz * (float)cz;
     CellNear n;
     n.xl = fmaxf(x - x0, 0.f);
     n.xr = fmaxf(x0 + g.cell_size - x, 0.f);
     n.yl = fmaxf(y - y0, 0.f);
-    n.yr = fmaxf(y0 + g.cell_size - y, 0.f);
+    n.yr = fmaxf(y0 + g.cell_yz - y, 0.f);
     n.zl = fmaxf(z - z0, 0.f);
-    n.zr = fmaxf(z0 + g.cell_size - z, 0.f);
+    n.zr = fmaxf(z0 + g.cell_yz - z, 0.f);
     const float r = re + 1e-4f * g.cell_size;
     n.re2 = r * r;
+    n.hyz = g.cell_yz;
     return n;
 }
 
 // link_row restricted to the cells that can hold a particle within re
-__device__ __forceinline__ RowRange link_row_near(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
-                                                  int row, const CellNear& n) {
-    int dz, dy;
-    if (g.dim == 3) { dz = row / 3 - 1; dy = row % 3 - 1; }
-    else { dz = 0; dy = row - 1; }
+// row (dz, dy) of the walk
+__device__ __forceinline__ RowRange link_row_near_at(const Grid& g, const uint32_t* __restrict__ cell_start,
+                                                     uint32_t c, int dz, int dy, const CellNear& n) {
+    // distance to the row: the face of the own cell plus the whole cells between
     float d2 = 0.f;
-    if (dy < 0) d2 += n.yl * n.yl;
-    else if (dy > 0) d2 += n.yr * n.yr;
-    if (dz < 0) d2 += n.zl * n.zl;
-    else if (dz > 0) d2 += n.zr * n.zr;
+    if (dy < 0) { const float t = fmaf(n.hyz, (float)(-dy - 1), n.yl); d2 += t * t; }
+    else if (dy > 0) { const float t = fmaf(n.hyz, (float)(dy - 1), n.yr); d2 += t * t; }
+    if (dz < 0) { const float t = fmaf(n.hyz, (float)(-dz - 1), n.zl); d2 += t * t; }
+    else if (dz > 0) { const float t = fmaf(n.hyz, (float)(dz - 1), n.zr); d2 += t * t; }
     RowRange r{0u, 0u};
     if (d2 >= n.re2) return r;
     const bool wa = d2 + n.xl * n.xl < n.re2, wb = d2 + n.xr * n.xr < n.re2;
@@ -220,6 +239,86 @@ __device__ __forceinline__ RowRange link_row_near(const Grid& g, const uint32_t*
     r.lo = __ldg(cell_start + first);
     r.hi = __ldg(cell_start + last + 1u);
     return r;
+}
+
+__device__ __forceinline__ RowRange link_row_near(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
+                                                  int row, const CellNear& n) {
+    int dz, dy;
+    row_offsets(g, row, &dz, &dy);
+    return link_row_near_at(g, cell_start, c, dz, dy, n);
+}
+
+// A warp's walk over all its rows as one list of candidates.  Lane r looks
+// up row r (link_row_near; at most 25 rows, so one lookup per lane, all in
+// parallel), an inclusive scan of the row lengths numbers the candidates of
+// all rows in walk order (rows in order, indices ascending within a row),
+// and candidate f of that numbering is fetched with a 5-step search over the
+// lanes' row ends.  Every 32 consecutive candidates fill one batch of the
+// warp, whichever rows they come from, in the same order as the row-by-row
+// walk: ordered sums over the batches add the same terms in the same order.
+struct FlatWalk {
+    uint32_t total;  // candidates over all rows
+    uint32_t end;    // this lane's row: one past its last candidate in walk order (total past the rows)
+    int base;        // this lane's row: particle index minus walk position
+};
+
+__device__ __forceinline__ FlatWalk flat_walk_of(RowRange rg, uint32_t lane) {
+    const uint32_t len = rg.hi - rg.lo;
+    uint32_t e = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, e, o);
+        if ((int)lane >= o) e += t;
+    }
+    FlatWalk w;
+    w.total = __shfl_sync(0xffffffffu, e, 31);
+    w.end = e;
+    w.base = (int)rg.lo - (int)(e - len);
+    return w;
+}
+
+__device__ __forceinline__ FlatWalk flat_walk(const Grid& g, const uint32_t* __restrict__ cell_start, uint32_t c,
+                                              const CellNear& n, uint32_t lane) {
+    RowRange rg{0u, 0u};
+    if ((int)lane < link_rows(g)) rg = link_row_near(g, cell_start, c, (int)lane, n);
+    return flat_walk_of(rg, lane);
+}
+
+// the particle index of candidate f (f < total; every lane calls it)
+__device__ __forceinline__ uint32_t flat_at(const FlatWalk& w, uint32_t f) {
+    int r = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t e = __shfl_sync(0xffffffffu, w.end, r + step - 1);
+        if (e <= f) r += step;
+    }
+    return (uint32_t)((int)f + __shfl_sync(0xffffffffu, w.base, r));
+}
+
+// body(j, in) for each batch of 32 candidates of a warp's walk, in walk
+// order (lane L gets the batch's L-th candidate; `in` is false past the
+// end).  FLAT walks the rows as one list (flat_walk: the rows' lookups in
+// parallel, full batches), the other form row by row; both visit the same
+// candidates in the same order.  The flat form pays on the refined grid (up
+// to 25 short rows); on the reference's grid (9 rows of about 200
+// candidates) the row form is as fast and is what the exact kernels use.
+template <bool FLAT, class F>
+__device__ __forceinline__ void walk_cells(const Grid& g, const uint32_t* __restrict__ cs, uint32_t c,
+                                           const CellNear& nr, uint32_t lane, F&& body) {
+    if (FLAT) {
+        const FlatWalk fw = flat_walk(g, cs, c, nr, lane);
+        for (uint32_t f0 = 0; f0 < fw.total; f0 += 32) {
+            const bool in = f0 + lane < fw.total;
+            body(flat_at(fw, in ? f0 + lane : fw.total - 1), in);
+        }
+    } else {
+        const int R = g.reach, nz = g.dim == 3 ? R : 0;
+        for (int dz = -nz; dz <= nz; dz++)
+            for (int dy = -R; dy <= R; dy++) {
+                const RowRange rg = link_row_near_at(g, cs, c, dz, dy, nr);
+                for (uint32_t base = rg.lo; base < rg.hi; base += 32) body(base + lane, base + lane < rg.hi);
+            }
+    }
 }
 
 }  // namespace mpsb

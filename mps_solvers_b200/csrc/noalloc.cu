@@ -94,6 +94,9 @@ extern "C" mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t 
     g.sheet = gg->cdx * gg->cdy;
     g.ncells = gg->ncells;
     g.dim = gg->dim;
+    g.base = 0;
+    g.cell_yz = gg->cell_yz > 0.f ? gg->cell_yz : gg->cell_size;
+    g.reach = 1;  // the sort reads only the cell edges
     SortScratch s;
     s.tiles = sort_tiles(n > 0 ? n : 1);
     s.keys[0] = base + kKeys0;

@@ -412,15 +412,12 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
     const float re = P.rlap, thr = P.rlap_thr;
     float ax = 0.f, ay = 0.f, az = 0.f;
     float4* obuf = ordered_buf();
-    const int rows = link_rows(L.g);
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             float tx = 0.f, ty = 0.f, tz = 0.f;
             bool hit = false;
-            if (j < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
@@ -438,7 +435,7 @@ __global__ void __launch_bounds__(256) k_visc_w(StageArgs a, const uint32_t* __r
             if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, ax, ay, az);
             else { ax += tx; ay += ty; az += tz; }
         }
-    }
+    });
     if (!ORD) { ax = warp_tree_add(ax); ay = warp_tree_add(ay); az = warp_tree_add(az); }
     if (lane != 0) return;
     const float dt = dt_of<BT>(a, L.s);
@@ -499,19 +496,41 @@ __global__ void __launch_bounds__(256) k_visc_w2(StageArgs a, const uint32_t* __
         }
     };
     if (shared) {
-        for (int row = 0; row < rows; row++) {
-            const RowRange r1 = link_row_near(L1.g, L1.cs, L1.c, row, n1);
-            const RowRange r2 = link_row_near(L1.g, L1.cs, L1.c, row, n2);
-            const uint32_t lo = r1.hi > r1.lo ? (r2.hi > r2.lo ? min(r1.lo, r2.lo) : r1.lo) : r2.lo;
-            const uint32_t hi = r1.hi > r1.lo ? (r2.hi > r2.lo ? max(r1.hi, r2.hi) : r1.hi) : r2.hi;
-            for (uint32_t base = lo; base < hi; base += 32) {
-                const uint32_t j = base + lane;
-                if (j < hi) {
-                    const float4 pj = __ldg(pos + j), uj = __ldg(vel + j);
-                    pair(p1, u1, i1, j, pj, uj, a1x, a1y, a1z);
-                    pair(p2, u2, i2, j, pj, uj, a2x, a2y, a2z);
-                }
+        auto both = [&](uint32_t j, bool in) {
+            if (in) {
+                const float4 pj = __ldg(pos + j), uj = __ldg(vel + j);
+                pair(p1, u1, i1, j, pj, uj, a1x, a1y, a1z);
+                pair(p2, u2, i2, j, pj, uj, a2x, a2y, a2z);
             }
+        };
+        // per row, the union of the two particles' culled ranges
+        auto union_row = [&](int dz, int dy) {
+            const RowRange r1 = link_row_near_at(L1.g, L1.cs, L1.c, dz, dy, n1);
+            const RowRange r2 = link_row_near_at(L1.g, L1.cs, L1.c, dz, dy, n2);
+            RowRange ru;
+            ru.lo = r1.hi > r1.lo ? (r2.hi > r2.lo ? min(r1.lo, r2.lo) : r1.lo) : r2.lo;
+            ru.hi = r1.hi > r1.lo ? (r2.hi > r2.lo ? max(r1.hi, r2.hi) : r1.hi) : r2.hi;
+            return ru;
+        };
+        if (L1.g.reach > 1) {  // the refined grid: all rows as one list
+            RowRange ru{0u, 0u};
+            if ((int)lane < rows) {
+                int dz, dy;
+                row_offsets(L1.g, (int)lane, &dz, &dy);
+                ru = union_row(dz, dy);
+            }
+            const FlatWalk fw = flat_walk_of(ru, lane);
+            for (uint32_t f0 = 0; f0 < fw.total; f0 += 32) {
+                const bool in = f0 + lane < fw.total;
+                both(flat_at(fw, in ? f0 + lane : fw.total - 1), in);
+            }
+        } else {
+            const int R = L1.g.reach, nz = L1.g.dim == 3 ? R : 0;
+            for (int dz = -nz; dz <= nz; dz++)
+                for (int dy = -R; dy <= R; dy++) {
+                    const RowRange ru = union_row(dz, dy);
+                    for (uint32_t base = ru.lo; base < ru.hi; base += 32) both(base + lane, base + lane < ru.hi);
+                }
         }
     } else {
         for (int k = 0; k < (two ? 2 : 1); k++) {
@@ -520,13 +539,11 @@ __global__ void __launch_bounds__(256) k_visc_w2(StageArgs a, const uint32_t* __
             const float4 pi = k ? p2 : p1, ui = k ? u2 : u1;
             const uint32_t i = k ? i2 : i1;
             float &ax = k ? a2x : a1x, &ay = k ? a2y : a1y, &az = k ? a2z : a1z;
-            for (int row = 0; row < rows; row++) {
-                const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-                for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-                    const uint32_t j = base + lane;
-                    if (j < rg.hi) pair(pi, ui, i, j, __ldg(pos + j), __ldg(vel + j), ax, ay, az);
-                }
-            }
+            auto one = [&](uint32_t j, bool in) {
+                if (in) pair(pi, ui, i, j, __ldg(pos + j), __ldg(vel + j), ax, ay, az);
+            };
+            if (L.g.reach > 1) walk_cells<true>(L.g, L.cs, L.c, nr, lane, one);
+            else walk_cells<false>(L.g, L.cs, L.c, nr, lane, one);
         }
     }
     a1x = warp_tree_add(a1x); a1y = warp_tree_add(a1y); a1z = warp_tree_add(a1z);
@@ -569,15 +586,12 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
     float4* obuf = ordered_buf();
     const Local L = local_of<BT>(a, i);
     const Phys P = phys_of<BT>(a, L.s);
-    const int rows = link_rows(L.g);
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, P.col_dis);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             float tx = 0.f, ty = 0.f, tz = 0.f;
             bool hit = false;
-            if (j < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
@@ -602,7 +616,7 @@ __global__ void __launch_bounds__(256) k_collision_w(StageArgs a, const uint32_t
             if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, cx, cy, cz);
             else { cx += tx; cy += ty; cz += tz; }
         }
-    }
+    });
     if (!ORD) { cx = warp_tree_add(cx); cy = warp_tree_add(cy); cz = warp_tree_add(cz); }
     if (lane == 0) a.tmp[i] = make_float4(cx, cy, cz, 0.f);
 }
@@ -621,14 +635,11 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
     const float re = P.rzero, thr = P.rzero_thr;
     float acc = 0.f;
     float4* obuf = ordered_buf();
-    const int rows = link_rows(L.g);
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             float w = 0.f;
-            if (j < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
@@ -637,7 +648,7 @@ __global__ void __launch_bounds__(256) k_pnd_w(StageArgs a, int eos, int all_typ
             if (ORD) ordered_add1<true>(reinterpret_cast<float*>(obuf), lane, w != 0.f, w, acc);
             else acc += w;
         }
-    }
+    });
     if (!ORD) acc = warp_tree_add(acc);
     if (lane != 0) return;
     a.cur.n[i] = acc;
@@ -661,7 +672,6 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     if (ptype(pi) != T_FLUID) return;
     const Local L = local_of<BT>(a, i);
     const Phys P = phys_of<BT>(a, L.s);
-    const int rows = link_rows(L.g);
     const float r02 = P.rzero2;
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, P.rzero);
     // p_hat: a minimum, independent of order.  The same walk keeps every
@@ -673,12 +683,10 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t nhit = 0;
     float hat = press[i];
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             bool near = false;
-            if (j < rg.hi) {
+            if (in) {
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
@@ -695,7 +703,7 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
             }
             nhit += __popc(m);
         }
-    }
+    });
     __syncwarp();
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) hat = fminf(hat, __shfl_xor_sync(0xffffffffu, hat, o));
@@ -706,15 +714,11 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
     // the gradient's terms: candidates of the kept slots, in the same
     // ascending order as the cell walk, or the cell walk itself
     const bool slotted = nhit <= DASH_SLOTS;
-    for (int row = 0; row < (slotted ? 1 : rows); row++) {
-        RowRange rg;
-        if (slotted) rg = RowRange{0u, nhit};
-        else rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = slotted ? (base + lane < rg.hi ? my[base + lane] : 0xFFFFFFFFu) : base + lane;
+    auto grad = [&](uint32_t j, bool in) {
+        {
             float tx = 0.f, ty = 0.f, tz = 0.f;
             bool hit = false;
-            if (base + lane < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 if (!(skip_dummy && ptype(pj) == T_DUMMY)) {
                     const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
@@ -734,6 +738,14 @@ __global__ void __launch_bounds__(256) k_dash_w(StageArgs a, const uint32_t* __r
             if (ORD) ordered_add3<true>(obuf, lane, hit, tx, ty, tz, gx, gy, gz);
             else { gx += tx; gy += ty; gz += tz; }
         }
+    };
+    if (slotted) {
+        for (uint32_t f0 = 0; f0 < nhit; f0 += 32) {
+            const bool in = f0 + lane < nhit;
+            grad(in ? my[f0 + lane] : 0xFFFFFFFFu, in);
+        }
+    } else {
+        walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, grad);
     }
     if (!ORD) { gx = warp_tree_add(gx); gy = warp_tree_add(gy); gz = warp_tree_add(gz); }
     if (lane != 0) return;
@@ -973,9 +985,11 @@ void launch_lambda(const StageArgs& a, const unsigned long long* best, float* la
 
 // i_normal (MPS_CAL_expl_v1.0/MPS.cpp:531-555): for a type-2 particle the
 // first type-1 particle in index order that improves r^2 below 2 r0^2.
-// `reach` cells in each direction cover sqrt(2) r0; rows are visited in
-// ascending cell order, so candidates come in ascending index order.
-__global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_t* __restrict__ normal_id_of) {
+// `reach` cells along x and `reach_yz` along y and z cover sqrt(2) r0; rows
+// are visited in ascending cell order, so candidates come in ascending index
+// order.
+__global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, int reach_yz,
+                                                 uint32_t* __restrict__ normal_id_of) {
     const uint32_t n = a.sc->np;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -991,9 +1005,9 @@ __global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_
     uint32_t best = 0xffffffffu;
     const uint32_t c = L.c;
     const Grid& g = L.g;
-    const int nz = g.dim == 3 ? reach : 0;
+    const int nz = g.dim == 3 ? reach_yz : 0;
     for (int dz = -nz; dz <= nz; dz++) {
-        for (int dy = -reach; dy <= reach; dy++) {
+        for (int dy = -reach_yz; dy <= reach_yz; dy++) {
             const uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
             uint32_t first = 0xffffffffu, last = 0;
             for (int dx = -reach; dx <= reach; dx++) {
@@ -1020,8 +1034,9 @@ __global__ void __launch_bounds__(256) k_normals(StageArgs a, int reach, uint32_
     normal_id_of[idi] = best == 0xffffffffu ? idi : a.cur.id[best];
 }
 
-void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint32_t cap, cudaStream_t st) {
-    k_normals<<<blocks_for(cap, 256), 256, 0, st>>>(a, reach, normal_id_of);
+void launch_normals(const StageArgs& a, int reach, int reach_yz, uint32_t* normal_id_of, uint32_t cap,
+                    cudaStream_t st) {
+    k_normals<<<blocks_for(cap, 256), 256, 0, st>>>(a, reach, reach_yz, normal_id_of);
 }
 
 // ---------------------------------------------------------------- boundary motion

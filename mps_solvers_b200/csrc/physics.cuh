@@ -135,7 +135,8 @@ void launch_nzero_range(const float* n, uint32_t lo, uint32_t hi, unsigned long 
 void launch_lambda(const StageArgs& a, const unsigned long long* best, float* lambda_out, cudaStream_t st);
 // nearest type-1 particle (first in index order) within sqrt(2) r0 of each
 // type-2 particle, stored by GEO.dat index
-void launch_normals(const StageArgs& a, int reach, uint32_t* normal_id_of, uint32_t cap, cudaStream_t st);
+void launch_normals(const StageArgs& a, int reach, int reach_yz, uint32_t* normal_id_of, uint32_t cap,
+                    cudaStream_t st);
 
 // Prescribed rigid motions of boundary particles (the reference's
 // MOTION::doMotion hook).  Motion m moves its particles to

@@ -91,16 +91,13 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
     float* wrow = A.wrm + (size_t)i * PPE_W;
     uint32_t count = 0;
     float diag_lane = 0.f;  // this lane's few nonzero weights, then a FP64 warp sum
-    const int rows = link_rows(L.g);
     const uint32_t lt = (1u << lane) - 1u;
     const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row_near(L.g, L.cs, L.c, row, nr);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             bool app = false;
             float w = 0.f;
-            if (j < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 if (ptype(pj) != T_DUMMY) {
                     const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
@@ -122,7 +119,7 @@ __global__ void __launch_bounds__(256) k_ppe_assemble(AsmArgs A) {
             }
             count += __popc(m);
         }
-    }
+    });
     const double diag = warp_sum_d((double)diag_lane);
     if (lane == 0) {
         if (count > PPE_W) {
@@ -1870,15 +1867,13 @@ __global__ void __launch_bounds__(256) k_cn_assemble(CnArgs A) {
     float* wrow = A.wrm + (size_t)i * PPE_W;
     uint32_t count = 0;
     double diag = 0.0, bi = 0.0;
-    const int rows = link_rows(L.g);
     const uint32_t lt = (1u << lane) - 1u;
-    for (int row = 0; row < rows; row++) {
-        const RowRange rg = link_row(L.g, L.cs, L.c, row);
-        for (uint32_t base = rg.lo; base < rg.hi; base += 32) {
-            const uint32_t j = base + lane;
+    const CellNear nr = cell_near(L.g, L.c, pi.x, pi.y, pi.z, re);
+    walk_cells<!EX>(L.g, L.cs, L.c, nr, lane, [&](uint32_t j, bool in) {
+        {
             bool app = false;
             float w = 0.f;
-            if (j < rg.hi && j != i) {
+            if (in && j != i) {
                 const float4 pj = __ldg(pos + j);
                 const float dx = fsub<EX>(pj.x, pi.x), dy = fsub<EX>(pj.y, pi.y), dz = fsub<EX>(pj.z, pi.z);
                 const float rr = dot3<EX>(dx, dy, dz, dx, dy, dz);
@@ -1901,7 +1896,7 @@ __global__ void __launch_bounds__(256) k_cn_assemble(CnArgs A) {
             }
             count += __popc(m);
         }
-    }
+    });
     diag = warp_sum_d(diag);
     bi = warp_sum_d(bi);
     if (lane == 0) {

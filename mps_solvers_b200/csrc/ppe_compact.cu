@@ -219,54 +219,68 @@ __device__ __forceinline__ bool sp_entry(const SpArgs& A, uint32_t jd, uint32_t 
     return d >= -32767 && d <= 32767;
 }
 
-// off-diagonal entries of every 32-row slice (thread per row, warp per slice)
+// Both passes take a warp per row: the lanes read the row's stored
+// neighbours (one contiguous run of s_col / s_val) side by side, so the
+// chain index_of_id -> rlen, cpos, diag64 is walked once per row instead of
+// once per entry.
+//
+// Pass 1: off[s] = 32 x (longest row of slice s); off is zeroed beforehand.
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t s = k / SP_SLICE;
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (k >= R) return;
+    const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
+    const uint32_t n = __ldg(A.s_cnt + id);
     uint32_t cnt = 0;
-    if (k < R) {
-        const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
-        const uint32_t n = __ldg(A.s_cnt + id);
-        for (uint32_t t = 0; t < n; t++) {
-            uint32_t j;
-            int d;
-            cnt += sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, k, &j, &d) ? 1u : 0u;
-        }
+    for (uint32_t t0 = 0; t0 < n; t0 += 32) {
+        const uint32_t t = t0 + lane;
+        uint32_t j;
+        int d;
+        const bool ok = t < n && sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, k, &j, &d);
+        cnt += __popc(__ballot_sync(0xffffffffu, ok));
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
-    if ((threadIdx.x & 31) == 0 && s <= A.maxslices) A.off[s] = cnt * SP_SLICE;
+    if (lane == 0 && cnt) atomicMax(A.off + k / SP_SLICE, cnt * SP_SLICE);
 }
 
 __device__ __forceinline__ uint32_t sp_bf16_bits(float v) {
     return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v));
 }
 
+// Pass 2 (after the scan of off): the kept entries of row k in stored order,
+// then zeros up to the slice's width.  A slice's rows past R are padded by
+// the warps of the slice's first row.
 __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
-    if (s >= (R + SP_SLICE - 1) / SP_SLICE) return;
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (k >= R) return;
+    const uint32_t s = k / SP_SLICE, col = k % SP_SLICE;
     const uint32_t base = A.off[s], W = (A.off[s + 1] - base) / SP_SLICE;
-    uint32_t t = 0;
-    if (k < R) {
-        const uint32_t i = __ldg(A.rowlist + k);
-        const uint32_t id = __ldg(A.idv + i);
-        const uint32_t n = __ldg(A.s_cnt + id);
-        const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
-        A.diag[k] = __ldg(A.s_diag + id) * (di * di);
-        for (uint32_t u = 0; u < n; u++) {
-            uint32_t j;
-            int d;
-            if (!sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, k, &j, &d)) continue;
+    const uint32_t i = __ldg(A.rowlist + k);
+    const uint32_t id = __ldg(A.idv + i);
+    const uint32_t n = __ldg(A.s_cnt + id);
+    const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
+    if (lane == 0) A.diag[k] = __ldg(A.s_diag + id) * (di * di);
+    uint32_t t = 0;  // entries written so far (the same in every lane)
+    for (uint32_t u0 = 0; u0 < n; u0 += 32) {
+        const uint32_t u = u0 + lane;
+        uint32_t j = 0;
+        int d = 0;
+        const bool ok = u < n && sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, k, &j, &d);
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
             const float dj = (float)(1.0 / sqrt(-__ldg(A.diag64 + j)));
             const float v = __ldg(A.s_val + (size_t)id * LP_GW + u) * (di * dj);
-            A.ent[base + SP_SLICE * t + lane] = ((uint32_t)(d & 0xffff) << 16) | sp_bf16_bits(v);
-            t++;
+            const uint32_t slot = t + __popc(m & ((1u << lane) - 1u));
+            A.ent[base + SP_SLICE * slot + col] = ((uint32_t)(d & 0xffff) << 16) | sp_bf16_bits(v);
         }
+        t += __popc(m);
     }
-    for (; t < W; t++) A.ent[base + SP_SLICE * t + lane] = 0u;
+    for (uint32_t p = t + lane; p < W; p += 32) A.ent[base + SP_SLICE * p + col] = 0u;
+    // rows of the last slice past R: all padding
+    if (col == 0 && s == (R - 1) / SP_SLICE) {
+        for (uint32_t c = R % SP_SLICE ? R % SP_SLICE : SP_SLICE; c < SP_SLICE; c++)
+            for (uint32_t p = lane; p < W; p += 32) A.ent[base + SP_SLICE * p + c] = 0u;
+    }
 }
 
 // ---------------------------------------------------------------- solve
@@ -763,9 +777,12 @@ int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, c
     A.diag = w.sp_diag;
     const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
-    k_sp_width<<<cblocks((maxslices + 1) * SP_SLICE, 256), 256, 0, st>>>(A);
+    // a warp per row (rows <= 32 maxslices)
+    const uint32_t blocks = cblocks(maxslices * SP_SLICE, 256 / 32);
+    cudaMemsetAsync(w.sp_off, 0, (maxslices + 1) * sizeof(uint32_t), st);
+    k_sp_width<<<blocks, 256, 0, st>>>(A);
     launch_scan_exclusive(w.sp_off, maxslices + 1, st);
-    k_sp_pack<<<cblocks(maxslices * SP_SLICE, 256), 256, 0, st>>>(A);
+    k_sp_pack<<<blocks, 256, 0, st>>>(A);
     return 3;
 }
 

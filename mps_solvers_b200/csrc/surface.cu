@@ -155,17 +155,19 @@ __global__ void __launch_bounds__(256) k_surface_vertex(StageArgs a, SurfaceGrid
     const float x = sg.ox + sg.hx * ix, y = sg.oy + sg.hy * iy, z = sg.oz + sg.hz * iz;
     const Grid& g = a.g;
     const float r0 = a.P.rzero;
-    auto cell_lo = [&](float p, float o, uint32_t dim) {
-        const float t = floorf((p - r0 - o) / g.cell_size);
+    auto cell_lo = [&](float p, float o, float h, uint32_t dim) {
+        const float t = floorf((p - r0 - o) / h);
         return t < 0.f ? 0 : (t >= (float)dim ? (int)dim : (int)t);
     };
-    auto cell_hi = [&](float p, float o, uint32_t dim) {
-        const float t = floorf((p + r0 - o) / g.cell_size);
+    auto cell_hi = [&](float p, float o, float h, uint32_t dim) {
+        const float t = floorf((p + r0 - o) / h);
         return t < 0.f ? -1 : (t >= (float)dim ? (int)dim - 1 : (int)t);
     };
-    const int x0 = cell_lo(x, g.left, g.cdx), x1 = cell_hi(x, g.left, g.cdx);
-    const int y0 = cell_lo(y, g.back, g.cdy), y1 = cell_hi(y, g.back, g.cdy);
-    const int z0 = g.dim == 3 ? cell_lo(z, g.bottom, g.cdz) : 0, z1 = g.dim == 3 ? cell_hi(z, g.bottom, g.cdz) : 0;
+    const float hx = g.cell_size, hyz = g.cell_yz;
+    const int x0 = cell_lo(x, g.left, hx, g.cdx), x1 = cell_hi(x, g.left, hx, g.cdx);
+    const int y0 = cell_lo(y, g.back, hyz, g.cdy), y1 = cell_hi(y, g.back, hyz, g.cdy);
+    const int z0 = g.dim == 3 ? cell_lo(z, g.bottom, hyz, g.cdz) : 0;
+    const int z1 = g.dim == 3 ? cell_hi(z, g.bottom, hyz, g.cdz) : 0;
     float acc = 0.f;
     if (x0 <= x1) {
         for (int cz = z0; cz <= z1; cz++)

@@ -130,6 +130,7 @@ def test_tensor_core_forward_matches_fp32(capi, tmp_path):
         s.set_precond_params(random_params(capi, 0, om_scale=0.3))
         s.step(3)
         diff = s.precond_tensor_cores(True)
+        print("tensor-core forward: largest relative difference of G", diff)
         assert 0.0 < diff < 2e-2, diff
         for _ in range(3):
             st = s.step(1)
