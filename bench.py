@@ -272,7 +272,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                          use_graph=1, precond=precond)
         return capi.Simulation(tmpd, method=method, arith=arith, device=local_rank, use_graph=1,
                                precond=precond if method == capi.METHOD_SEMI_IMPLICIT else capi.PRECOND_DIAGONAL,
-                               visc_implicit=int(method == capi.METHOD_SEMI_IMPLICIT and args.visc == "implicit"))
+                               visc_implicit=int(method == capi.METHOD_SEMI_IMPLICIT and args.visc == "implicit"),
+                               ppe_layout=-1 if args.ppe_layout == "sliced" else 0)
 
     def load_learned(s):
         from mps_solvers_b200 import precond_weights
@@ -299,6 +300,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         nb2 = sum(sim.scene_info(s).nb2 for s in range(len(dirs)))
         nb1 = sum(sim.scene_info(s).nb1 for s in range(len(dirs)))
     if tune is not None:
+        if args.ppe_layout == "compact" and "ppe_compact" in tune:
+            tune = dict(tune, ppe_compact=1)  # the other launch choices stay the autotuner's
         sim.apply_tuning(tune)
     tc_diff = None
     extra_warm = 0
@@ -409,9 +412,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     else:
         alg_bytes = STAGE_BYTES[dom] * n
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
-    # the committed traffic figures are for the full-size workloads
-    traffic = (_traffic_from_profiles("pressure" if dom == "ppe_solve" else dom, args.workload)
-               if args.size == "full" else None)
+    # the committed traffic figures are for the full-size workloads, and for
+    # the PPE per stencil layout (scalar ppe_escaped is -1 on the 8-byte one)
+    sliced = method == capi.METHOD_SEMI_IMPLICIT and scal.get("ppe_escaped", 0) < 0
+    tkey = ("pressure_sell" if sliced else "pressure") if dom == "ppe_solve" else dom
+    traffic = _traffic_from_profiles(tkey, args.workload) if args.size == "full" else None
     # FP32 pipe (the secondary roofline of the stencil stages): pair
     # evaluations of the fixed model, |{j: r_ij < re}| x FLOP per pair (PND 10
     # over all particles at r0; viscosity 16 at rlap, collision 20 and
@@ -434,7 +439,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    f"{args.workload} small profiling tank", "particles": n,
                    "precond": args.precond if method == capi.METHOD_SEMI_IMPLICIT else None,
                    "fluid": int(n - nb2 - nb1), "arith": args.arith,
-                   "viscosity": ("Crank-Nicolson" if args.visc == "implicit" else "explicit")
+                   "viscosity": ("Crank-Nicolson" if args.visc == "implicit" else "explicit"),
+                   "ppe_layout": (None if method != capi.METHOD_SEMI_IMPLICIT else
+                                  "sliced 8-byte" if sliced else "compact 6-byte")
                    if method == capi.METHOD_SEMI_IMPLICIT else "explicit",
                    "l2": "flushed (256 MB write) before every timed step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -556,6 +563,8 @@ def main():
                     help="PPE preconditioner of the semi-implicit timed run")
     ap.add_argument("--no-ppe-compare", action="store_true",
                     help="skip the diagonal-vs-learned PPE comparison (semi-implicit)")
+    ap.add_argument("--ppe-layout", default="auto", choices=["auto", "compact", "sliced"],
+                    help="PPE stencil layout (auto: the library's default and the autotuner's choice)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (short launch lists for profiling)")
     ap.add_argument("--no-sub-runs", action="store_true",

@@ -119,7 +119,7 @@ typedef struct {
                             between two evaluations of the network; between
                             them the symmetric form of the factor is kept by
                             particle (GEO index) and re-packed for the current
-                            rows every step (0: 10; 1: every step)           */
+                            rows every step (0: 40; 1: every step)           */
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after

@@ -573,7 +573,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
             return MPS_ERR_INVALID;
         }
         h->ppe.c16_smem_chunks = h->opt.ppe_smem_chunks == 0 ? 8 : (h->opt.ppe_smem_chunks < 0 ? 0 : h->opt.ppe_smem_chunks);
-        h->ppe.precond_every = h->opt.precond_every > 0 ? h->opt.precond_every : 10;
+        h->ppe.precond_every = h->opt.precond_every > 0 ? h->opt.precond_every : 40;
         h->ppe.index_of_id = h->index_of_id;
         if (h->opt.ppe_layout == 0 && !h->nscenes) {
             e = ppe_c16_enable(h->ppe, &h->err);
@@ -1616,12 +1616,14 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
                 continue;
             }
             if (form == 3 && !compact_ok) continue;
-            if (ppe_set_threads(h->ppe, ppe_cand[c % 3]) != MPS_OK) {
+            const bool pipe = form == 2;
+            const int threads = ppe_cand[c % 3];
+            if (ppe_set_threads(h->ppe, threads) != MPS_OK) {
                 if (form < 3) r.ppe_ms[c] = -1.f;  // the device cannot hold this shape
                 continue;
             }
             h->ppe.stored_weights = form != 1;
-            h->ppe.pipelined = form == 2;
+            h->ppe.pipelined = pipe;
             set_compact(h, form == 3);
             drop_graphs(h);
             double tot = 0.0;
@@ -1635,9 +1637,9 @@ extern "C" mps_status mps_autotune(mps_handle* h, int steps, mps_tune_report* re
             else r.ppe_compact_ms[c % 3] = (float)t;
             if (t < best) {
                 best = t;
-                best_p = ppe_cand[c % 3];
+                best_p = threads;
                 best_sw = form != 1;
-                best_pipe = form == 2;
+                best_pipe = pipe;
                 best_c16 = form == 3;
             }
         }

@@ -248,6 +248,31 @@ __device__ __forceinline__ RowRange link_row_near(const Grid& g, const uint32_t*
     return link_row_near_at(g, cell_start, c, dz, dy, n);
 }
 
+// link_row_near on the reference's grid (reach 1): row r of 9 (3 in 2D)
+__device__ __forceinline__ RowRange link_row_near_ref(const Grid& g, const uint32_t* __restrict__ cell_start,
+                                                      uint32_t c, int row, const CellNear& n) {
+    int dz, dy;
+    if (g.dim == 3) { dz = row / 3 - 1; dy = row % 3 - 1; }
+    else { dz = 0; dy = row - 1; }
+    float d2 = 0.f;
+    if (dy < 0) d2 += n.yl * n.yl;
+    else if (dy > 0) d2 += n.yr * n.yr;
+    if (dz < 0) d2 += n.zl * n.zl;
+    else if (dz > 0) d2 += n.zr * n.zr;
+    RowRange r{0u, 0u};
+    if (d2 >= n.re2) return r;
+    const bool wa = d2 + n.xl * n.xl < n.re2, wb = d2 + n.xr * n.xr < n.re2;
+    const uint32_t c0 = c + (uint32_t)dz * g.sheet + (uint32_t)dy * g.cdx;
+    const uint32_t a = c0 - 1u, b = c0 + 1u;
+    const bool va = wa && a < g.ncells, v0 = c0 < g.ncells, vb = wb && b < g.ncells;
+    uint32_t first, last;
+    if (va) first = a; else if (v0) first = c0; else if (vb) first = b; else return r;
+    if (vb) last = b; else if (v0) last = c0; else last = a;
+    r.lo = __ldg(cell_start + first);
+    r.hi = __ldg(cell_start + last + 1u);
+    return r;
+}
+
 // A warp's walk over all its rows as one list of candidates.  Lane r looks
 // up row r (link_row_near; at most 25 rows, so one lookup per lane, all in
 // parallel), an inclusive scan of the row lengths numbers the candidates of
@@ -298,10 +323,12 @@ __device__ __forceinline__ uint32_t flat_at(const FlatWalk& w, uint32_t f) {
 // body(j, in) for each batch of 32 candidates of a warp's walk, in walk
 // order (lane L gets the batch's L-th candidate; `in` is false past the
 // end).  FLAT walks the rows as one list (flat_walk: the rows' lookups in
-// parallel, full batches), the other form row by row; both visit the same
-// candidates in the same order.  The flat form pays on the refined grid (up
-// to 25 short rows); on the reference's grid (9 rows of about 200
-// candidates) the row form is as fast and is what the exact kernels use.
+// parallel, full batches) on any grid; the other form walks the reference's
+// grid (reach 1) row by row.  Both visit the same candidates in the same
+// order.  The flat form pays on the refined grid (up to 25 short rows); on
+// the reference's grid (9 rows of about 200 candidates) the row form is as
+// fast and is what the exact kernels use: exact arithmetic keeps the
+// reference's grid (the refined one is built for fast arithmetic only).
 template <bool FLAT, class F>
 __device__ __forceinline__ void walk_cells(const Grid& g, const uint32_t* __restrict__ cs, uint32_t c,
                                            const CellNear& nr, uint32_t lane, F&& body) {
@@ -312,12 +339,11 @@ __device__ __forceinline__ void walk_cells(const Grid& g, const uint32_t* __rest
             body(flat_at(fw, in ? f0 + lane : fw.total - 1), in);
         }
     } else {
-        const int R = g.reach, nz = g.dim == 3 ? R : 0;
-        for (int dz = -nz; dz <= nz; dz++)
-            for (int dy = -R; dy <= R; dy++) {
-                const RowRange rg = link_row_near_at(g, cs, c, dz, dy, nr);
-                for (uint32_t base = rg.lo; base < rg.hi; base += 32) body(base + lane, base + lane < rg.hi);
-            }
+        const int rows = g.dim == 3 ? 9 : 3;
+        for (int row = 0; row < rows; row++) {
+            const RowRange rg = link_row_near_ref(g, cs, c, row, nr);
+            for (uint32_t base = rg.lo; base < rg.hi; base += 32) body(base + lane, base + lane < rg.hi);
+        }
     }
 }
 

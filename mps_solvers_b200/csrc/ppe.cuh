@@ -107,7 +107,7 @@ struct PpeWork {
     // (S the symmetric form in LearnedWork, kept by GEO index) in 4-row
     // slices, one product fused into the residual update of every iteration
     bool c16_learned = false;          // the compact solve applies S'
-    int precond_every = 10;            // steps between network evaluations
+    int precond_every = 40;            // steps between network evaluations
     uint32_t* sp_off = nullptr;        // first entry of every 32-row slice (widths, then scanned)
     uint32_t* sp_ent = nullptr;        // off-diagonal entries: column - row (16 bits) << 16 | BF16 value
     float* sp_diag = nullptr;          // the diagonal, per compact row

@@ -208,38 +208,59 @@ struct SpArgs {
     uint32_t maxslices;
 };
 
-// the stored neighbour jd of compact row k: a row now, close enough to code
-__device__ __forceinline__ bool sp_entry(const SpArgs& A, uint32_t jd, uint32_t np, uint32_t k, uint32_t* j,
-                                         int* delta) {
-    const uint32_t jj = __ldg(A.index_of_id + jd);
-    *j = jj;
-    if (jj >= np || __ldg(A.rlen + jj) == PPE_DIRICHLET) return false;
-    const int d = (int)__ldg(A.cpos + jj) - (int)k;
-    *delta = d;
-    return d >= -32767 && d <= 32767;
+// Both passes take a thread per row (lane = row of the 32-row slice, so the
+// packed words leave as coalesced 128-byte rows) and eight of its stored
+// neighbours at a time, their loads issued together: the chain s_col ->
+// index_of_id -> rlen, cpos, diag64 costs three dependent rounds per eight
+// entries instead of per entry.
+constexpr uint32_t SP_BATCH = 8;
+
+// the batch [u0, u0 + 8) of row k's stored neighbours: kept or not, the
+// column offset and the neighbour's particle index
+__device__ __forceinline__ void sp_batch(const SpArgs& A, uint32_t id, uint32_t n, uint32_t u0, uint32_t np,
+                                         uint32_t k, bool (&ok)[SP_BATCH], int (&d)[SP_BATCH],
+                                         uint32_t (&j)[SP_BATCH]) {
+    uint32_t jd[SP_BATCH];
+#pragma unroll
+    for (uint32_t b = 0; b < SP_BATCH; b++)
+        jd[b] = u0 + b < n ? __ldg(A.s_col + (size_t)id * LP_GW + u0 + b) : 0u;
+#pragma unroll
+    for (uint32_t b = 0; b < SP_BATCH; b++) j[b] = u0 + b < n ? __ldg(A.index_of_id + jd[b]) : np;
+    uint32_t len[SP_BATCH], cp[SP_BATCH];
+#pragma unroll
+    for (uint32_t b = 0; b < SP_BATCH; b++) {
+        const bool live = j[b] < np;
+        len[b] = live ? __ldg(A.rlen + j[b]) : PPE_DIRICHLET;
+        cp[b] = live ? __ldg(A.cpos + j[b]) : 0u;
+    }
+#pragma unroll
+    for (uint32_t b = 0; b < SP_BATCH; b++) {
+        d[b] = (int)cp[b] - (int)k;
+        ok[b] = len[b] != PPE_DIRICHLET && d[b] >= -32767 && d[b] <= 32767;
+    }
 }
 
-// Both passes take a warp per row: the lanes read the row's stored
-// neighbours (one contiguous run of s_col / s_val) side by side, so the
-// chain index_of_id -> rlen, cpos, diag64 is walked once per row instead of
-// once per entry.
-//
-// Pass 1: off[s] = 32 x (longest row of slice s); off is zeroed beforehand.
+// Pass 1: off[s] = 32 x (longest row of slice s), every slice up to maxslices.
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (k >= R) return;
-    const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
-    const uint32_t n = __ldg(A.s_cnt + id);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = k / SP_SLICE;
     uint32_t cnt = 0;
-    for (uint32_t t0 = 0; t0 < n; t0 += 32) {
-        const uint32_t t = t0 + lane;
-        uint32_t j;
-        int d;
-        const bool ok = t < n && sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + t), np, k, &j, &d);
-        cnt += __popc(__ballot_sync(0xffffffffu, ok));
+    if (k < R) {
+        const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
+        const uint32_t n = __ldg(A.s_cnt + id);
+        for (uint32_t u0 = 0; u0 < n; u0 += SP_BATCH) {
+            bool ok[SP_BATCH];
+            int d[SP_BATCH];
+            uint32_t j[SP_BATCH];
+            sp_batch(A, id, n, u0, np, k, ok, d, j);
+#pragma unroll
+            for (uint32_t b = 0; b < SP_BATCH; b++) cnt += ok[b] ? 1u : 0u;
+        }
     }
-    if (lane == 0 && cnt) atomicMax(A.off + k / SP_SLICE, cnt * SP_SLICE);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
+    if ((threadIdx.x & 31) == 0 && s <= A.maxslices) A.off[s] = cnt * SP_SLICE;
 }
 
 __device__ __forceinline__ uint32_t sp_bf16_bits(float v) {
@@ -247,40 +268,43 @@ __device__ __forceinline__ uint32_t sp_bf16_bits(float v) {
 }
 
 // Pass 2 (after the scan of off): the kept entries of row k in stored order,
-// then zeros up to the slice's width.  A slice's rows past R are padded by
-// the warps of the slice's first row.
+// then zeros up to the slice's width.
 __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
-    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (k >= R) return;
-    const uint32_t s = k / SP_SLICE, col = k % SP_SLICE;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
+    if (s >= (R + SP_SLICE - 1) / SP_SLICE) return;
     const uint32_t base = A.off[s], W = (A.off[s + 1] - base) / SP_SLICE;
-    const uint32_t i = __ldg(A.rowlist + k);
-    const uint32_t id = __ldg(A.idv + i);
-    const uint32_t n = __ldg(A.s_cnt + id);
-    const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
-    if (lane == 0) A.diag[k] = __ldg(A.s_diag + id) * (di * di);
-    uint32_t t = 0;  // entries written so far (the same in every lane)
-    for (uint32_t u0 = 0; u0 < n; u0 += 32) {
-        const uint32_t u = u0 + lane;
-        uint32_t j = 0;
-        int d = 0;
-        const bool ok = u < n && sp_entry(A, __ldg(A.s_col + (size_t)id * LP_GW + u), np, k, &j, &d);
-        const uint32_t m = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
-            const float dj = (float)(1.0 / sqrt(-__ldg(A.diag64 + j)));
-            const float v = __ldg(A.s_val + (size_t)id * LP_GW + u) * (di * dj);
-            const uint32_t slot = t + __popc(m & ((1u << lane) - 1u));
-            A.ent[base + SP_SLICE * slot + col] = ((uint32_t)(d & 0xffff) << 16) | sp_bf16_bits(v);
+    uint32_t t = 0;
+    if (k < R) {
+        const uint32_t i = __ldg(A.rowlist + k);
+        const uint32_t id = __ldg(A.idv + i);
+        const uint32_t n = __ldg(A.s_cnt + id);
+        const float di = (float)(1.0 / sqrt(-__ldg(A.diag64 + i)));
+        A.diag[k] = __ldg(A.s_diag + id) * (di * di);
+        for (uint32_t u0 = 0; u0 < n; u0 += SP_BATCH) {
+            bool ok[SP_BATCH];
+            int d[SP_BATCH];
+            uint32_t j[SP_BATCH];
+            sp_batch(A, id, n, u0, np, k, ok, d, j);
+            double dg[SP_BATCH];
+            float sv[SP_BATCH];
+#pragma unroll
+            for (uint32_t b = 0; b < SP_BATCH; b++) {
+                dg[b] = ok[b] ? __ldg(A.diag64 + j[b]) : -1.0;
+                sv[b] = ok[b] ? __ldg(A.s_val + (size_t)id * LP_GW + u0 + b) : 0.f;
+            }
+#pragma unroll
+            for (uint32_t b = 0; b < SP_BATCH; b++) {
+                if (!ok[b]) continue;
+                const float dj = (float)(1.0 / sqrt(-dg[b]));
+                const float v = sv[b] * (di * dj);
+                A.ent[base + SP_SLICE * t + lane] = ((uint32_t)(d[b] & 0xffff) << 16) | sp_bf16_bits(v);
+                t++;
+            }
         }
-        t += __popc(m);
     }
-    for (uint32_t p = t + lane; p < W; p += 32) A.ent[base + SP_SLICE * p + col] = 0u;
-    // rows of the last slice past R: all padding
-    if (col == 0 && s == (R - 1) / SP_SLICE) {
-        for (uint32_t c = R % SP_SLICE ? R % SP_SLICE : SP_SLICE; c < SP_SLICE; c++)
-            for (uint32_t p = lane; p < W; p += 32) A.ent[base + SP_SLICE * p + c] = 0u;
-    }
+    for (; t < W; t++) A.ent[base + SP_SLICE * t + lane] = 0u;
 }
 
 // ---------------------------------------------------------------- solve
@@ -777,12 +801,9 @@ int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, c
     A.diag = w.sp_diag;
     const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
-    // a warp per row (rows <= 32 maxslices)
-    const uint32_t blocks = cblocks(maxslices * SP_SLICE, 256 / 32);
-    cudaMemsetAsync(w.sp_off, 0, (maxslices + 1) * sizeof(uint32_t), st);
-    k_sp_width<<<blocks, 256, 0, st>>>(A);
+    k_sp_width<<<cblocks((maxslices + 1) * SP_SLICE, 256), 256, 0, st>>>(A);
     launch_scan_exclusive(w.sp_off, maxslices + 1, st);
-    k_sp_pack<<<blocks, 256, 0, st>>>(A);
+    k_sp_pack<<<cblocks(maxslices * SP_SLICE, 256), 256, 0, st>>>(A);
     return 3;
 }
 

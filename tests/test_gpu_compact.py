@@ -90,3 +90,4 @@ def test_compact_layout_without_shared_memory_chunks(capi, tmp_path):
     for o in out[1:]:
         for f in ("pos", "vel", "press"):
             assert np.array_equal(out[0][f], o[f]), f
+

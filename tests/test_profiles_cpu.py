@@ -14,7 +14,7 @@ import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PROFILES = os.path.join(ROOT, "profiles")
-STAGES = {"visc", "collision", "pnd", "dash", "pressure", "assemble"}
+STAGES = {"visc", "collision", "pnd", "dash", "pressure", "pressure_sell", "assemble"}
 WORKLOADS = {"explicit", "semi", "batch", "large"}
 
 
