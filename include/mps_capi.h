@@ -112,9 +112,10 @@ typedef struct {
                             scaling, else the 8-byte layout; -1 = always the
                             8-byte layout.  Same matrix either way;
                             mps_autotune may change it.                       */
-    int ppe_smem_chunks; /* compact layout: 128-entry chunks of the matrix
-                            each warp keeps in shared memory across CG
-                            iterations (0: 8; -1: none; at most 8)           */
+    int ppe_smem_chunks; /* 128-entry chunks of the matrix each warp keeps
+                            in shared memory across CG iterations (0: 8;
+                            -1: none; at most 8 in the compact layout, 6 in
+                            the 8-byte layout with stored weights)           */
     int precond_every;   /* learned preconditioner on the compact layout: steps
                             between two evaluations of the network; between
                             them the symmetric form of the factor is kept by

@@ -177,6 +177,7 @@ struct SolveArgs {
     int max_iter;
     int inner_cap;
     int max_outer;
+    int smem_chunks;  // stored weights: each warp's last chunks held in shared memory
 };
 
 // The weight of a stored neighbour, recomputed from the positions with the
@@ -254,6 +255,41 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t parts = ppe_split(nslices, nw);
     const uint32_t* __restrict__ rowlist = S.rowlist;
+    // With stored weights each warp keeps the last C chunks of its share of
+    // the products (the same chunks in every product: the deal of work items
+    // to warps is fixed) in shared memory for the whole solve; chunk g of
+    // the warp's sequence comes from shared memory when g >= g0.
+    extern __shared__ __align__(16) unsigned char sol_sm[];
+    const uint32_t C = SW ? (uint32_t)S.smem_chunks : 0u;
+    const uint32_t wib = threadIdx.x >> 5;
+    uint4* smc = reinterpret_cast<uint4*>(sol_sm) + (size_t)wib * C * 32;
+    float4* smw = reinterpret_cast<float4*>(sol_sm + (size_t)(blockDim.x >> 5) * C * 32 * sizeof(uint4)) +
+                  (size_t)wib * C * 32;
+    uint32_t g0 = 0xffffffffu;
+    if (C) {
+        uint32_t U = 0;
+        for (uint32_t u = gw; u < parts * nslices; u += nw) {
+            const uint32_t sl = u / parts, part = u % parts;
+            const uint32_t T = (__ldg(S.off + sl + 1) - __ldg(S.off + sl)) >> 7;
+            U += (part + 1) * T / parts - part * T / parts;
+        }
+        g0 = U > C ? U - C : 0u;
+        uint32_t g = 0;
+        for (uint32_t u = gw; u < parts * nslices; u += nw) {
+            const uint32_t sl = u / parts, part = u % parts;
+            const uint32_t base = __ldg(S.off + sl);
+            const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;
+            const uint32_t t0 = part * T / parts, t1 = (part + 1) * T / parts;
+            const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
+            const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
+            for (uint32_t t = t0; t < t1; t++, g++)
+                if (g >= g0) {
+                    smc[(g - g0) * 32 + lane] = __ldg(cols + 32 * t);
+                    smw[(g - g0) * 32 + lane] = __ldg(wts + 32 * t);
+                }
+        }
+        __syncwarp();
+    }
     int total = 0, outers = 0;
     double relres = 0.0;
     bool converged = false;
@@ -345,6 +381,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
             // to qp[p - 1], and p.q adds every part's p_i * (its share of
             // q_i), which is linear in the shares.
             double pq[1] = {0.0};
+            uint32_t g = 0;  // this warp's chunks so far (the shared-memory tail)
             for (uint32_t u = gw; u < parts * nslices; u += nw) {
                 const uint32_t sl = u / parts, part = u % parts;
                 const uint32_t k = sl * SELL_C + rsub;
@@ -352,13 +389,15 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const uint64_t pol = mat_policy(base, S.keep);
                 const uint32_t T = (__ldg(S.off + sl + 1) - base) >> 7;  // chunks of 16 per row
                 const uint32_t t0 = part * T / parts, t1 = (part + 1) * T / parts;
+                // chunks [ts, t1) of this item come from shared memory
+                const uint32_t ts = g >= g0 ? t0 : (g0 - g >= t1 - t0 ? t1 : t0 + (g0 - g));
                 const uint4* cols = reinterpret_cast<const uint4*>(S.scols + base) + lane;
                 const float4* wts = reinterpret_cast<const float4*>(S.sw + base) + lane;
                 const uint32_t ii = k < R ? __ldg(rowlist + k) : 0u;
                 const float4 pi = __ldg(S.pos + ii);
                 float s0 = 0.f, s1 = 0.f;
 #pragma unroll 4  // measured: 4 chunks per step beat 2 (and a cp.async ring)
-                for (uint32_t t = t0; t < t1; t++) {
+                for (uint32_t t = t0; t < ts; t++) {
                     const uint4 c = ld_mat(cols + 32 * t, pol);
                     const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, S.rlap, S.rlap_thr, pi, ii, c);
                     const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
@@ -367,6 +406,20 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     s0 = fmaf(w.z, fmaf(beta, a2.y, a2.x), s0);
                     s1 = fmaf(w.w, fmaf(beta, a3.y, a3.x), s1);
                 }
+                if (SW) {
+                    const uint32_t gs = g + (ts - t0) - g0;  // shared-memory slot of chunk ts
+#pragma unroll 2
+                    for (uint32_t t = ts; t < t1; t++) {
+                        const uint4 c = smc[(gs + t - ts) * 32 + lane];
+                        const float4 w = smw[(gs + t - ts) * 32 + lane];
+                        const float2 a0 = zc[c.x], a1 = zc[c.y], a2 = zc[c.z], a3 = zc[c.w];
+                        s0 = fmaf(w.x, fmaf(beta, a0.y, a0.x), s0);
+                        s1 = fmaf(w.y, fmaf(beta, a1.y, a1.x), s1);
+                        s0 = fmaf(w.z, fmaf(beta, a2.y, a2.x), s0);
+                        s1 = fmaf(w.w, fmaf(beta, a3.y, a3.x), s1);
+                    }
+                }
+                g += t1 - t0;
                 float s = s0 + s1;
                 s += __shfl_xor_sync(0xffffffffu, s, 8);
                 s += __shfl_xor_sync(0xffffffffu, s, 16);
@@ -1439,6 +1492,15 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
         return MPS_ERR_CUDA;
     }
     if (per_sm > 1) per_sm = 1;
+    {
+        const int most = PPE_THREADS / 32 * PPE_SMEM_CHUNKS * 32 * (int)(sizeof(uint4) + sizeof(float4));
+        for (const void* f : {(const void*)k_ppe_solve<true, 0, true>, (const void*)k_ppe_solve<false, 0, true>,
+                              (const void*)k_ppe_solve<true, 1, true>, (const void*)k_ppe_solve<false, 1, true>})
+            if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, most) != cudaSuccess) {
+                *err = "the PPE solver cannot have its shared memory";
+                return MPS_ERR_CUDA;
+            }
+    }
     w.sms = sms;
     w.threads = PPE_THREADS;
     w.blocks = sms * per_sm;
@@ -1693,6 +1755,10 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.eta_min = pow(10.0, -(double)(opt.cg_inner_digits > 0 ? opt.cg_inner_digits : 4));
     S.max_outer = 40;
     S.keep = w.l2_keep_entries;
+    // shared-memory chunks (1 KB a warp each with stored weights): at most
+    // PPE_SMEM_CHUNKS, 192 KB for the 32 warps of an SM
+    S.smem_chunks = w.stored_weights ? (w.c16_smem_chunks < PPE_SMEM_CHUNKS ? w.c16_smem_chunks : PPE_SMEM_CHUNKS) : 0;
+    if (S.smem_chunks < 0) S.smem_chunks = 0;
     if (a.batch.n) {
         BatchSolveArgs B;
         B.rowlist = w.rowlist;
@@ -1804,7 +1870,8 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     else
         fn = a.exact ? (learned ? (const void*)k_ppe_solve<true, 1, false> : (const void*)k_ppe_solve<true, 0, false>)
                      : (learned ? (const void*)k_ppe_solve<false, 1, false> : (const void*)k_ppe_solve<false, 0, false>);
-    w.launch_err = launch_cooperative(fn, w.blocks, w.threads, args, st);
+    const size_t smem = (size_t)(w.threads / 32) * (size_t)S.smem_chunks * 32 * (sizeof(uint4) + sizeof(float4));
+    w.launch_err = launch_cooperative_smem(fn, w.blocks, w.threads, smem, args, st);
     if (!w.write_pressure) return 1;
     k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
     return 2;

@@ -28,6 +28,7 @@ constexpr uint32_t PPE_DIRICHLET = 0xffffffffu;
 constexpr int PPE_THREADS = 1024;
 constexpr int PPE_PARTS = 4;           // FP64 partial sums per block
 constexpr uint32_t SELL_C = 8;         // rows per sliced-ELL slice
+constexpr int PPE_SMEM_CHUNKS = 6;     // 8-byte layout: most 1 KB chunks a warp keeps in shared memory
 constexpr uint32_t PPE_MAX_SCENES = 256;  // scenes of a batch the solver holds in shared memory
 
 // PPE constants of one scene of a batch (MPS_CAL_v4.0/MPS_CPU.cpp:619-650)

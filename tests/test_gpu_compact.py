@@ -91,3 +91,19 @@ def test_compact_layout_without_shared_memory_chunks(capi, tmp_path):
         for f in ("pos", "vel", "press"):
             assert np.array_equal(out[0][f], o[f]), f
 
+
+
+def test_8_byte_layout_shared_memory_chunks(capi, tmp_path):
+    """The 8-byte layout's solver also keeps each warp's last chunks in
+    shared memory (stored weights): the same products in the same order
+    with any number of them, so the states are identical bit for bit."""
+    g = load_golden("semi_tank")
+    d = write_golden_case(g, str(tmp_path / "s"))
+    out = []
+    for chunks in (0, -1, 3):
+        with capi.Simulation(d, method=capi.METHOD_SEMI_IMPLICIT, ppe_layout=-1, ppe_smem_chunks=chunks) as s:
+            s.step(6)
+            out.append(s.state())
+    for o in out[1:]:
+        for f in ("pos", "vel", "press"):
+            assert np.array_equal(out[0][f], o[f]), f
