@@ -390,7 +390,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     compare = None
     if method == capi.METHOD_SEMI_IMPLICIT and rank == 0 and not args.no_ppe_compare:
         if batch_counts is None:
-            compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)))
+            compare = ppe_compare(tmpd, arith, local_rank, args.warmup, max(3, min(args.steps, 10)),
+                                  tune_diag=tune if precond == capi.PRECOND_DIAGONAL else None)
         else:
             compare = ppe_compare(dirs, arith, local_rank, args.warmup, max(3, min(args.steps, 5)), accel=accel)
 
@@ -478,12 +479,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     return line
 
 
-def ppe_compare(case_dir, arith: int, device: int, warm: int, steps: int, accel=None):
+def ppe_compare(case_dir, arith: int, device: int, warm: int, steps: int, accel=None, tune_diag=None):
     """PPE solve milliseconds and PCG iterations per step (FP64 true residual
     to 1e-8) with diagonal scaling and with the trained learned factor, each
     on a fresh copy of the scene (or of the batch, when case_dir is a list of
     scene directories: iterations are then the mean over scenes) after
-    `warm` steps."""
+    `warm` steps.  A single scene runs each arm with its own autotuned launch
+    shapes and stencil layout (the diagonal arm with the main run's)."""
     from mps_solvers_b200 import capi, precond_weights
     out = {"tolerance": 1e-8, "steps": steps, "warmup": warm,
            "weights": os.path.relpath(precond_weights.PATH, ROOT)}
@@ -493,9 +495,17 @@ def ppe_compare(case_dir, arith: int, device: int, warm: int, steps: int, accel=
             sim = capi.Simulation.batch(case_dir, accel=accel, method=capi.METHOD_SEMI_IMPLICIT, arith=arith,
                                         device=device, precond=pc)
         else:
-            sim = capi.Simulation(case_dir, method=capi.METHOD_SEMI_IMPLICIT, arith=arith, device=device,
-                                  precond=pc)
+            mk = lambda: capi.Simulation(case_dir, method=capi.METHOD_SEMI_IMPLICIT, arith=arith, device=device,
+                                         precond=pc)
+            tune = tune_diag if pc == capi.PRECOND_DIAGONAL else None
+            if pc == capi.PRECOND_LEARNED:
+                with mk() as scratch:
+                    scratch.set_precond_params(precond_weights.load())
+                    tune = scratch.autotune(2)
+            sim = mk()
         with sim as s:
+            if not batch and tune is not None:
+                s.apply_tuning(tune)
             if pc == capi.PRECOND_LEARNED:
                 s.set_precond_params(precond_weights.load())
                 s.step(1)
