@@ -1260,10 +1260,11 @@ __global__ void __launch_bounds__(256) k_rows_scatter(const uint32_t* __restrict
 // longest of them rounded up to a multiple of 16, padded with the row's own
 // index and weight 0.  A warp takes one slice with 4 lanes per row; lane
 // L = 8q + r owns, in every chunk t of 16 entries of row r, the 4 entries
-// 16t + 4q .. 16t + 4q + 3, stored together at word
+// 16t + q, 16t + q + 4, 16t + q + 8 and 16t + q + 12, stored together at word
 // sell_off[s] + 4 (32t + L), so each lane reads them (columns, and weights
 // in the same layout) as one 16-byte vector and a warp's load is one
-// contiguous 512-byte block.
+// contiguous 512-byte block; the four lanes of a row then gather four
+// consecutive entries per instruction.
 __global__ void __launch_bounds__(256) k_sell_width(const uint32_t* __restrict__ rlen,
                                                     const uint32_t* __restrict__ rowlist,
                                                     const uint32_t* __restrict__ nrows, uint32_t* __restrict__ width,
@@ -1299,22 +1300,22 @@ __global__ void __launch_bounds__(256) k_sell_pack(const uint32_t* __restrict__ 
     const bool has = k < R;
     const uint32_t i = has ? rowlist[k] : 0u;
     const uint32_t len = has ? rlen[i] : 0u;
-    const uint4* rc = reinterpret_cast<const uint4*>(cols_rm + (size_t)i * PPE_W);
-    const float4* rw = reinterpret_cast<const float4*>(w_rm + (size_t)i * PPE_W);
+    const uint32_t* rc = cols_rm + (size_t)i * PPE_W;
+    const float* rw = w_rm + (size_t)i * PPE_W;
     uint4* dc = reinterpret_cast<uint4*>(scols + base) + lane;
     float4* dw = reinterpret_cast<float4*>(sw + base) + lane;
     for (uint32_t t = 0; t < T; t++) {
-        const uint32_t e = 16u * t + 4u * q;
+        // lane (r, q) holds entries q, q + 4, q + 8, q + 12 of the row's 16
+        // in this chunk, so that one gather instruction of the solver reads
+        // 4 consecutive entries of each row: neighbouring columns, mostly in
+        // the same 32-byte sectors of the gathered vector
+        const uint32_t e = 16u * t + q;
         uint4 c = make_uint4(i, i, i, i);
         float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e < len) {
-            const uint4 lc = rc[e >> 2];
-            const float4 lw = rw[e >> 2];
-            c.x = lc.x; w.x = lw.x;
-            if (e + 1 < len) { c.y = lc.y; w.y = lw.y; }
-            if (e + 2 < len) { c.z = lc.z; w.z = lw.z; }
-            if (e + 3 < len) { c.w = lc.w; w.w = lw.w; }
-        }
+        if (e < len) { c.x = rc[e]; w.x = rw[e]; }
+        if (e + 4 < len) { c.y = rc[e + 4]; w.y = rw[e + 4]; }
+        if (e + 8 < len) { c.z = rc[e + 8]; w.z = rw[e + 8]; }
+        if (e + 12 < len) { c.w = rc[e + 12]; w.w = rw[e + 12]; }
         dc[32 * t] = c;
         dw[32 * t] = w;
     }
@@ -1577,7 +1578,7 @@ __global__ void __launch_bounds__(256) k_sell_export(const uint32_t* __restrict_
     const uint32_t o = row_start[i];
     for (uint32_t t = 0; t < T; t++) {
         for (uint32_t u = 0; u < 4; u++) {
-            const uint32_t e = 16u * t + 4u * q + u;
+            const uint32_t e = 16u * t + q + 4u * u;  // the pack's order (k_sell_pack)
             if (e < len) {
                 const size_t src = (size_t)base + 4u * (32u * t + lane) + u;
                 cols[o + e] = scols[src];
