@@ -9,8 +9,9 @@
 //    (ascending particle) order; every solver vector is indexed that way, so
 //    the neighbour gathers touch a dense 8-byte-per-row vector;
 //  * slices of 4 rows; a warp takes a slice with 8 lanes per row, lane
-//    8 r + l holding entries 32 t + 4 l .. 32 t + 4 l + 3 of row r in chunk t
-//    (rows padded to a multiple of 32 entries with weight 0);
+//    8 r + l holding entries 32 t + l, + 8, + 16 and + 24 of row r in chunk t
+//    (rows padded to a multiple of 32 entries with weight 0), so the lanes
+//    of a row gather 8 consecutive entries per instruction;
 //  * a column is stored as 16 bits, column - 4 * slice + 32768 (the rows a
 //    row couples to lie within a few cell layers of it in this numbering);
 //    a column out of that range is stored as 65535 and its full value is
@@ -96,29 +97,27 @@ __global__ void __launch_bounds__(256) k_c16_pack(const uint32_t* __restrict__ c
     const uint32_t pad = r + (uint32_t)C16_BIAS;  // the row itself, weight 0
     uint32_t nesc = 0;
     for (uint32_t t = 0; t < T; t++) {
-        const uint32_t e = 32u * t + 4u * l;
+        // lane 8 r + l holds entries l, l + 8, l + 16, l + 24 of the row's 32
+        // in this chunk, so that one gather instruction of the solver reads
+        // 8 consecutive entries of each row (neighbouring columns)
+        const uint32_t e = 32u * t + l;
         uint32_t c[4] = {pad, pad, pad, pad};
         float w[4] = {0.f, 0.f, 0.f, 0.f};
         const size_t at = (size_t)(g0 + t) * C16_CHUNK + 4u * lane;
-        if (e < len) {
-            const uint4 lc = *reinterpret_cast<const uint4*>(cols_rm + (size_t)i * PPE_W + e);
-            const float4 lw = *reinterpret_cast<const float4*>(w_rm + (size_t)i * PPE_W + e);
-            const uint32_t jc[4] = {lc.x, lc.y, lc.z, lc.w};
-            const float jw[4] = {lw.x, lw.y, lw.z, lw.w};
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                if (e + u < len) {
-                    const uint32_t col = cpos[jc[u]];
-                    const int code = (int)col - base;
-                    if (code >= 0 && code < (int)C16_ESC) {
-                        c[u] = (uint32_t)code;
-                    } else {
-                        c[u] = C16_ESC;
-                        side[at + u] = col;
-                        nesc++;
-                    }
-                    w[u] = jw[u];
+        for (int u = 0; u < 4; u++) {
+            const uint32_t eu = e + 8u * u;
+            if (eu < len) {
+                const uint32_t col = cpos[cols_rm[(size_t)i * PPE_W + eu]];
+                const int code = (int)col - base;
+                if (code >= 0 && code < (int)C16_ESC) {
+                    c[u] = (uint32_t)code;
+                } else {
+                    c[u] = C16_ESC;
+                    side[at + u] = col;
+                    nesc++;
                 }
+                w[u] = w_rm[(size_t)i * PPE_W + eu];
             }
         }
         *reinterpret_cast<uint2*>(codes + at) = make_uint2(c[0] | (c[1] << 16), c[2] | (c[3] << 16));
@@ -166,7 +165,7 @@ __global__ void __launch_bounds__(256) k_c16_export(const uint32_t* __restrict__
     const int base = (int)(slice * C16_ROWS) - C16_BIAS;
     for (uint32_t t = 0; t < T; t++)
         for (uint32_t u = 0; u < 4; u++) {
-            const uint32_t e = 32u * t + 4u * l + u;
+            const uint32_t e = 32u * t + l + 8u * u;  // the pack's order (k_c16_pack)
             if (e >= len) continue;
             const size_t at = (size_t)(g0 + t) * C16_CHUNK + 4u * lane + u;
             const uint32_t c = codes[at];
