@@ -48,6 +48,7 @@ struct mps_handle {
     uint32_t* list_fluid = nullptr;
     uint32_t* list_solid = nullptr;
     uint32_t cap_fluid = 0, cap_solid = 0;
+    uint32_t cap_flist = 1;  // fluid list entries: the fluid and a gap per gather warp at most
     SortScratch sort{};
     Scalars* sc = nullptr;
     unsigned long long* best = nullptr;
@@ -148,7 +149,7 @@ static StageArgs stage_args(mps_handle* h) {
     a.semi = h->opt.method == MPS_METHOD_SEMI_IMPLICIT;
     a.list_fluid = h->list_fluid;
     a.n_fluid = &h->sc->n_fluid;
-    a.cap_fluid = h->cap_fluid;
+    a.cap_fluid = h->cap_flist;
     a.list_solid = h->list_solid;
     a.n_solid = &h->sc->n_solid;
     a.cap_solid = h->cap_solid;
@@ -382,6 +383,15 @@ static int walk_reach(float cell_size, float cell_yz) {
     return cell_yz < cell_size ? (int)std::ceil((double)cell_size / (double)cell_yz - 1e-9) : 1;
 }
 
+// the fluid list's capacity: every fluid particle, and one gap for each warp
+// of a gather over cap particles (blocks of 256) that can hold fluid
+static uint32_t fluid_list_cap(uint32_t nfluid, uint32_t cap) {
+    const uint64_t warps = ((uint64_t)cap + 255) / 256 * 8;
+    const uint64_t gaps = warps < nfluid ? warps : nfluid;
+    const uint64_t c = (uint64_t)nfluid + gaps;
+    return c > 0 ? (uint32_t)c : 1u;
+}
+
 static Grid device_grid(const HostGrid& hg, uint32_t base) {
     Grid g;
     g.left = hg.left;
@@ -447,7 +457,8 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
     // lists never outgrow the initial counts
     h->cap_fluid = np - nb2 - nb1;
     h->cap_solid = np - nb2;
-    CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
+    h->cap_flist = fluid_list_cap(h->cap_fluid, cap);
+    CK(dalloc(h, &h->list_fluid, h->cap_flist));
     CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
     for (int b = 0; b < 2; b++) CK(dalloc(h, &h->cell_tab[b], (size_t)g.ncells + 1));
     CK(merge_setup(h));
@@ -719,7 +730,8 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
     CK(dalloc(h, &h->normal_id_of, cap));
     h->cap_fluid = nfluid;
     h->cap_solid = np - h->nb2;
-    CK(dalloc(h, &h->list_fluid, h->cap_fluid > 0 ? h->cap_fluid : 1));
+    h->cap_flist = fluid_list_cap(h->cap_fluid, cap);
+    CK(dalloc(h, &h->list_fluid, h->cap_flist));
     CK(dalloc(h, &h->list_solid, h->cap_solid > 0 ? h->cap_solid : 1));
     for (int b = 0; b < 2; b++) CK(dalloc(h, &h->cell_tab[b], (size_t)h->g.ncells + 1));
     CK(merge_setup(h));

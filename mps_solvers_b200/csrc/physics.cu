@@ -71,9 +71,13 @@ __device__ __forceinline__ uint32_t store_particle(const State& dst, Moved v, ui
 }
 
 // The end of both gathers: this warp's particles (type ty, new position p)
-// appended to the compact lists of the active fluid and non-dummy particles
-// (order within a list does not matter: every particle's stage result is
-// independent), then the last block to finish publishes the new active count.
+// appended to the compact lists of the active fluid and non-dummy particles,
+// then the last block to finish publishes the new active count.  The warps'
+// runs land in the lists in the order the warps finish, which changes from
+// run to run; every stage kernel treats its particles independently, except
+// the fast viscosity, which pairs list entries 2w and 2w + 1.  Each warp's
+// fluid run is therefore padded to an even length with a LIST_GAP entry, so
+// that a pair never spans two runs and the pairs are the same in every run.
 __device__ __forceinline__ void gather_tail(uint32_t ty, uint32_t p, uint32_t n, Scalars* __restrict__ sc,
                                             uint32_t* __restrict__ list_fluid, uint32_t* __restrict__ list_solid) {
     if (list_fluid) {
@@ -81,13 +85,15 @@ __device__ __forceinline__ void gather_tail(uint32_t ty, uint32_t p, uint32_t n,
         const bool f = ty == T_FLUID, s2 = ty == T_FLUID || ty == T_WALL;
         const uint32_t mf = __ballot_sync(0xffffffffu, f), ms = __ballot_sync(0xffffffffu, s2);
         uint32_t bf = 0, bs = 0;
+        const uint32_t nf = __popc(mf);
         if (lane == 0) {
-            if (mf) bf = atomicAdd(&sc->n_fluid, __popc(mf));
+            if (mf) bf = atomicAdd(&sc->n_fluid, nf + (nf & 1u));
             if (ms) bs = atomicAdd(&sc->n_solid, __popc(ms));
         }
         bf = __shfl_sync(0xffffffffu, bf, 0);
         bs = __shfl_sync(0xffffffffu, bs, 0);
         if (f) list_fluid[bf + __popc(mf & lt)] = p;
+        if (lane == 0 && (nf & 1u)) list_fluid[bf + nf] = LIST_GAP;
         if (s2) list_solid[bs + __popc(ms & lt)] = p;
     }
     __syncthreads();
@@ -335,8 +341,8 @@ __device__ __forceinline__ WarpTask warp_task(const StageArgs& a, const uint32_t
     WarpTask t;
     if (list) {
         const uint32_t n = *list_n;
-        t.ok = w < n;
-        t.i = t.ok ? list[w] : 0u;
+        t.i = w < n ? list[w] : LIST_GAP;
+        t.ok = t.i != LIST_GAP;
     } else {
         t.ok = w < a.sc->np;
         t.i = w;
@@ -468,9 +474,10 @@ __global__ void __launch_bounds__(256, BT ? 3 : 5) k_visc_w2(StageArgs a, const 
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nl = *list_n;
     if (2 * w >= nl) return;
-    const uint32_t i1 = list[2 * w];
-    const bool two = 2 * w + 1 < nl;
-    const uint32_t i2 = two ? list[2 * w + 1] : i1;
+    const uint32_t i1 = list[2 * w];  // never a gap: gaps sit at odd positions
+    const uint32_t i2r = 2 * w + 1 < nl ? list[2 * w + 1] : LIST_GAP;
+    const bool two = i2r != LIST_GAP;
+    const uint32_t i2 = two ? i2r : i1;
     const float4* __restrict__ pos = a.cur.pos;
     const float4* __restrict__ vel = a.cur.vel;
     const float4 p1 = pos[i1], p2 = pos[i2];

@@ -8,6 +8,10 @@
 
 namespace mpsb {
 
+// A fluid-list entry that holds no particle (it pads each gather warp's run
+// of fluid particles to an even length)
+constexpr uint32_t LIST_GAP = 0xffffffffu;
+
 // Particle state in one buffer set (sorted order).
 struct State {
     float4* pos;      // x y z, w = type bits
@@ -27,7 +31,9 @@ struct StageArgs {
     Phys P;
     bool exact;
     int semi;                  // semi-implicit (v4.0) rules
-    // compact particle lists from the last rebuild (nullptr: all particles)
+    // compact particle lists from the last rebuild (nullptr: all particles);
+    // the fluid list holds LIST_GAP entries (see gather_tail), cap_fluid
+    // counts them
     const uint32_t* list_fluid = nullptr;
     const uint32_t* n_fluid = nullptr;
     uint32_t cap_fluid = 0;
