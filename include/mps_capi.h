@@ -272,8 +272,15 @@ mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint64_t seed, 
  * in FP32 on the CUDA cores and with BF16 activations on the tensor cores
  * (tcgen05, accumulators in tensor memory), report the largest difference
  * of the factor's entries relative to the largest entry, and keep the
- * tensor cores for inference when enable != 0 (training always uses FP32). */
+ * tensor cores for inference when enable != 0 (training: the call below). */
 mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double* max_rel_diff);
+/* Training (mps_precond_loss_grad, mps_precond_train) with the network's
+ * 64 -> 64 layers on the tensor cores when enable != 0: the forward, the
+ * input gradients dx = W^T dy and the weight gradients dW = sum dy x^T
+ * (rows of the system as the contraction) with BF16 operands and FP32
+ * accumulators in tensor memory.  0, the default, trains in FP32 on the CUDA
+ * cores, the network the float64 oracle's gradients are checked against. */
+mps_status mps_precond_train_tensor_cores(mps_handle* h, int enable);
 mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
                             double* diag, uint32_t* count);
 /* The off-diagonal entries of the last assembled PPE matrix exactly as the

@@ -43,7 +43,8 @@ EXPORTS = ("mps_status_string", "mps_default_options", "mps_create", "mps_create
            "mps_autotune", "mps_surface_setup", "mps_surface_extract_async", "mps_surface_extract",
            "mps_surface_get", "mps_surface_vertex_values", "mps_surface_write_stl",
            "mps_surface_case_table", "mps_precond_tensor_cores", "mps_add_wall_motion",
-           "mps_clear_wall_motion", "mps_set_device_wait_limit", "mps_ppe_stencil", "mps_apply_tuning")
+           "mps_clear_wall_motion", "mps_set_device_wait_limit", "mps_ppe_stencil", "mps_apply_tuning",
+           "mps_precond_train_tensor_cores")
 
 
 class mps_options(C.Structure):
@@ -174,6 +175,7 @@ def lib():
             "mps_surface_write_stl": (C.c_int, [H, C.c_char_p]),
             "mps_surface_case_table": (C.c_int, [C.POINTER(C.c_uint8), C.POINTER(C.c_int8)]),
             "mps_precond_tensor_cores": (C.c_int, [H, C.c_int, C.POINTER(C.c_double)]),
+            "mps_precond_train_tensor_cores": (C.c_int, [H, C.c_int]),
         }
         for name, (rt, args) in sig.items():
             f = getattr(L, name)
@@ -409,6 +411,12 @@ class Simulation:
         d = C.c_double()
         self._check(lib().mps_precond_tensor_cores(self.h, int(enable), C.byref(d)))
         return d.value
+
+    def precond_train_tensor_cores(self, enable: bool = True):
+        """Train with the network's 64 -> 64 layers (forward, dx and dW) on
+        the tensor cores, BF16 operands and FP32 accumulation; off: FP32 on
+        the CUDA cores."""
+        self._check(lib().mps_precond_train_tensor_cores(self.h, int(enable)))
 
     def ppe_snapshot(self) -> Dict[str, np.ndarray]:
         n = self.counts()["np"]

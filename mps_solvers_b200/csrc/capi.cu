@@ -1506,6 +1506,13 @@ extern "C" mps_status mps_precond_tensor_cores(mps_handle* h, int enable, double
     return read_status(h, &sc);
 }
 
+extern "C" mps_status mps_precond_train_tensor_cores(mps_handle* h, int enable) {
+    mps_status s = need_semi(h);
+    if (s != MPS_OK) return s;
+    h->ppe.lp.train_tensor_cores = enable != 0;
+    return MPS_OK;
+}
+
 extern "C" mps_status mps_ppe_snapshot(mps_handle* h, float* pos4, float* n, uint32_t* id, uint32_t* is_row,
                                        double* diag, uint32_t* count) {
     mps_status s = need_semi(h);

@@ -864,11 +864,14 @@ constexpr uint32_t TC_SA = 0, TC_SB = TC_M * LP_H * 2, TC_SC = TC_SB + LP_H * LP
 constexpr uint32_t TC_CST = LP_H + 4;
 constexpr uint32_t TC_SMEM = TC_SC + TC_M * TC_CST * 4;
 
+// wt: multiply by W^T instead of W (the backward pass's dx = W^T dy);
+// accum: add the product to what out holds.
 __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ x, const __nv_bfloat16* __restrict__ w,
                                                       int woff, int boff, const float* __restrict__ resid,
                                                       float* __restrict__ pre_out, float* __restrict__ out, int act,
                                                       const uint32_t* __restrict__ rowlist,
-                                                      const uint32_t* __restrict__ nrows, uint32_t* __restrict__ err) {
+                                                      const uint32_t* __restrict__ nrows, uint32_t* __restrict__ err,
+                                                      int wt, int accum) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* sA = smem + TC_SA;
     uint8_t* sB = smem + TC_SB;
@@ -879,10 +882,20 @@ __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ 
     const uint32_t R = *nrows;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) failed = 0;
-    // W (n, k) into the K-major layout, N / 8 = 8 row groups
+    // B (n, k) = W (n, k), or W (k, n) with wt, into the K-major layout,
+    // N / 8 = 8 row groups
     for (uint32_t e = tid; e < LP_H * LP_H / 8; e += TC_M) {
         const uint32_t n = e / 8, kc = e % 8;  // row n, 8-element chunk kc
-        const uint4 v = *reinterpret_cast<const uint4*>(w + woff + n * LP_H + kc * 8);
+        uint4 v;
+        if (!wt) {
+            v = *reinterpret_cast<const uint4*>(w + woff + n * LP_H + kc * 8);
+        } else {
+            const unsigned short* wb = reinterpret_cast<const unsigned short*>(w + woff) + kc * 8 * LP_H + n;
+            uint32_t u[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) u[j] = (uint32_t)wb[2 * j * LP_H] | ((uint32_t)wb[(2 * j + 1) * LP_H] << 16);
+            v = make_uint4(u[0], u[1], u[2], u[3]);
+        }
         *reinterpret_cast<uint4*>(sB + (kc * 8 + n / 8) * 128 + (n % 8) * 16) = v;
     }
     if (warp == 0) {
@@ -1010,6 +1023,13 @@ __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ 
                     r.z += e.z;
                     r.w += e.w;
                 }
+                if (accum) {
+                    const float4 e = *reinterpret_cast<const float4*>(out + o);
+                    r.x += e.x;
+                    r.y += e.y;
+                    r.z += e.z;
+                    r.w += e.w;
+                }
                 *reinterpret_cast<float4*>(out + o) = r;
             }
         }
@@ -1017,6 +1037,167 @@ __global__ void __launch_bounds__(TC_M) k_lp_dense_tc(const float* __restrict__ 
         __syncthreads();
     }
     if (tid == 0 && failed) atomicOr(err, ERR_DEVICE_TIMEOUT);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+    }
+}
+
+// ---------------------------------------------------------------- tensor-core weight gradient
+// dW of a 64 -> 64 layer on the fifth-generation tensor cores (training):
+// grad[woff + 64 o + c] += sum over the rows of dy(o) x(c), and
+// grad[boff + o] += sum of dy(o) when boff >= 0.  The product is D = A B^T
+// with the rows of the system as K, 128 of them a tile: A (M = 128) holds
+// dy^T in its first 64 rows and zeros in the other 64 (written once), B
+// (N = 64) holds x^T, both BF16 in the same no-swizzle K-major core-matrix
+// layout as k_lp_dense_tc.  A persistent CTA accumulates all of its tiles in
+// one 64-column FP32 accumulator in tensor memory (lane = o), then adds it
+// to grad.  Staging: lane l of a warp takes features l and l + 32 of 8
+// consecutive rows (eight coalesced 128-byte loads per operand and feature
+// half), and writes each feature's 8 BF16 values as one 16-byte row of a
+// core matrix; a warp's stores cover 512 contiguous bytes.  Eight warps a
+// CTA, two k groups each, and two CTAs an SM keep enough loads in flight
+// (with four warps and one CTA an SM the kernel ran at 16 % of DRAM peak).
+constexpr uint32_t TW_K = 128, TW_THREADS = 256;
+constexpr uint32_t TW_SA = 0, TW_SB = TC_M * TW_K * 2, TW_SMEM = TW_SB + LP_H * TW_K * 2;
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&p);
+}
+
+__global__ void __launch_bounds__(TW_THREADS) k_lp_wgrad_tc(const float* __restrict__ dy, const float* __restrict__ x,
+                                                      int woff, int boff, float* __restrict__ grad,
+                                                      const uint32_t* __restrict__ rowlist,
+                                                      const uint32_t* __restrict__ nrows, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sA = smem + TW_SA;
+    uint8_t* sB = smem + TW_SB;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    const uint32_t R = *nrows;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) failed = 0;
+    // rows 64 .. 127 of A are zero: (k group, row) units of 16 bytes
+    for (uint32_t e = tid; e < (TW_K / 8) * 64; e += TW_THREADS) {
+        const uint32_t kg = e / 64, m = 64 + e % 64;
+        *reinterpret_cast<uint4*>(sA + (kg * (TC_M / 8) + m / 8) * 128 + (m % 8) * 16) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(64));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    float db0 = 0.f, db1 = 0.f;  // bias gradient of features lane and lane + 32
+    uint32_t phase = 0, ntile = 0;
+    const uint32_t ntiles = (R + TW_K - 1) / TW_K;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // warp w stages the k groups 2w and 2w + 1 of the tile
+#pragma unroll 1
+        for (uint32_t g = 0; g < 2; g++) {
+            const uint32_t kg = warp * 2 + g;
+            float a0[8], a1[8], b0[8], b1[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const uint32_t k = tile * TW_K + kg * 8 + j;
+                if (k < R) {
+                    const size_t o = (size_t)__ldg(rowlist + k) * LP_H + lane;
+                    a0[j] = __ldg(dy + o);
+                    a1[j] = __ldg(dy + o + 32);
+                    b0[j] = __ldg(x + o);
+                    b1[j] = __ldg(x + o + 32);
+                } else {
+                    a0[j] = a1[j] = b0[j] = b1[j] = 0.f;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                db0 += a0[j];
+                db1 += a1[j];
+            }
+            const uint32_t lo = (lane / 8) * 128 + (lane % 8) * 16, hi = lo + 4 * 128;  // features l, l + 32
+            uint8_t* ra = sA + kg * (TC_M / 8) * 128;
+            uint8_t* rb = sB + kg * (LP_H / 8) * 128;
+            *reinterpret_cast<uint4*>(ra + lo) = make_uint4(pack_bf16x2(a0[0], a0[1]), pack_bf16x2(a0[2], a0[3]),
+                                                            pack_bf16x2(a0[4], a0[5]), pack_bf16x2(a0[6], a0[7]));
+            *reinterpret_cast<uint4*>(ra + hi) = make_uint4(pack_bf16x2(a1[0], a1[1]), pack_bf16x2(a1[2], a1[3]),
+                                                            pack_bf16x2(a1[4], a1[5]), pack_bf16x2(a1[6], a1[7]));
+            *reinterpret_cast<uint4*>(rb + lo) = make_uint4(pack_bf16x2(b0[0], b0[1]), pack_bf16x2(b0[2], b0[3]),
+                                                            pack_bf16x2(b0[4], b0[5]), pack_bf16x2(b0[6], b0[7]));
+            *reinterpret_cast<uint4*>(rb + hi) = make_uint4(pack_bf16x2(b1[0], b1[1]), pack_bf16x2(b1[2], b1[3]),
+                                                            pack_bf16x2(b1[4], b1[5]), pack_bf16x2(b1[6], b1[7]));
+        }
+        asm volatile("fence.proxy.async.shared::cta;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int kk = 0; kk < (int)(TW_K / 16); kk++) {
+                const uint64_t da = umma_desc(smem_addr(sA) + kk * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
+                const uint64_t dbd = umma_desc(smem_addr(sB) + kk * 2 * (LP_H / 8) * 128, (LP_H / 8) * 128, 128);
+                const uint32_t acc = (ntile > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(dbd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_addr(&mbar)));
+        }
+        // bounded wait for this tile's MMAs (they read the staged operands)
+        {
+            uint32_t done = 0;
+            for (uint32_t spin = 0; spin < (1u << 22) && !done; spin++) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(smem_addr(&mbar)), "r"(phase));
+                if (!done) __nanosleep(20);
+            }
+            if (!done) failed = 1;
+        }
+        phase ^= 1u;
+        ntile++;
+        __syncthreads();
+        if (failed) break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // accumulator rows 0 .. 63 (TMEM lanes of warps 0 and 1) through shared
+    // memory (the A tile's space, stride 65 floats) to coalesced atomics
+    float* sD = reinterpret_cast<float*>(sA);
+    const bool have = ntile > 0 && !failed;
+    if (have && warp < 2) {
+        float v[LP_H];
+        const uint32_t lane_base = (warp * 32u) << 16;
+#pragma unroll
+        for (int c = 0; c < LP_H / 16; c++) tmem_ld16(tmem + lane_base + c * 16, v + 16 * c);
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+        for (int c = 0; c < LP_H; c++) sD[tid * (LP_H + 1) + c] = v[c];
+    }
+    __syncthreads();
+    if (have) {
+        for (uint32_t t = tid; t < LP_H * LP_H; t += TW_THREADS)
+            atomicAdd(grad + woff + t, sD[(t / LP_H) * (LP_H + 1) + t % LP_H]);
+        if (boff >= 0) {
+            atomicAdd(grad + boff + lane, db0);
+            atomicAdd(grad + boff + lane + 32, db1);
+        }
+    }
+    if (tid == 0 && failed) atomicOr(err, ERR_DEVICE_TIMEOUT);
+    asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -1158,28 +1339,40 @@ void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStrea
                                                              const_cast<Scalars*>(S.sc));
 }
 
-void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
-                bool pack_factor) {
-    (void)exact;
-    const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
-    const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
-    const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;
-    // one resident wave of the tensor-core kernel (it loops over the tiles)
-    static uint32_t tc_resident = 0;
-    if (tensor_cores && tc_resident == 0) {
+// Grids of the tensor-core kernels: one resident wave of k_lp_dense_tc (it
+// loops over the tiles) and two CTAs an SM for k_lp_wgrad_tc (few partial
+// accumulators to add up, enough loads in flight).
+struct TcGrids {
+    uint32_t dense, wgrad;
+};
+static TcGrids tc_grids(uint32_t cap) {
+    static uint32_t resident = 0, sms_seen = 0;
+    if (resident == 0) {
         cudaFuncSetAttribute(k_lp_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+        cudaFuncSetAttribute(k_lp_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TW_SMEM);
         int per_sm = 0, dev = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lp_dense_tc, TC_M, TC_SMEM);
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        tc_resident = (uint32_t)((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 148));
+        sms_seen = (uint32_t)(sms > 0 ? sms : 148);
+        resident = (uint32_t)(per_sm > 0 ? per_sm : 1) * sms_seen;
     }
-    const uint32_t tgrid = blocks_for(cap, TC_M) < tc_resident ? blocks_for(cap, TC_M) : tc_resident;
+    const uint32_t t = blocks_for(cap, TC_M), w = blocks_for(cap, TW_K);
+    return TcGrids{t < resident ? t : resident, w < 2 * sms_seen ? w : 2 * sms_seen};
+}
+
+void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
+                bool pack_factor, bool keep_pre) {
+    (void)exact;
+    const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
+    const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
+    const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;
+    const uint32_t tgrid = tensor_cores ? tc_grids(cap).dense : 0u;
     uint32_t* err = const_cast<uint32_t*>(&S.sc->err);
     auto dense = [&](const float* x, int woff, int boff, const float* resid, float* pre, float* out, int act) {
-        if (tensor_cores)  // inference only: the pre-activations feed nothing but the backward pass
-            k_lp_dense_tc<<<tgrid, TC_M, TC_SMEM, st>>>(x, L.w16, woff, boff, resid, nullptr, out, act, S.rowlist,
-                                                        S.nrows, err);
+        if (tensor_cores)  // the pre-activations feed nothing but the backward pass
+            k_lp_dense_tc<<<tgrid, TC_M, TC_SMEM, st>>>(x, L.w16, woff, boff, resid, keep_pre ? pre : nullptr, out,
+                                                        act, S.rowlist, S.nrows, err, 0, 0);
         else
             k_lp_dense_fwd<<<dgrid, 256, 0, st>>>(x, L.w16, woff, boff, resid, pre, out, act, S.rowlist, S.nrows);
     };
@@ -1266,10 +1459,27 @@ int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, u
     // the stencil of this system (a step may have kept an older one between
     // network evaluations)
     lp_build_stencil(L, S, cap, st);
-    lp_forward(L, S, exact, cap, st, false);  // training: FP32 activations (the oracle's network)
+    // training: FP32 activations on the CUDA cores (the oracle's network), or
+    // the 64 -> 64 layers' forward, dx and dW products on the tensor cores
+    const bool tc = L.train_tensor_cores;
+    lp_forward(L, S, exact, cap, st, tc, true, true);
     const uint32_t tb = blocks_for(cap, 256), wb = blocks_for(cap * 32u, 256);
     const uint32_t db = blocks_for(cap, 4);
     const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;
+    const TcGrids tg = tc ? tc_grids(cap) : TcGrids{0u, 0u};
+    uint32_t* err = const_cast<uint32_t*>(&S.sc->err);
+    // dx (+)= W^T dy, grad(W) += dy x^T, grad(b) += dy (boff >= 0)
+    auto dense_bwd = [&](const float* dy, const float* x, int woff, float* dx, int accumulate, int boff) {
+        if (tc) {
+            k_lp_dense_tc<<<tg.dense, TC_M, TC_SMEM, st>>>(dy, L.w16, woff, -1, nullptr, nullptr, dx, 0, S.rowlist,
+                                                           S.nrows, err, 1, accumulate);
+            k_lp_wgrad_tc<<<tg.wgrad, TW_THREADS, TW_SMEM, st>>>(dy, x, woff, boff, L.grad, S.rowlist, S.nrows,
+                                                                 err);
+        } else {
+            k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(dy, x, L.w16, woff, dx, accumulate, L.grad, boff, S.rowlist,
+                                                  S.nrows);
+        }
+    };
     cudaMemsetAsync(L.grad, 0, LP_NPARAM * 4, st);
     cudaMemsetAsync(L.loss, 0, 4 * sizeof(double), st);
     // Kaporin's condition number of G Ahat G^T with a Rademacher probe z:
@@ -1307,19 +1517,19 @@ int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, u
     B.grad = L.grad;
     k_lp_readout_bwd_a<<<wb, 256, 0, st>>>(B);
     k_lp_readout_bwd_b<<<wb, 256, 0, st>>>(B);
-    k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.dra, L.h2, L.w16, LP_RA, L.dh2, 1, L.grad, -1, S.rowlist, S.nrows);
-    k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.drb, L.h2, L.w16, LP_RB, L.dh2, 1, L.grad, -1, S.rowlist, S.nrows);
+    dense_bwd(L.dra, L.h2, LP_RA, L.dh2, 1, -1);
+    dense_bwd(L.drb, L.h2, LP_RB, L.dh2, 1, -1);
     // second message pass, node: h2 = GELU(pre2) + h1
     const uint32_t eb = blocks_for(cap * (uint32_t)LP_H, 256);
     k_lp_copy_rows<<<eb, 256, 0, st>>>(L.dh2, L.dh1, S.rowlist, S.nrows);
     k_lp_gelu_bwd<<<eb, 256, 0, st>>>(L.dh2, L.pre2, L.dra, S.rowlist, S.nrows);  // dra reused as dpre2
-    k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.dra, L.a2, L.w16, LP_V2, L.da, 0, L.grad, LP_C2, S.rowlist, S.nrows);
+    dense_bwd(L.dra, L.a2, LP_V2, L.da, 0, LP_C2);
     k_lp_edge_bwd_a<2><<<wb, 256, 0, st>>>(B);
     k_lp_edge2_bwd_b<<<wb, 256, 0, st>>>(B, L.duh1);
-    k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.duh1, L.h1, L.w16, LP_U2, L.dh1, 1, L.grad, -1, S.rowlist, S.nrows);
+    dense_bwd(L.duh1, L.h1, LP_U2, L.dh1, 1, -1);
     // first message pass, node: h1 = GELU(pre1)
     k_lp_gelu_bwd<<<eb, 256, 0, st>>>(L.dh1, L.pre1, L.dra, S.rowlist, S.nrows);  // dpre1
-    k_lp_dense_bwd<<<dgrid, 256, 0, st>>>(L.dra, L.a1, L.w16, LP_V1, L.da, 0, L.grad, LP_C1, S.rowlist, S.nrows);
+    dense_bwd(L.dra, L.a1, LP_V1, L.da, 0, LP_C1);
     k_lp_edge_bwd_a<1><<<wb, 256, 0, st>>>(B);
     return MPS_OK;
 }

@@ -66,6 +66,7 @@ enum : int {
 struct LearnedWork {
     bool ready = false;
     bool tensor_cores = false;       // inference forward on tcgen05 (set after a self-check)
+    bool train_tensor_cores = false; // training's 64 -> 64 products on tcgen05 (BF16 operands)
     uint32_t cap = 0;
     // parameters
     float* w32 = nullptr;            // FP32 master
@@ -145,10 +146,11 @@ struct LpSystem {            // the assembled PPE system the network works on
 // neighbours within r0 of every non-Dirichlet row, and D^-1/2
 void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStream_t st);
 // network forward on the built stencil -> gdiag, gval (G and G^T values);
-// tensor_cores: the 64 -> 64 layers on tcgen05 with BF16 activations
-// (inference), else in FP32 on the CUDA cores (training)
+// tensor_cores: the 64 -> 64 layers on tcgen05 with BF16 activations, else
+// in FP32 on the CUDA cores; keep_pre: store the pre-activations for the
+// backward pass (the CUDA-core forward always does)
 void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
-                bool pack_factor = true);
+                bool pack_factor = true, bool keep_pre = false);
 // loss sums (L.loss = {z^T M z, sum log G_ii}) and the parameter gradient
 // (L.grad) for a probe seed; the loss is lp_loss_value of those sums
 int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, uint32_t cap, cudaStream_t st);

@@ -9,7 +9,11 @@ every step the network takes `--iters-per-step` Adam steps on that step's
 PPE system, each with a new Rademacher probe.  Defaults: 50 scenes x 400
 steps = 20,000 PPE systems.
 
-    python -m mps_solvers_b200.train_precond [--scenes 50] [--steps 400]
+    python -m mps_solvers_b200.train_precond [--scenes 50] [--steps 400] [--tensor-cores]
+
+--tensor-cores trains with the network's 64 -> 64 layers (forward, input
+and weight gradients) on the tensor cores, BF16 operands and FP32
+accumulation; without it training runs in FP32 on the CUDA cores.
 """
 from __future__ import annotations
 
@@ -70,6 +74,8 @@ def main():
     ap.add_argument("--log", default=None)
     ap.add_argument("--init", default=None, help="start from these weights (.npy)")
     ap.add_argument("--eval-only", action="store_true", help="only compare --init with diagonal scaling")
+    ap.add_argument("--tensor-cores", action="store_true", help="train the 64 -> 64 layers on tcgen05 (BF16)")
+    ap.add_argument("--no-eval", action="store_true", help="skip the held-out comparison at the end")
     args = ap.parse_args()
     w = precond_weights.load(args.init) if args.init else None
     if args.eval_only:
@@ -89,6 +95,7 @@ def main():
                         w = _initial_params()
                     # enables the learned stencil; the solve keeps diagonal scaling
                     s.set_precond_params(w)
+                    s.precond_train_tensor_cores(args.tensor_cores)
                     for step in range(args.steps):
                         s.step(1)
                         a, _ = s.precond_train(args.iters_per_step, args.lr, seed=(k << 20) + step * 16)
@@ -103,8 +110,9 @@ def main():
         log.append(rec)
         print(json.dumps(rec), flush=True)
         np.save(args.out, w.astype(np.float32))
-    ev = evaluate(w)
-    print(json.dumps(dict(evaluation=ev)), flush=True)
+    ev = None if args.no_eval else evaluate(w)
+    if ev is not None:
+        print(json.dumps(dict(evaluation=ev)), flush=True)
     if args.log:
         with open(args.log, "w") as f:
             json.dump(dict(training=log, evaluation=ev), f, indent=1)
