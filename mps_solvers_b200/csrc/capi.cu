@@ -184,12 +184,13 @@ static void mark(mps_handle* h, int tag) {
 // The merge rebuild (cellsort.cuh) when at most MERGE_SMEM_CAP particles can
 // change cell between two rebuilds (fluid and moving walls) and the current
 // order is a sorted one; else the full radix sort.  Both give the same order.
-// The compact PPE layout on or off; with the learned preconditioner it
-// carries the learned symmetric form (the factor form needs the 8-byte
-// layout).
+// The compact PPE layout on or off; with the learned preconditioner the
+// compact solver applies S' by compact columns (the 8-byte solver by
+// particle columns).
 static void set_compact(mps_handle* h, bool on) {
     h->ppe.c16 = on && h->ppe.c16_ready;
-    h->ppe.c16_learned = h->ppe.c16 && h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.sp_ent != nullptr;
+    h->ppe.c16_learned = h->ppe.c16 && h->opt.precond == MPS_PRECOND_LEARNED && h->ppe.sp_ent != nullptr &&
+                         h->ppe.cr2 != nullptr;
 }
 
 static bool use_merge(const mps_handle* h) {
@@ -577,6 +578,7 @@ static mps_status setup(mps_handle* h, const mps_params& prm, uint32_t np, uint3
         h->ppe.l2_keep_entries = h->opt.ppe_l2_keep_mb < 0 ? 0xFFFFFFFFu : (uint32_t)(keep_bytes / 8);
         if (h->opt.precond == MPS_PRECOND_LEARNED) {
             e = ppe_enable_learned(h->ppe, &h->err);
+            if (e == MPS_OK) e = ppe_sp_enable(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
         }
         if (h->opt.ppe_layout != 0 && h->opt.ppe_layout != -1) {
@@ -890,8 +892,11 @@ static mps_status setup_batch(mps_handle* h, const std::vector<mps_params>& prms
         if (e != MPS_OK) return (mps_status)e;
         e = ppe_setup_batch(h->ppe, ppe_scenes.data(), S, h->stream, &h->err);
         if (e != MPS_OK) return (mps_status)e;
+        h->ppe.precond_every = h->opt.precond_every > 0 ? h->opt.precond_every : 40;
+        h->ppe.index_of_id = h->index_of_id;
         if (h->opt.precond == MPS_PRECOND_LEARNED) {
             e = ppe_enable_learned(h->ppe, &h->err);
+            if (e == MPS_OK) e = ppe_sp_enable(h->ppe, &h->err);
             if (e != MPS_OK) return (mps_status)e;
         }
     }
@@ -1084,10 +1089,12 @@ extern "C" const char* mps_last_error(mps_handle* h) { return h ? h->err.c_str()
 
 // ---------------------------------------------------------------- stepping
 // Before every step: whether it evaluates the learned network (the learned
-// compact preconditioner re-evaluates it every precond_every steps); false
-// for every other configuration.
+// preconditioner re-evaluates it every precond_every steps); false for every
+// other configuration.
 static bool begin_step(mps_handle* h) {
-    if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT || !h->ppe.c16_learned) return false;
+    if (h->opt.method != MPS_METHOD_SEMI_IMPLICIT || h->opt.precond != MPS_PRECOND_LEARNED || !h->ppe.lp.ready ||
+        !h->ppe.sp_ent)
+        return false;
     return ppe_begin_step(h->ppe);
 }
 
@@ -1457,8 +1464,10 @@ extern "C" mps_status mps_precond_train(mps_handle* h, int iters, float lr, uint
         }
         lp_adam(h->ppe.lp, lr, h->stream);
     }
-    // refresh G for the current system with the updated weights
+    // refresh G for the current system with the updated weights; the next
+    // step rebuilds the preconditioner from them
     lp_forward(h->ppe.lp, L, h->opt.arith == MPS_ARITH_EXACT, h->cap, h->stream, h->ppe.lp.tensor_cores);
+    h->ppe.lp.s_ready = false;
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaGetLastError());
     if (loss_first) *loss_first = first;

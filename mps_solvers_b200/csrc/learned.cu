@@ -739,82 +739,6 @@ __global__ void k_lp_to_bf16(const float* __restrict__ w, __nv_bfloat16* __restr
     if (k < n) w16[k] = __float2bfloat16(w[k]);
 }
 
-// ---------------------------------------------------------------- solve layout
-// widths (entries including the diagonal) x LP_SLICE of every slice of the
-// lower and upper packed factors; entry maxslices is 0 (the scan's total)
-__global__ void __launch_bounds__(256) k_lp_slice_width(const uint32_t* __restrict__ scnt, const uint32_t* __restrict__ nlow,
-                                                        const uint32_t* __restrict__ rowlist,
-                                                        const uint32_t* __restrict__ nrows, uint32_t* __restrict__ lo_off,
-                                                        uint32_t* __restrict__ up_off, uint32_t maxslices) {
-    const uint32_t R = *nrows;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s > maxslices) return;
-    uint32_t ml = 0, mu = 0;
-    for (uint32_t r = 0; r < LP_SLICE; r++) {
-        const uint32_t k = s * LP_SLICE + r;
-        if (k < R) {
-            const uint32_t i = rowlist[k];
-            const uint32_t nl = nlow[i];
-            ml = max(ml, nl + 1u);
-            mu = max(mu, scnt[i] - nl + 1u);
-        }
-    }
-    lo_off[s] = ml * LP_SLICE;
-    up_off[s] = mu * LP_SLICE;
-}
-
-// G'_ij = G_ij d_j (row i: the diagonal, then its j < i entries) and
-// G'_ji = G_ji d_i (column i: the diagonal, then its j > i entries), padded
-// with (i, 0) to the slice width
-__global__ void __launch_bounds__(256) k_lp_pack(const uint32_t* __restrict__ scols, const uint32_t* __restrict__ scnt,
-                                                 const uint32_t* __restrict__ nlow, const float* __restrict__ gval,
-                                                 const float* __restrict__ gdiag, const float* __restrict__ dinv,
-                                                 const uint32_t* __restrict__ rowlist, const uint32_t* __restrict__ nrows,
-                                                 const uint32_t* __restrict__ lo_off, const uint32_t* __restrict__ up_off,
-                                                 uint32_t* __restrict__ lo_cols, float* __restrict__ lo_vals,
-                                                 uint32_t* __restrict__ up_cols, float* __restrict__ up_vals) {
-    const uint32_t R = *nrows;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t sl = k / LP_SLICE, ln = k % LP_SLICE;
-    if (sl >= (R + LP_SLICE - 1) / LP_SLICE) return;
-    const bool has = k < R;
-    const uint32_t i = rowlist[has ? k : sl * LP_SLICE];
-    const uint32_t nl = has ? nlow[i] : 0u, cnt = has ? scnt[i] : 0u;
-    const float di = dinv[i];
-    const float gd = has ? gdiag[i] * di : 0.f;
-    const size_t row = (size_t)i * LP_GW;
-    {
-        const uint32_t base = lo_off[sl], W = (lo_off[sl + 1] - base) / LP_SLICE;
-        lo_cols[base + ln] = i;
-        lo_vals[base + ln] = gd;
-        for (uint32_t t = 1; t < W; t++) {
-            uint32_t c = i;
-            float v = 0.f;
-            if (t - 1 < nl) {
-                c = scols[row + t - 1];
-                v = gval[row + t - 1] * dinv[c];
-            }
-            lo_cols[base + t * LP_SLICE + ln] = c;
-            lo_vals[base + t * LP_SLICE + ln] = v;
-        }
-    }
-    {
-        const uint32_t base = up_off[sl], W = (up_off[sl + 1] - base) / LP_SLICE;
-        up_cols[base + ln] = i;
-        up_vals[base + ln] = gd;
-        for (uint32_t t = 1; t < W; t++) {
-            uint32_t c = i;
-            float v = 0.f;
-            if (nl + t - 1 < cnt) {
-                c = scols[row + nl + t - 1];
-                v = gval[row + nl + t - 1] * di;
-            }
-            up_cols[base + t * LP_SLICE + ln] = c;
-            up_vals[base + t * LP_SLICE + ln] = v;
-        }
-    }
-}
-
 // ---------------------------------------------------------------- tensor-core dense layer
 // The same 64 -> 64 layer on the fifth-generation tensor cores (inference):
 // out = act(x W^T + b) + resid for a tile of 128 rows per step of a
@@ -1228,13 +1152,6 @@ int lp_setup(LearnedWork& L, uint32_t cap, std::string* err) {
     for (float** p : nodes) al((void**)p, NH * 4);
     al((void**)&L.dgpre, N * 4);
     al((void**)&L.dinv, N * 4);
-    const size_t nsl = N / LP_SLICE + 2, NP = (N + LP_SLICE) * (LP_GW + 1);
-    al((void**)&L.lo_off, nsl * 4);
-    al((void**)&L.up_off, nsl * 4);
-    al((void**)&L.lo_cols, NP * 4);
-    al((void**)&L.up_cols, NP * 4);
-    al((void**)&L.lo_vals, NP * 4);
-    al((void**)&L.up_vals, NP * 4);
     if (!ok) {
         *err = "cudaMalloc failed for the learned preconditioner";
         return MPS_ERR_CUDA;
@@ -1270,7 +1187,6 @@ void lp_free(LearnedWork& L) {
     void* ps[] = {L.s_cnt, L.s_col, L.s_val, L.s_diag,
                   L.w32, L.w16, L.grad, L.adam_m, L.adam_v, L.scols, L.scnt, L.nlow, L.gdiag, L.gval,
                   L.a1,  L.pre1, L.h1,  L.uh1,  L.a2,  L.pre2, L.h2,  L.ra,   L.rb,  L.dgpre, L.dinv,
-                  L.lo_off, L.up_off, L.lo_cols, L.up_cols, L.lo_vals, L.up_vals,
                   L.dh1, L.dh2, L.dra,  L.drb,  L.duh1, L.da,  L.dgval, L.dgdiag, L.z, L.v1, L.v2,
                   L.loss};
     for (void* p : ps)
@@ -1362,7 +1278,7 @@ static TcGrids tc_grids(uint32_t cap) {
 }
 
 void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
-                bool pack_factor, bool keep_pre) {
+                bool keep_pre) {
     (void)exact;
     const uint32_t wb = blocks_for(cap * 32u, 256);   // warp per row
     const uint32_t db = blocks_for(cap, 4);           // 4 rows per dense block
@@ -1386,16 +1302,6 @@ void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cud
     dense(L.h2, LP_RB, -1, nullptr, nullptr, L.rb, 0);
     k_lp_readout_fwd<<<wb, 256, 0, st>>>(A);
     k_lp_transpose<<<blocks_for(cap, 256), 256, 0, st>>>(L.scols, L.scnt, L.nlow, L.gval, S.rowlist, S.nrows);
-    if (!pack_factor) return;
-    // the solve layout
-    const uint32_t maxslices = (cap + LP_SLICE - 1) / LP_SLICE;
-    k_lp_slice_width<<<blocks_for(maxslices + 1, 256), 256, 0, st>>>(L.scnt, L.nlow, S.rowlist, S.nrows, L.lo_off,
-                                                                     L.up_off, maxslices);
-    launch_scan_exclusive(L.lo_off, maxslices + 1, st);
-    launch_scan_exclusive(L.up_off, maxslices + 1, st);
-    k_lp_pack<<<blocks_for(maxslices * LP_SLICE, 256), 256, 0, st>>>(L.scols, L.scnt, L.nlow, L.gval, L.gdiag, L.dinv,
-                                                                    S.rowlist, S.nrows, L.lo_off, L.up_off, L.lo_cols,
-                                                                    L.lo_vals, L.up_cols, L.up_vals);
 }
 
 // ---------------------------------------------------------------- symmetric form
@@ -1462,7 +1368,7 @@ int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, u
     // training: FP32 activations on the CUDA cores (the oracle's network), or
     // the 64 -> 64 layers' forward, dx and dW products on the tensor cores
     const bool tc = L.train_tensor_cores;
-    lp_forward(L, S, exact, cap, st, tc, true, true);
+    lp_forward(L, S, exact, cap, st, tc, true);
     const uint32_t tb = blocks_for(cap, 256), wb = blocks_for(cap * 32u, 256);
     const uint32_t db = blocks_for(cap, 4);
     const uint32_t dgrid = db < 148u * 8u ? db : 148u * 8u;

@@ -27,6 +27,10 @@
 // sparsity pattern its minimiser is the factorized sparse approximate inverse
 // (Kolotilina and Yeremin, 1993); CG's iteration bound follows beta
 // (Kaporin, 1994).
+//
+// The solvers apply the symmetric first-order form S of G^T G (below),
+// scaled to S' = D^-1/2 S D^-1/2: one product a PCG iteration, fused into
+// the residual update.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -94,13 +98,6 @@ struct LearnedWork {
     float *z = nullptr, *v1 = nullptr, *v2 = nullptr;
     double* loss = nullptr;          // [4]: z^T M z, sum log G_ii
     float* dinv = nullptr;           // D^-1/2 per particle
-    // the factor as the PCG applies it, M^-1 = G'^T G' with G' = G D^-1/2:
-    // sliced ELL over the ordered rows (slices of LP_SLICE rows, entry t of
-    // row position k at off[k / LP_SLICE] + t * LP_SLICE + k % LP_SLICE),
-    // diagonal first.  lo: row i of G'; up: column i of G' (the G_ji).
-    uint32_t *lo_off = nullptr, *up_off = nullptr;
-    uint32_t *lo_cols = nullptr, *up_cols = nullptr;
-    float *lo_vals = nullptr, *up_vals = nullptr;
     // The symmetric first-order form of G^T G on G's own pattern (both
     // triangles), S = G_d^2 + G_d G_L + G_L^T G_d (G_d the diagonal, G_L the
     // strict lower part), with the diagonal raised where needed so that S is
@@ -112,8 +109,6 @@ struct LearnedWork {
     float* s_diag = nullptr;         // cap: S_ii
     bool s_ready = false;            // built at least once
 };
-
-constexpr uint32_t LP_SLICE = 32;
 
 int lp_setup(LearnedWork& L, uint32_t cap, std::string* err);
 void lp_free(LearnedWork& L);
@@ -150,7 +145,7 @@ void lp_build_stencil(LearnedWork& L, const LpSystem& S, uint32_t cap, cudaStrea
 // in FP32 on the CUDA cores; keep_pre: store the pre-activations for the
 // backward pass (the CUDA-core forward always does)
 void lp_forward(LearnedWork& L, const LpSystem& S, bool exact, uint32_t cap, cudaStream_t st, bool tensor_cores,
-                bool pack_factor = true, bool keep_pre = false);
+                bool keep_pre = false);
 // loss sums (L.loss = {z^T M z, sum log G_ii}) and the parameter gradient
 // (L.grad) for a probe seed; the loss is lp_loss_value of those sums
 int lp_loss_grad(LearnedWork& L, const LpSystem& S, bool exact, uint64_t seed, uint32_t cap, cudaStream_t st);

@@ -161,14 +161,10 @@ struct SolveArgs {
     const float* sw;          // stored weights (same layout as scols)
     const float4* pos;
     float rlap, rlap_thr;
-    // learned preconditioner
-    const uint32_t* lo_off;   // G' rows, sliced ELL (learned.cuh)
-    const uint32_t* lo_cols;
-    const float* lo_vals;
-    const uint32_t* up_off;   // G' columns
-    const uint32_t* up_cols;
-    const float* up_vals;
-    float* y;
+    // learned preconditioner S' by particle columns (ppe_device.cuh)
+    const uint32_t* sp_off;
+    const uint32_t* sp_ent;
+    const float* sp_diag;
     float* ralt;
     Scalars* sc;
     double tol;
@@ -204,21 +200,6 @@ __device__ __forceinline__ float4 chunk_weights(const float4* __restrict__ w4, u
         return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
     };
     return make_float4(one(c.x), one(c.y), one(c.z), one(c.w));
-}
-
-// Row position k of the learned factor's packed layout: sum over its
-// entries of val * x(col), x given as a functor of the column.
-template <class X>
-__device__ __forceinline__ float lp_packed_row(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cols,
-                                               const float* __restrict__ vals, uint32_t k, X x) {
-    const uint32_t base = __ldg(off + k / LP_SLICE) + k % LP_SLICE;
-    const uint32_t W = (__ldg(off + k / LP_SLICE + 1) - __ldg(off + k / LP_SLICE)) / LP_SLICE;
-    float s = 0.f;
-    for (uint32_t t = 0; t < W; t++) {
-        const uint32_t e = base + t * LP_SLICE;
-        s = fmaf(__ldg(vals + e), x(__ldg(cols + e)), s);
-    }
-    return s;
 }
 
 // SW: stored weights (the pack's) instead of recomputing them from the
@@ -346,21 +327,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         }
         if (total >= S.max_iter) break;
         if (PREC == 1) {
-            // z = D^-1/2 G^T G D^-1/2 r: y = G D^-1/2 r, then z from y
-            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
-                const uint32_t i = __ldg(rowlist + kk);
-                const float* r = S.r;
-                S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r](uint32_t j) { return r[j]; });
-            }
-            double dummy[1] = {0.0}, td[1];
-            if (!grid_reduce<1>(dummy, S.part, S.result, S.bar, S.sc, td)) return;
+            // z = S' r of the new residual, r.z
             double rzp[1] = {0.0};
+            const float* r = S.r;
             for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                 const uint32_t i = __ldg(rowlist + kk);
-                const float* y = S.y;
-                const float zi = lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r](uint32_t j) { return r[j]; });
                 zc[i].x = zi;
-                rzp[0] += (double)S.r[i] * (double)zi;
+                rzp[0] += (double)r[i] * (double)zi;
             }
             double tz[1];
             if (!grid_reduce<1>(rzp, S.part, S.result, S.bar, S.sc, tz)) return;
@@ -459,37 +433,26 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 }
                 if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
             } else {
-                // new residual into the second buffer; y = G D^-1/2 r_new with
-                // the neighbours' r_new recomputed from r and q
+                // z = S' r_new with each neighbour's r_new = r - alpha q formed
+                // on the fly; the new residual into the second buffer (the
+                // neighbours read the old one); r.z and r.r
                 float* rnew = S.ralt;
+                const float* r = S.r;
+                const SolveArgs& SS = S;
                 for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                     const uint32_t i = __ldg(rowlist + kk);
                     const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
-                    const float ri = fmaf(-alpha_f, q_total(S, i, parts), S.r[i]);
+                    const float ri = fmaf(-alpha_f, q_total(S, i, parts), r[i]);
                     rnew[i] = ri;
-                    const float* r = S.r;
-                    const SolveArgs& SS = S;
-                    S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r, &SS, alpha_f, parts](uint32_t j) {
+                    const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r, &SS, alpha_f, parts](uint32_t j) {
                         return fmaf(-alpha_f, q_total(SS, j, parts), r[j]);
                     });
+                    zn[i] = make_float2(zi, pn);
+                    acc2[0] += (double)ri * (double)zi;
                     acc2[1] += (double)ri * (double)ri;
                 }
-                double rrp[1] = {acc2[1]}, trr[1];
-                if (!grid_reduce<1>(rrp, S.part, S.result, S.bar, S.sc, trr)) return;
-                double rzp[1] = {0.0};
-                for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
-                    const uint32_t i = __ldg(rowlist + kk);
-                    const float* y = S.y;
-                    const float zi =
-                        lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
-                    zn[i].x = zi;
-                    rzp[0] += (double)rnew[i] * (double)zi;
-                }
-                double trz[1];
-                if (!grid_reduce<1>(rzp, S.part, S.result, S.bar, S.sc, trz)) return;
-                tot2[0] = trz[0];
-                tot2[1] = trr[0];
+                if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
                 // swap the residual buffers
                 S.ralt = S.r;
                 S.r = rnew;
@@ -759,14 +722,12 @@ struct BatchSolveArgs {
     int* iters;
     int* outers;
     double* relres;
-    // learned preconditioner: G' rows and columns (learned.cuh), y = G' r
-    const uint32_t* lo_off;
-    const uint32_t* lo_cols;
-    const float* lo_vals;
-    const uint32_t* up_off;
-    const uint32_t* up_cols;
-    const float* up_vals;
-    float* y;
+    // learned preconditioner S' by particle columns (ppe_device.cuh) and the
+    // second residual buffer of its update
+    const uint32_t* sp_off;
+    const uint32_t* sp_ent;
+    const float* sp_diag;
+    float* ralt;
     uint32_t ns;
     double tol;
     double eta_min;
@@ -883,13 +844,18 @@ __device__ __forceinline__ float batch_weight(const float4* __restrict__ pos, fl
     return (j != i && rr < thr) ? weight_rr<EX>(rlap, rr) : 0.f;
 }
 
-// PREC 0: diagonal scaling; PREC 1: the learned factor, M^-1 = G'^T G'
-// (G' = G D^-1/2; neighbours of a row are rows of its own scene, so y = G'r
-// and z = G'^T y run over all rows of the scenes still iterating at once).
+// PREC 0: diagonal scaling; PREC 1: the learned S' (neighbours of a row are
+// rows of its own scene, so one pass of z = S' r serves all scenes still
+// iterating; each neighbour's new residual is formed on the fly with its
+// scene's alpha, the row's own goes to the second residual buffer).  Both
+// keep two grid-wide reductions per iteration.  The residual buffers swap
+// after every iteration; the rows of a scene that sits the iteration out
+// keep theirs in the other buffer, which is harmless: a scene becomes active
+// again only after the next FP64 pass, which rewrites the residual of every
+// open scene's rows into the current buffer.
 template <bool EX, bool SW, int PREC>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs S) {
     __shared__ double acc[3 * PPE_MAX_SCENES];
-    __shared__ double rrn[PREC == 1 ? PPE_MAX_SCENES : 1];
     __shared__ double rz[PPE_MAX_SCENES], stop[PPE_MAX_SCENES], alpha[PPE_MAX_SCENES], rel[PPE_MAX_SCENES];
     __shared__ float beta[PPE_MAX_SCENES];
     __shared__ int its[PPE_MAX_SCENES], outs[PPE_MAX_SCENES];
@@ -914,6 +880,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
     int total = 0;
     float2* zc = S.zp0;   // (z, p) per row, current and next
     float2* zn = S.zp1;
+    float* rc = S.r;      // learned: the residual, and the buffer its update writes
+    float* ra = S.ralt;
     for (int outer = 0; outer < S.max_outer; outer++) {
         for (uint32_t t = threadIdx.x; t < 3 * ns; t += blockDim.x) acc[t] = 0.0;
         __syncthreads();
@@ -949,7 +917,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const double ri = bi - (S.diag64[ii] * S.x64[ii] + sum);
                 const float rf = (float)ri;
                 const float zf = PREC == 0 ? rf * S.inv_diag[ii] : 0.f;
-                S.r[ii] = rf;
+                (PREC == 1 ? rc : S.r)[ii] = rf;
                 zc[ii] = make_float2(zf, 0.f);
                 v[0] = ri * ri;
                 v[1] = bi * bi;
@@ -979,15 +947,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
         }
         __syncthreads();
         if (PREC == 1) {
-            // z = G'^T G' r on the rows of the scenes still open; r.z per scene
-            for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += stride) {
-                if (done[__ldg(S.row_scene + kk)]) continue;
-                const uint32_t i = __ldg(rowlist + kk);
-                const float* r = S.r;
-                S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk, [r](uint32_t j) { return r[j]; });
-            }
-            for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[t] = 0.0;
-            if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;  // barrier: y complete
+            // z = S' r on the rows of the scenes still open; r.z per scene
             for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[t] = 0.0;
             __syncthreads();
             for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
@@ -998,11 +958,11 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 double v[1] = {0.0};
                 if (contrib) {
                     const uint32_t i = __ldg(rowlist + kk);
-                    const float* y = S.y;
+                    const float* r = rc;
                     const float zi =
-                        lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
+                        sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r](uint32_t j) { return r[j]; });
                     zc[i].x = zi;
-                    v[0] = (double)S.r[i] * (double)zi;
+                    v[0] = (double)r[i] * (double)zi;
                 }
                 scene_add<1>(acc, ns, s, contrib, v);
             }
@@ -1039,6 +999,7 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const float bs = beta[s];
                 float sum = 0.f, sum1 = 0.f;
                 if (work)
+#pragma unroll 4
                     for (uint32_t t = 0; t < T; t++) {
                         const uint4 c = ld_mat(cols + 32 * t, pol);
                         const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, rl, thr, pi, ii, c);
@@ -1093,58 +1054,37 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 }
                 if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
             } else {
-                // pass A: x64 += alpha p; y = G' r_new with each neighbour's
-                // r_new = r - alpha q formed on the fly (same scene, same
-                // alpha); r_new . r_new per scene
+                // x64 += alpha p; z = S' r_new with each neighbour's r_new =
+                // r - alpha q formed on the fly (same scene, same alpha); the
+                // new residual into the other buffer; r.z and r.r per scene
                 for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
                     const uint32_t kk = k0 + lane;
                     const bool has = kk < R;
                     const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
                     const bool contrib = has && active[s];
-                    double v[1] = {0.0};
+                    double v[2] = {0.0, 0.0};
                     if (contrib) {
                         const uint32_t i = __ldg(rowlist + kk);
                         const double al = alpha[s];
                         const float af = (float)al;
-                        S.x64[i] += al * (double)zn[i].y;
-                        const float ri = fmaf(-af, S.q[i], S.r[i]);
-                        const float* r = S.r;
+                        const float pn = zn[i].y;
+                        S.x64[i] += al * (double)pn;
+                        const float* r = rc;
                         const float* q = S.q;
-                        S.y[i] = lp_packed_row(S.lo_off, S.lo_cols, S.lo_vals, kk,
-                                               [r, q, af](uint32_t j) { return fmaf(-af, q[j], r[j]); });
-                        v[0] = (double)ri * (double)ri;
-                    }
-                    scene_add<1>(acc, ns, s, contrib, v);
-                }
-                if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
-                for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) {
-                    rrn[t] = acc[t];
-                    acc[t] = 0.0;
-                }
-                __syncthreads();
-                // pass B: r = r_new in place (no neighbour reads r now),
-                // z = G'^T y; r.z per scene
-                for (uint32_t k0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); k0 < R; k0 += stride) {
-                    const uint32_t kk = k0 + lane;
-                    const bool has = kk < R;
-                    const uint32_t s = has ? __ldg(S.row_scene + kk) : 0u;
-                    const bool contrib = has && active[s];
-                    double v[1] = {0.0};
-                    if (contrib) {
-                        const uint32_t i = __ldg(rowlist + kk);
-                        const float ri = fmaf(-(float)alpha[s], S.q[i], S.r[i]);
-                        S.r[i] = ri;
-                        const float* y = S.y;
-                        const float zi =
-                            lp_packed_row(S.up_off, S.up_cols, S.up_vals, kk, [y](uint32_t j) { return y[j]; });
-                        zn[i] = make_float2(zi, zn[i].y);
+                        const float ri = fmaf(-af, q[i], r[i]);
+                        ra[i] = ri;
+                        const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i,
+                                                   [r, q, af](uint32_t j) { return fmaf(-af, q[j], r[j]); });
+                        zn[i] = make_float2(zi, pn);
                         v[0] = (double)ri * (double)zi;
+                        v[1] = (double)ri * (double)ri;
                     }
-                    scene_add<1>(acc, ns, s, contrib, v);
+                    scene_add<2>(acc, ns, s, contrib, v);
                 }
-                if (!grid_reduce_scenes<1>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
-                for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) acc[ns + t] = rrn[t];
-                __syncthreads();
+                if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
+                float* t_ = rc;
+                rc = ra;
+                ra = t_;
             }
             for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
                 if (!active[s]) continue;
@@ -1462,7 +1402,6 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.qp, (size_t)cap * (PPE_MAX_SPLIT - 1) * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
-    ok &= al((void**)&w.y, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.ralt, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.pos_snap, (size_t)cap * sizeof(float4));
     ok &= al((void**)&w.n_snap, (size_t)cap * sizeof(float));
@@ -1667,22 +1606,17 @@ int ppe_enqueue_setup(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     cudaMemcpyAsync(w.n_snap, a.cur.n, (size_t)cap * sizeof(float), cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(w.id_snap, a.cur.id, (size_t)cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
     w.have_snapshot = true;
-    if (w.lp.ready && w.c16_learned && !a.batch.n) {
+    if (opt.precond == MPS_PRECOND_LEARNED && w.lp.ready && w.sp_ent) {
         // the symmetric form by GEO index, rebuilt every precond_every steps;
-        // S' of the current rows every step
+        // S' of the current rows every step (compact or particle columns)
         if (w.build_net) {
             const LpSystem L = ppe_lp_system(w, a);
             lp_build_stencil(w.lp, L, cap, st);
-            lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores, false);
+            lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores);
             lp_build_symmetric(w.lp, L, cap, st);
             launched += 12;
         }
-        launched += ppe_c16_enqueue_learned_pack(w, a, cap, st);
-    } else if (w.lp.ready) {
-        const LpSystem L = ppe_lp_system(w, a);
-        lp_build_stencil(w.lp, L, cap, st);
-        lp_forward(w.lp, L, a.exact, cap, st, w.lp.tensor_cores);
-        launched += 10;
+        launched += ppe_sp_enqueue_pack(w, a, cap, st, !(w.c16_learned && !a.batch.n));
     }
     return launched;
 }
@@ -1741,13 +1675,9 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.pos = a.cur.pos;
     S.rlap = a.P.rlap;
     S.rlap_thr = a.P.rlap_thr;
-    S.lo_off = w.lp.lo_off;
-    S.lo_cols = w.lp.lo_cols;
-    S.lo_vals = w.lp.lo_vals;
-    S.up_off = w.lp.up_off;
-    S.up_cols = w.lp.up_cols;
-    S.up_vals = w.lp.up_vals;
-    S.y = w.y;
+    S.sp_off = w.sp_off;
+    S.sp_ent = w.sp_ent;
+    S.sp_diag = w.sp_diag;
     S.ralt = w.ralt;
     S.sc = a.sc;
     S.tol = opt.cg_tol;
@@ -1793,15 +1723,12 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.max_outer = S.max_outer;
         B.eta_min = S.eta_min;
         B.keep = S.keep;
-        B.lo_off = w.lp.lo_off;
-        B.lo_cols = w.lp.lo_cols;
-        B.lo_vals = w.lp.lo_vals;
-        B.up_off = w.lp.up_off;
-        B.up_cols = w.lp.up_cols;
-        B.up_vals = w.lp.up_vals;
-        B.y = w.y;
+        B.sp_off = w.sp_off;
+        B.sp_ent = w.sp_ent;
+        B.sp_diag = w.sp_diag;
+        B.ralt = w.ralt;
         void* bargs[] = {&B};
-        const bool blearned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+        const bool blearned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready && w.sp_ent;
         const void* bfn;
         if (blearned)
             bfn = w.stored_weights ? (a.exact ? (const void*)k_ppe_solve_batch<true, true, 1>
@@ -1818,7 +1745,7 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         k_ppe_finish<<<blocks_for(cap, 256), 256, 0, st>>>(w.x64, w.rlen, a.cur.press, a.sc);
         return 2;
     }
-    const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready;
+    const bool learned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready && w.sp_ent;
     if (w.c16 && (!learned || w.c16_learned)) return ppe_c16_enqueue_solve(w, a, opt, cap, st);
     if (w.pipelined && !learned) {
         PipeArgs Pa;
@@ -2069,9 +1996,9 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.wrm, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.zp[0], w.zp[1], w.q,    w.qp,   w.part,     w.result, w.bar,
-                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.y, w.ralt, w.pos_snap, w.n_snap,
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.ralt, w.pos_snap, w.n_snap,
                   w.id_snap, w.pu, w.pw, w.pz, w.pq, w.ps, w.pp, w.pm[0], w.pm[1], w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
-                  w.scene_relres};
+                  w.scene_relres, w.sp_off, w.sp_ent, w.sp_diag};
     lp_free(w.lp);
     ppe_c16_free(w);
     for (void* p : ps)

@@ -70,8 +70,7 @@ struct PpeWork {
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
     // learned preconditioner (set up on first use)
     LearnedWork lp;
-    float* y = nullptr;                // G D^-1/2 r
-    float* ralt = nullptr;             // second residual buffer
+    float* ralt = nullptr;             // second residual buffer (the learned update writes the new residual there)
     // state at the last assembly (the system the network and its training see)
     float4* pos_snap = nullptr;
     float* n_snap = nullptr;
@@ -104,22 +103,25 @@ struct PpeWork {
     double *cb64 = nullptr, *cx64 = nullptr, *cdiag64 = nullptr;
     float *cdiag32 = nullptr, *cinv_diag = nullptr, *cr = nullptr, *cq = nullptr;
     float2* czp[2] = {nullptr, nullptr};
-    // the learned preconditioner on the compact layout: S' = D^-1/2 S D^-1/2
-    // (S the symmetric form in LearnedWork, kept by GEO index) in 4-row
-    // slices, one product fused into the residual update of every iteration
+    // the learned preconditioner: S' = D^-1/2 S D^-1/2 (S the symmetric form
+    // in LearnedWork, kept by GEO index, rebuilt every precond_every steps)
+    // packed for the current rows every step (layout: ppe_device.cuh), one
+    // product fused into the residual update of every PCG iteration; its
+    // columns are compact positions for the compact solver and particle
+    // indices for the 8-byte and batch solvers
     bool c16_learned = false;          // the compact solve applies S'
     int precond_every = 40;            // steps between network evaluations
     uint32_t* sp_off = nullptr;        // first entry of every 32-row slice (widths, then scanned)
-    uint32_t* sp_ent = nullptr;        // off-diagonal entries: column - row (16 bits) << 16 | BF16 value
-    float* sp_diag = nullptr;          // the diagonal, per compact row
-    float* cr2 = nullptr;              // second residual buffer of the fused update
+    uint32_t* sp_ent = nullptr;        // off-diagonal entries: column - own column (16 bits) << 16 | BF16 value
+    float* sp_diag = nullptr;          // the diagonal, per row position
+    float* cr2 = nullptr;              // second residual buffer of the compact solver's fused update
     size_t sp_cap_chunks = 0;
     const uint32_t* index_of_id = nullptr;  // the handle's GEO index -> sorted position
-    bool build_net = true;             // this step evaluates the network (c16_learned)
+    bool build_net = true;             // this step evaluates the network (learned preconditioner)
     uint64_t net_steps = 0;            // steps since the handle was created
 };
 
-// The learned compact form re-evaluates its network every precond_every
+// The learned preconditioner re-evaluates its network every precond_every
 // steps (and whenever its form has not been built): decide for the next
 // step, count it, and return the decision.
 inline bool ppe_begin_step(PpeWork& w) {
@@ -159,10 +161,13 @@ int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt
 int ppe_c16_export(const PpeWork& w, uint32_t np, const uint32_t* d_row_start, uint32_t* d_cols, float* d_w,
                    cudaStream_t st);
 void ppe_c16_free(PpeWork& w);
-// the learned S' on the compact layout: buffers, and its per-step pack from
-// the symmetric form kept by GEO index (after ppe_c16_enqueue_pack)
+// the learned S': its buffers (ppe_sp_enable; the compact solver's second
+// residual buffer too with ppe_c16_learned_enable), and its per-step pack
+// from the symmetric form kept by GEO index, after the row list (and, for
+// the compact columns, after ppe_c16_enqueue_pack)
+int ppe_sp_enable(PpeWork& w, std::string* err);
 int ppe_c16_learned_enable(PpeWork& w, std::string* err);
-int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st);
+int ppe_sp_enqueue_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st, bool by_particle);
 // the persistent solver's block size (256, 512 or 1024; 1024 threads per SM
 // either way); MPS_ERR_INVALID when the device cannot hold that shape
 int ppe_set_threads(PpeWork& w, int threads);

@@ -176,18 +176,14 @@ __global__ void __launch_bounds__(256) k_c16_export(const uint32_t* __restrict__
 }
 
 // ---------------------------------------------------------------- learned S'
-// S' = D^-1/2 S D^-1/2 on the compact rows, S the symmetric form of the
-// learned factor kept by GEO index (learned.cuh).  Row k: its diagonal in
-// FP32 (sp_diag) and its stored neighbours that are rows now, each as one
-// 32-bit word, (column - k) in the upper 16 bits and the value in BF16 in the
-// lower 16 (S is built diagonally dominant with a 1 % margin, more than BF16
-// rounding takes away, so S' stays SPD).  A pair farther apart than 32,767
-// rows is left out from both its rows, which keeps S' symmetric and
-// dominant.  Sliced ELL with a thread per row: slices of 32 consecutive rows,
-// width = the longest row of the slice, entry t of row k at
-// off[k / 32] + 32 t + k % 32, padding = 0 (the row itself, value 0).
-constexpr uint32_t SP_SLICE = 32;
-
+// S' (its layout: ppe_device.cuh) of the current rows, from S kept by GEO
+// index (learned.cuh): row position k holds its FP32 diagonal and its stored
+// neighbours that are rows now.  A pair whose columns lie farther apart than
+// 32,767 is left out from both its rows, which keeps S' symmetric and
+// diagonally dominant (S is built dominant with a 1 % margin, more than BF16
+// rounding of the entries takes away, so S' stays SPD).  PART selects the
+// columns: particle indices (the particle-indexed solvers) or compact
+// positions (the compact solver).
 struct SpArgs {
     const uint32_t* rowlist;
     const uint32_t* nrows;
@@ -214,10 +210,11 @@ struct SpArgs {
 // entries instead of per entry.
 constexpr uint32_t SP_BATCH = 8;
 
-// the batch [u0, u0 + 8) of row k's stored neighbours: kept or not, the
-// column offset and the neighbour's particle index
+// the batch [u0, u0 + 8) of the stored neighbours of a row with own column
+// c: kept or not, the column offset and the neighbour's particle index
+template <bool PART>
 __device__ __forceinline__ void sp_batch(const SpArgs& A, uint32_t id, uint32_t n, uint32_t u0, uint32_t np,
-                                         uint32_t k, bool (&ok)[SP_BATCH], int (&d)[SP_BATCH],
+                                         uint32_t c, bool (&ok)[SP_BATCH], int (&d)[SP_BATCH],
                                          uint32_t (&j)[SP_BATCH]) {
     uint32_t jd[SP_BATCH];
 #pragma unroll
@@ -230,29 +227,31 @@ __device__ __forceinline__ void sp_batch(const SpArgs& A, uint32_t id, uint32_t 
     for (uint32_t b = 0; b < SP_BATCH; b++) {
         const bool live = j[b] < np;
         len[b] = live ? __ldg(A.rlen + j[b]) : PPE_DIRICHLET;
-        cp[b] = live ? __ldg(A.cpos + j[b]) : 0u;
+        cp[b] = PART ? j[b] : (live ? __ldg(A.cpos + j[b]) : 0u);
     }
 #pragma unroll
     for (uint32_t b = 0; b < SP_BATCH; b++) {
-        d[b] = (int)cp[b] - (int)k;
+        d[b] = (int)cp[b] - (int)c;
         ok[b] = len[b] != PPE_DIRICHLET && d[b] >= -32767 && d[b] <= 32767;
     }
 }
 
 // Pass 1: off[s] = 32 x (longest row of slice s), every slice up to maxslices.
+template <bool PART>
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t s = k / SP_SLICE;
     uint32_t cnt = 0;
     if (k < R) {
-        const uint32_t id = __ldg(A.idv + __ldg(A.rowlist + k));
+        const uint32_t i = __ldg(A.rowlist + k);
+        const uint32_t id = __ldg(A.idv + i);
         const uint32_t n = __ldg(A.s_cnt + id);
         for (uint32_t u0 = 0; u0 < n; u0 += SP_BATCH) {
             bool ok[SP_BATCH];
             int d[SP_BATCH];
             uint32_t j[SP_BATCH];
-            sp_batch(A, id, n, u0, np, k, ok, d, j);
+            sp_batch<PART>(A, id, n, u0, np, PART ? i : k, ok, d, j);
 #pragma unroll
             for (uint32_t b = 0; b < SP_BATCH; b++) cnt += ok[b] ? 1u : 0u;
         }
@@ -268,6 +267,7 @@ __device__ __forceinline__ uint32_t sp_bf16_bits(float v) {
 
 // Pass 2 (after the scan of off): the kept entries of row k in stored order,
 // then zeros up to the slice's width.
+template <bool PART>
 __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
     const uint32_t R = *A.nrows, np = A.sc->np;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) k_sp_pack(SpArgs A) {
             bool ok[SP_BATCH];
             int d[SP_BATCH];
             uint32_t j[SP_BATCH];
-            sp_batch(A, id, n, u0, np, k, ok, d, j);
+            sp_batch<PART>(A, id, n, u0, np, PART ? i : k, ok, d, j);
             double dg[SP_BATCH];
             float sv[SP_BATCH];
 #pragma unroll
@@ -337,36 +337,10 @@ struct C16Args {
     float* r2;
 };
 
-// Row k of S' x (thread per row; x_j given by a functor of the compact
-// column).  Eight entries a round: their words first, then the eight x_j,
-// so a row of ~25 entries costs four rounds of dependent loads.
-// S' is read every iteration and is small next to the matrix: keep it in L2
-__device__ __forceinline__ uint32_t sp_load(const uint32_t* p, uint64_t pol) {
-    uint32_t v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
-    return v;
-}
-
+// Row k of S' x on the compact rows (own column k).
 template <class X>
 __device__ __forceinline__ float sp_row(const C16Args& S, uint32_t k, X x) {
-    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
-    const uint32_t base = __ldg(S.sp_off + s), W = (__ldg(S.sp_off + s + 1) - base) / SP_SLICE;
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (uint32_t t0 = 0; t0 < W; t0 += 8) {
-        uint32_t e[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-            e[u] = t0 + u < W ? sp_load(S.sp_ent + base + SP_SLICE * (size_t)(t0 + u) + lane, pol) : 0u;
-        float xv[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) xv[u] = x((uint32_t)((int)k + ((int)e[u] >> 16)));
-#pragma unroll
-        for (int u = 0; u < 8; u++) acc[u] = fmaf(__uint_as_float(e[u] << 16), xv[u], acc[u]);
-    }
-    const float off = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
-    return fmaf(__ldg(S.sp_diag + k), x(k), off);
+    return sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, k, k, x);
 }
 
 // The four columns of a lane's chunk entries.
@@ -680,7 +654,7 @@ int ppe_c16_enable(PpeWork& w, std::string* err) {
 
 void ppe_c16_free(PpeWork& w) {
     void* ps[] = {w.cpos, w.c16_width, w.c16_codes, w.c16_w, w.c16_side, w.c16_esc, w.cb64, w.cx64, w.cdiag64,
-                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1], w.sp_off, w.sp_ent, w.sp_diag, w.cr2};
+                  w.cdiag32, w.cinv_diag, w.cr, w.cq, w.czp[0], w.czp[1], w.cr2};
     for (void* p : ps)
         if (p) cudaFree(p);
     w.cpos = w.c16_width = w.c16_esc = nullptr;
@@ -690,9 +664,6 @@ void ppe_c16_free(PpeWork& w) {
     w.cb64 = w.cx64 = w.cdiag64 = nullptr;
     w.cdiag32 = w.cinv_diag = w.cr = w.cq = nullptr;
     w.czp[0] = w.czp[1] = nullptr;
-    w.sp_off = nullptr;
-    w.sp_ent = nullptr;
-    w.sp_diag = nullptr;
     w.cr2 = nullptr;
     w.c16_ready = false;
     w.c16 = false;
@@ -761,7 +732,7 @@ int ppe_c16_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt
     return 2;
 }
 
-int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
+int ppe_sp_enable(PpeWork& w, std::string* err) {
     if (lp_alloc_symmetric(w.lp) != MPS_OK) {
         if (err) *err = "cudaMalloc failed for the learned symmetric form";
         return MPS_ERR_CUDA;
@@ -772,8 +743,18 @@ int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
     bool ok = c16_alloc(&w.sp_off, slices + 2);
     ok &= c16_alloc(&w.sp_ent, w.sp_cap_chunks * SP_SLICE);
     ok &= c16_alloc(&w.sp_diag, (size_t)w.cap + 8);
-    ok &= c16_alloc(&w.cr2, (size_t)w.cap + 8);
     if (!ok) {
+        if (err) *err = "cudaMalloc failed for the learned preconditioner";
+        return MPS_ERR_CUDA;
+    }
+    return MPS_OK;
+}
+
+int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
+    const int e = ppe_sp_enable(w, err);
+    if (e != MPS_OK) return e;
+    if (w.cr2) return MPS_OK;
+    if (!c16_alloc(&w.cr2, (size_t)w.cap + 8)) {
         if (err) *err = "cudaMalloc failed for the learned compact preconditioner";
         return MPS_ERR_CUDA;
     }
@@ -781,7 +762,7 @@ int ppe_c16_learned_enable(PpeWork& w, std::string* err) {
     return MPS_OK;
 }
 
-int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st) {
+int ppe_sp_enqueue_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream_t st, bool by_particle) {
     SpArgs A;
     A.rowlist = w.rowlist;
     A.nrows = w.nrows;
@@ -800,9 +781,12 @@ int ppe_c16_enqueue_learned_pack(PpeWork& w, const StageArgs& a, uint32_t cap, c
     A.diag = w.sp_diag;
     const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
-    k_sp_width<<<cblocks((maxslices + 1) * SP_SLICE, 256), 256, 0, st>>>(A);
+    const uint32_t wb = cblocks((maxslices + 1) * SP_SLICE, 256), pb = cblocks(maxslices * SP_SLICE, 256);
+    if (by_particle) k_sp_width<true><<<wb, 256, 0, st>>>(A);
+    else k_sp_width<false><<<wb, 256, 0, st>>>(A);
     launch_scan_exclusive(w.sp_off, maxslices + 1, st);
-    k_sp_pack<<<cblocks(maxslices * SP_SLICE, 256), 256, 0, st>>>(A);
+    if (by_particle) k_sp_pack<true><<<pb, 256, 0, st>>>(A);
+    else k_sp_pack<false><<<pb, 256, 0, st>>>(A);
     return 3;
 }
 

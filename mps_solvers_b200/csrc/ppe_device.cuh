@@ -146,6 +146,50 @@ __device__ __forceinline__ float4 ld_mat(const float4* p, uint64_t pol) {
     return v;
 }
 
+// ---------------------------------------------------------------- learned S'
+// The learned preconditioner S' = D^-1/2 S D^-1/2 (S the symmetric form of
+// the network's factor) in sliced ELL with a thread per row: slices of 32
+// consecutive row positions, width = the longest row of the slice, entry t
+// of row position k at off[k / 32] + 32 t + k % 32.  Each entry is one
+// 32-bit word: (column - c) in the upper 16 bits, the value in BF16 in the
+// lower 16, where c is the row's own column (its compact position in the
+// compact solver, its particle index in the particle-indexed solvers);
+// padding is 0 (the row itself, value 0).  The diagonal is kept in FP32 by
+// row position.
+constexpr uint32_t SP_SLICE = 32;
+
+// S' is read every iteration and is small next to the matrix: keep it in L2
+__device__ __forceinline__ uint32_t sp_load(const uint32_t* p, uint64_t pol) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+// Row position k (own column c) of S' x, x_j given by a functor of the
+// column.  Eight entries a round: their words first, then the eight x_j, so
+// a row of ~25 entries costs four rounds of dependent loads.
+template <class X>
+__device__ __forceinline__ float sp_row_at(const uint32_t* __restrict__ off, const uint32_t* __restrict__ ent,
+                                           const float* __restrict__ diag, uint32_t k, uint32_t c, X x) {
+    const uint32_t s = k / SP_SLICE, lane = k % SP_SLICE;
+    const uint32_t base = __ldg(off + s), W = (__ldg(off + s + 1) - base) / SP_SLICE;
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (uint32_t t0 = 0; t0 < W; t0 += 8) {
+        uint32_t e[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            e[u] = t0 + u < W ? sp_load(ent + base + SP_SLICE * (size_t)(t0 + u) + lane, pol) : 0u;
+        float xv[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) xv[u] = x((uint32_t)((int)c + ((int)e[u] >> 16)));
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[u] = fmaf(__uint_as_float(e[u] << 16), xv[u], acc[u]);
+    }
+    const float offd = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    return fmaf(__ldg(diag + k), x(c), offd);
+}
 
 // A cooperative launch through the launch-attribute form, which stream
 // capture records as a cooperative graph kernel node.

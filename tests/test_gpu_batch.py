@@ -150,9 +150,11 @@ def test_batch_scene_table(capi, tmp_path):
 
 
 def test_learned_batch_matches_single_scenes(capi, tmp_path):
-    """The learned factor inside the batched PCG: every scene converges to
-    1e-8 in fewer iterations than with diagonal scaling and evolves within
-    the solve tolerance of its own learned single-scene handle."""
+    """The learned S' inside the batched PCG (particle columns, one product
+    fused into the residual update, each scene's own alpha): every scene
+    converges to 1e-8 in fewer iterations than with diagonal scaling and
+    evolves within the solve tolerance of its own learned single-scene
+    handle."""
     from mps_solvers_b200 import precond_weights
     wts = precond_weights.load()
     dirs = write_scenes(tmp_path, 5e-4)

@@ -70,9 +70,11 @@ def test_gradients_match_cpu_oracle(capi, tmp_path):
 
 
 def test_learned_pcg_is_spd_safe(capi, tmp_path):
-    """With untrained random network weights M^-1 = D^-1/2 G^T G D^-1/2 is
-    still SPD, so the learned PCG reaches the FP64 tolerance and its pressure
-    agrees with the diagonally scaled CG's to the accuracy of the solves."""
+    """With untrained random network weights the preconditioner
+    S' = D^-1/2 S D^-1/2 is still SPD (S is diagonally dominant by
+    construction), so the learned PCG reaches the FP64 tolerance and its
+    pressure agrees with the diagonally scaled CG's to the accuracy of the
+    solves."""
     g = load_golden("semi_tank")
     d = write_golden_case(g, str(tmp_path / "s"))
     press = {}
@@ -225,10 +227,24 @@ def test_learned_compact_form_kept_between_evaluations(capi, tmp_path):
     assert sum(it10) <= 1.15 * sum(it1) + 2, (it1, it10)
 
 
-def test_learned_factor_form_on_the_8_byte_layout(capi, tmp_path):
-    """The factor form M^-1 = D^-1/2 G^T G D^-1/2 (two products a
-    PCG iteration) still runs on the 8-byte layout and converges."""
-    g = load_golden("semi_tank")
-    d = write_golden_case(g, str(tmp_path / "s"))
-    it, _ = _run_steps(capi, d, 4, precond=capi.PRECOND_LEARNED, ppe_layout=-1)
-    assert all(k > 0 for k in it)
+def test_learned_form_on_the_8_byte_layout(capi, tmp_path):
+    """The learned S' on the 8-byte layout (particle columns, one product
+    fused into the residual update, as on the compact layout): with the
+    trained weights every solve reaches the FP64 tolerance in fewer PCG
+    iterations than diagonal scaling on the same layout, about as many as
+    the compact layout's learned solve (the two forms differ only in which
+    far pairs they leave out), and the state agrees with both to the
+    semi-implicit tolerances."""
+    from helpers import rel_err
+    from mps_solvers_b200 import scene
+    d = str(tmp_path / "c")
+    scene.write_case(d, scene.dam_break_semi(seed=11))
+    it_d, st_d = _run_steps(capi, d, 12, precond=capi.PRECOND_DIAGONAL, arith=capi.ARITH_FAST, ppe_layout=-1)
+    it_8, st_8 = _run_steps(capi, d, 12, precond=capi.PRECOND_LEARNED, arith=capi.ARITH_FAST, ppe_layout=-1)
+    it_c, st_c = _run_steps(capi, d, 12, precond=capi.PRECOND_LEARNED, arith=capi.ARITH_FAST)
+    print("iterations diagonal", it_d, "learned 8-byte", it_8, "learned compact", it_c)
+    assert sum(it_8) < 0.9 * sum(it_d), (it_d, it_8)
+    assert abs(sum(it_8) - sum(it_c)) <= 0.05 * sum(it_c) + 2, (it_8, it_c)
+    for other in (st_d, st_c):
+        assert rel_err(st_8["press"], other["press"]) < 2e-3
+        assert rel_err(st_8["vel"], other["vel"]) < 1e-3
