@@ -649,7 +649,8 @@ def sub_runs(args, local_rank: int):
         a.workload, a.steps, a.warmup = wl, steps, warm
         a.arith = "exact" if wl == "explicit" else "fast"
         a.no_ppe_compare = True
-        a.precond = "diagonal"
+        # the batched and large configurations name the learned preconditioner
+        a.precond = "learned" if wl in ("batch", "large") else "diagonal"
         try:
             sub = run_ours(a, 0, 1, local_rank)
             res = {k: sub.get(k) for k in SUB_KEYS}

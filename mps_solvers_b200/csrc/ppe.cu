@@ -999,7 +999,6 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const float bs = beta[s];
                 float sum = 0.f, sum1 = 0.f;
                 if (work)
-#pragma unroll 4
                     for (uint32_t t = 0; t < T; t++) {
                         const uint4 c = ld_mat(cols + 32 * t, pol);
                         const float4 w = chunk_weights<EX, SW>(wts + 32 * t, pol, S.pos, rl, thr, pi, ii, c);
