@@ -161,11 +161,14 @@ struct SolveArgs {
     const float* sw;          // stored weights (same layout as scols)
     const float4* pos;
     float rlap, rlap_thr;
-    // learned preconditioner S' by particle columns (ppe_device.cuh)
+    // learned preconditioner S' by particle columns (ppe_device.cuh), and
+    // its residual and q interleaved per particle, current and next pair
+    // buffer (a neighbour's r - alpha q is one 8-byte load)
     const uint32_t* sp_off;
     const uint32_t* sp_ent;
     const float* sp_diag;
-    float* ralt;
+    float2* rq0;
+    float2* rq1;
     Scalars* sc;
     double tol;
     double eta_min;   // smallest inner reduction asked of one FP32 solve
@@ -221,6 +224,15 @@ __device__ __forceinline__ float q_total(const SolveArgs& S, uint32_t i, uint32_
     float v = S.q[i];
     for (uint32_t p = 1; p < parts; p++) v += S.qp[(size_t)(p - 1) * S.cap + i];
     return v;
+}
+
+// the learned form: r_j - alpha q_j from the (r, q) pairs, q_j added up over
+// the parts in the same order as q_total
+__device__ __forceinline__ float rq_next(const SolveArgs& S, const float2* rq, uint32_t j, uint32_t parts, float a) {
+    const float2 v = rq[j];
+    float qv = v.y;
+    for (uint32_t p = 1; p < parts; p++) qv += S.qp[(size_t)(p - 1) * S.cap + j];
+    return fmaf(-a, qv, v.x);
 }
 
 template <bool EX, int PREC, bool SW>
@@ -304,7 +316,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 const double bi = S.b64[i];
                 const double ri = bi - (S.diag64[i] * S.x64[i] + s);
                 const float rf = (float)ri;
-                S.r[i] = rf;
+                if (PREC == 1) S.rq0[i].x = rf;
+                else S.r[i] = rf;
                 acc[0] += ri * ri;
                 acc[1] += bi * bi;
                 if (PREC == 0) {
@@ -329,12 +342,13 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
         if (PREC == 1) {
             // z = S' r of the new residual, r.z
             double rzp[1] = {0.0};
-            const float* r = S.r;
+            const float2* rq = S.rq0;
             for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                 const uint32_t i = __ldg(rowlist + kk);
-                const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r](uint32_t j) { return r[j]; });
+                const float zi =
+                    sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [rq](uint32_t j) { return rq[j].x; });
                 zc[i].x = zi;
-                rzp[0] += (double)r[i] * (double)zi;
+                rzp[0] += (double)rq[i].x * (double)zi;
             }
             double tz[1];
             if (!grid_reduce<1>(rzp, S.part, S.result, S.bar, S.sc, tz)) return;
@@ -405,7 +419,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                     if (part == 0) {
                         qi = fmaf(S.diag32[i], pn, s);
                         zn[i].y = pn;
-                        S.q[i] = qi;
+                        if (PREC == 1) S.rq0[i].y = qi;
+                        else S.q[i] = qi;
                     } else {
                         S.qp[(size_t)(part - 1) * S.cap + i] = s;
                     }
@@ -436,26 +451,27 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
                 // z = S' r_new with each neighbour's r_new = r - alpha q formed
                 // on the fly; the new residual into the second buffer (the
                 // neighbours read the old one); r.z and r.r
-                float* rnew = S.ralt;
-                const float* r = S.r;
+                float2* rnew = S.rq1;
+                const float2* rq = S.rq0;
                 const SolveArgs& SS = S;
                 for (uint32_t kk = blockIdx.x * blockDim.x + threadIdx.x; kk < R; kk += gridDim.x * blockDim.x) {
                     const uint32_t i = __ldg(rowlist + kk);
                     const float pn = zn[i].y;
                     S.x64[i] += alpha * (double)pn;
-                    const float ri = fmaf(-alpha_f, q_total(S, i, parts), r[i]);
-                    rnew[i] = ri;
-                    const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r, &SS, alpha_f, parts](uint32_t j) {
-                        return fmaf(-alpha_f, q_total(SS, j, parts), r[j]);
-                    });
+                    const float ri = rq_next(S, rq, i, parts, alpha_f);
+                    rnew[i] = make_float2(ri, 0.f);
+                    const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i,
+                                               [rq, &SS, alpha_f, parts](uint32_t j) {
+                                                   return rq_next(SS, rq, j, parts, alpha_f);
+                                               });
                     zn[i] = make_float2(zi, pn);
                     acc2[0] += (double)ri * (double)zi;
                     acc2[1] += (double)ri * (double)ri;
                 }
                 if (!grid_reduce<2>(acc2, S.part, S.result, S.bar, S.sc, tot2)) return;
-                // swap the residual buffers
-                S.ralt = S.r;
-                S.r = rnew;
+                // swap the pair buffers
+                S.rq1 = S.rq0;
+                S.rq0 = rnew;
             }
             total++;
             beta = (float)(tot2[0] / rz);
@@ -722,12 +738,13 @@ struct BatchSolveArgs {
     int* iters;
     int* outers;
     double* relres;
-    // learned preconditioner S' by particle columns (ppe_device.cuh) and the
-    // second residual buffer of its update
+    // learned preconditioner S' by particle columns (ppe_device.cuh) and its
+    // (r, q) pair buffers, as in SolveArgs
     const uint32_t* sp_off;
     const uint32_t* sp_ent;
     const float* sp_diag;
-    float* ralt;
+    float2* rq0;
+    float2* rq1;
     uint32_t ns;
     double tol;
     double eta_min;
@@ -880,8 +897,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
     int total = 0;
     float2* zc = S.zp0;   // (z, p) per row, current and next
     float2* zn = S.zp1;
-    float* rc = S.r;      // learned: the residual, and the buffer its update writes
-    float* ra = S.ralt;
+    float2* rqc = S.rq0;  // learned: the (r, q) pairs, and the buffer its update writes
+    float2* rqn = S.rq1;
     for (int outer = 0; outer < S.max_outer; outer++) {
         for (uint32_t t = threadIdx.x; t < 3 * ns; t += blockDim.x) acc[t] = 0.0;
         __syncthreads();
@@ -917,7 +934,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 const double ri = bi - (S.diag64[ii] * S.x64[ii] + sum);
                 const float rf = (float)ri;
                 const float zf = PREC == 0 ? rf * S.inv_diag[ii] : 0.f;
-                (PREC == 1 ? rc : S.r)[ii] = rf;
+                if (PREC == 1) rqc[ii].x = rf;
+                else S.r[ii] = rf;
                 zc[ii] = make_float2(zf, 0.f);
                 v[0] = ri * ri;
                 v[1] = bi * bi;
@@ -958,11 +976,11 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                 double v[1] = {0.0};
                 if (contrib) {
                     const uint32_t i = __ldg(rowlist + kk);
-                    const float* r = rc;
+                    const float2* rq = rqc;
                     const float zi =
-                        sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [r](uint32_t j) { return r[j]; });
+                        sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [rq](uint32_t j) { return rq[j].x; });
                     zc[i].x = zi;
-                    v[0] = (double)r[i] * (double)zi;
+                    v[0] = (double)rq[i].x * (double)zi;
                 }
                 scene_add<1>(acc, ns, s, contrib, v);
             }
@@ -1018,7 +1036,8 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                     const float pn = fmaf(bs, o.y, o.x);
                     const float qi = fmaf(S.diag32[ii], pn, sum);
                     zn[ii].y = pn;
-                    S.q[ii] = qi;
+                    if (PREC == 1) rqc[ii].y = qi;
+                    else S.q[ii] = qi;
                     v[0] = (double)pn * (double)qi;
                 }
                 scene_add<1>(acc, ns, s, contrib, v);
@@ -1068,12 +1087,14 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                         const float af = (float)al;
                         const float pn = zn[i].y;
                         S.x64[i] += al * (double)pn;
-                        const float* r = rc;
-                        const float* q = S.q;
-                        const float ri = fmaf(-af, q[i], r[i]);
-                        ra[i] = ri;
-                        const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i,
-                                                   [r, q, af](uint32_t j) { return fmaf(-af, q[j], r[j]); });
+                        const float2* rq = rqc;
+                        const float2 o = rq[i];
+                        const float ri = fmaf(-af, o.y, o.x);
+                        rqn[i] = make_float2(ri, 0.f);
+                        const float zi = sp_row_at(S.sp_off, S.sp_ent, S.sp_diag, kk, i, [rq, af](uint32_t j) {
+                            const float2 v = rq[j];
+                            return fmaf(-af, v.y, v.x);
+                        });
                         zn[i] = make_float2(zi, pn);
                         v[0] = (double)ri * (double)zi;
                         v[1] = (double)ri * (double)ri;
@@ -1081,9 +1102,9 @@ __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve_batch(BatchSolveArgs 
                     scene_add<2>(acc, ns, s, contrib, v);
                 }
                 if (!grid_reduce_scenes<2>(acc, ns, S.part, S.result, S.bar, S.sc)) return;
-                float* t_ = rc;
-                rc = ra;
-                ra = t_;
+                float2* t_ = rqc;
+                rqc = rqn;
+                rqn = t_;
             }
             for (uint32_t s = threadIdx.x; s < ns; s += blockDim.x) {
                 if (!active[s]) continue;
@@ -1401,7 +1422,6 @@ int ppe_setup(PpeWork& w, uint32_t cap, const Grid&, const Phys&, const mps_para
     ok &= al((void**)&w.q, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.qp, (size_t)cap * (PPE_MAX_SPLIT - 1) * sizeof(float));
     ok &= al((void**)&w.rowlist, (size_t)cap * sizeof(uint32_t));
-    ok &= al((void**)&w.ralt, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.pos_snap, (size_t)cap * sizeof(float4));
     ok &= al((void**)&w.n_snap, (size_t)cap * sizeof(float));
     ok &= al((void**)&w.id_snap, (size_t)cap * sizeof(uint32_t));
@@ -1677,7 +1697,8 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
     S.sp_off = w.sp_off;
     S.sp_ent = w.sp_ent;
     S.sp_diag = w.sp_diag;
-    S.ralt = w.ralt;
+    S.rq0 = w.rq[0];
+    S.rq1 = w.rq[1];
     S.sc = a.sc;
     S.tol = opt.cg_tol;
     S.max_iter = opt.cg_max_iter;
@@ -1725,7 +1746,8 @@ int ppe_enqueue_solve(PpeWork& w, const StageArgs& a, const mps_options& opt, ui
         B.sp_off = w.sp_off;
         B.sp_ent = w.sp_ent;
         B.sp_diag = w.sp_diag;
-        B.ralt = w.ralt;
+        B.rq0 = w.rq[0];
+        B.rq1 = w.rq[1];
         void* bargs[] = {&B};
         const bool blearned = opt.precond == MPS_PRECOND_LEARNED && w.lp.ready && w.sp_ent;
         const void* bfn;
@@ -1995,9 +2017,9 @@ int ppe_setup_batch(PpeWork& w, const PpeScene* scenes, uint32_t nscenes, cudaSt
 void ppe_free(PpeWork& w) {
     void* ps[] = {w.cols, w.wrm, w.rlen, w.diag64, w.diag32, w.inv_diag, w.b64, w.x64,
                   w.r,    w.zp[0], w.zp[1], w.q,    w.qp,   w.part,     w.result, w.bar,
-                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.ralt, w.pos_snap, w.n_snap,
+                  w.rowlist, w.tilecnt, w.nrows, w.sell_off, w.sell_cols, w.sell_w, w.pos_snap, w.n_snap,
                   w.id_snap, w.pu, w.pw, w.pz, w.pq, w.ps, w.pp, w.pm[0], w.pm[1], w.scenes, w.row_scene, w.bpart, w.bresult, w.scene_iters, w.scene_outer,
-                  w.scene_relres, w.sp_off, w.sp_ent, w.sp_diag};
+                  w.scene_relres, w.sp_off, w.sp_ent, w.sp_diag, w.rq[0], w.rq[1]};
     lp_free(w.lp);
     ppe_c16_free(w);
     for (void* p : ps)

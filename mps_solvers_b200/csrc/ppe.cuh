@@ -70,7 +70,6 @@ struct PpeWork {
     unsigned* bar = nullptr;           // [0] arrival count, [1] generation
     // learned preconditioner (set up on first use)
     LearnedWork lp;
-    float* ralt = nullptr;             // second residual buffer (the learned update writes the new residual there)
     // state at the last assembly (the system the network and its training see)
     float4* pos_snap = nullptr;
     float* n_snap = nullptr;
@@ -115,6 +114,7 @@ struct PpeWork {
     uint32_t* sp_ent = nullptr;        // off-diagonal entries: column - own column (16 bits) << 16 | BF16 value
     float* sp_diag = nullptr;          // the diagonal, per row position
     float* cr2 = nullptr;              // second residual buffer of the compact solver's fused update
+    float2* rq[2] = {nullptr, nullptr};  // the 8-byte and batch solvers' (r, q) pairs, current and next
     size_t sp_cap_chunks = 0;
     const uint32_t* index_of_id = nullptr;  // the handle's GEO index -> sorted position
     bool build_net = true;             // this step evaluates the network (learned preconditioner)

@@ -743,10 +743,14 @@ int ppe_sp_enable(PpeWork& w, std::string* err) {
     bool ok = c16_alloc(&w.sp_off, slices + 2);
     ok &= c16_alloc(&w.sp_ent, w.sp_cap_chunks * SP_SLICE);
     ok &= c16_alloc(&w.sp_diag, (size_t)w.cap + 8);
+    ok &= c16_alloc(&w.rq[0], (size_t)w.cap + 8);
+    ok &= c16_alloc(&w.rq[1], (size_t)w.cap + 8);
     if (!ok) {
         if (err) *err = "cudaMalloc failed for the learned preconditioner";
         return MPS_ERR_CUDA;
     }
+    cudaMemset(w.rq[0], 0, ((size_t)w.cap + 8) * sizeof(float2));
+    cudaMemset(w.rq[1], 0, ((size_t)w.cap + 8) * sizeof(float2));
     return MPS_OK;
 }
 
