@@ -243,11 +243,13 @@ mps_status mps_profile_steps(mps_handle* h, int nsteps, double* stage_ms, int ma
 const char* mps_stage_name(int k);
 
 /* ---- learned PPE preconditioner (no counterpart in the reference) --------
- * M^-1 = D^-1/2 G^T G D^-1/2 with G lower triangular on each row's r0
- * neighbours, its entries produced by a two-round message-passing network
- * (hidden 64, GELU, BF16 weights, FP32 accumulation); selected with
- * options.precond = MPS_PRECOND_LEARNED (semi-implicit method).  The
- * parameter vector has mps_precond_num_params() floats. */
+ * A factor G, lower triangular on each row's r0 neighbours, its entries
+ * produced by a two-round message-passing network (hidden 64, GELU, BF16
+ * weights, FP32 accumulation); the solvers apply M^-1 = D^-1/2 S D^-1/2 with
+ * S the symmetric first-order form of G^T G on G's pattern, made diagonally
+ * dominant (so SPD), re-evaluated every options.precond_every steps.
+ * Selected with options.precond = MPS_PRECOND_LEARNED (semi-implicit
+ * method).  The parameter vector has mps_precond_num_params() floats. */
 uint32_t mps_precond_num_params(void);
 mps_status mps_precond_get_params(mps_handle* h, float* w, uint32_t n);
 /* Load parameters (also enables the network on a handle created with the
@@ -355,7 +357,7 @@ mps_status mps_cell_sort_dev_noalloc(const float* pos4_dev, uint32_t n, const mp
  * its own input.dat / GEO.dat, grid, constants, dt and time) as one particle
  * set: every stage is one launch over all scenes, and the semi-implicit PPE
  * of all scenes is one persistent launch in which each scene runs its own
- * PCG to options.cg_tol (diagonally scaled, or with the learned factor when
+ * PCG to options.cg_tol (diagonally scaled, or with the learned form when
  * options.precond = MPS_PRECOND_LEARNED: mps_precond_set_params and
  * mps_precond_tensor_cores take batch handles; training takes single scenes).
  * Each scene evolves as it would in its own handle.
