@@ -203,7 +203,7 @@ struct SpArgs {
     uint32_t maxslices;
 };
 
-// Both passes take a thread per row (lane = row of the 32-row slice, so the
+// The pack takes a thread per row (lane = row of the 32-row slice, so the
 // packed words leave as coalesced 128-byte rows) and eight of its stored
 // neighbours at a time, their loads issued together: the chain s_col ->
 // index_of_id -> rlen, cpos, diag64 costs three dependent rounds per eight
@@ -236,26 +236,17 @@ __device__ __forceinline__ void sp_batch(const SpArgs& A, uint32_t id, uint32_t 
     }
 }
 
-// Pass 1: off[s] = 32 x (longest row of slice s), every slice up to maxslices.
-template <bool PART>
+// Pass 1: off[s] = 32 x (the most stored entries of a row of slice s), every
+// slice up to maxslices.  The stored count bounds the kept entries (the pack
+// leaves out neighbours that are not rows now and far pairs, and pads the
+// row with zeros), so this pass reads one count a row instead of following
+// every entry to its row.
 __global__ void __launch_bounds__(256) k_sp_width(SpArgs A) {
-    const uint32_t R = *A.nrows, np = A.sc->np;
+    const uint32_t R = *A.nrows;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t s = k / SP_SLICE;
     uint32_t cnt = 0;
-    if (k < R) {
-        const uint32_t i = __ldg(A.rowlist + k);
-        const uint32_t id = __ldg(A.idv + i);
-        const uint32_t n = __ldg(A.s_cnt + id);
-        for (uint32_t u0 = 0; u0 < n; u0 += SP_BATCH) {
-            bool ok[SP_BATCH];
-            int d[SP_BATCH];
-            uint32_t j[SP_BATCH];
-            sp_batch<PART>(A, id, n, u0, np, PART ? i : k, ok, d, j);
-#pragma unroll
-            for (uint32_t b = 0; b < SP_BATCH; b++) cnt += ok[b] ? 1u : 0u;
-        }
-    }
+    if (k < R) cnt = __ldg(A.s_cnt + __ldg(A.idv + __ldg(A.rowlist + k)));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_xor_sync(0xffffffffu, cnt, o));
     if ((threadIdx.x & 31) == 0 && s <= A.maxslices) A.off[s] = cnt * SP_SLICE;
@@ -786,8 +777,7 @@ int ppe_sp_enqueue_pack(PpeWork& w, const StageArgs& a, uint32_t cap, cudaStream
     const uint32_t maxslices = (cap + SP_SLICE - 1) / SP_SLICE;
     A.maxslices = maxslices;
     const uint32_t wb = cblocks((maxslices + 1) * SP_SLICE, 256), pb = cblocks(maxslices * SP_SLICE, 256);
-    if (by_particle) k_sp_width<true><<<wb, 256, 0, st>>>(A);
-    else k_sp_width<false><<<wb, 256, 0, st>>>(A);
+    k_sp_width<<<wb, 256, 0, st>>>(A);
     launch_scan_exclusive(w.sp_off, maxslices + 1, st);
     if (by_particle) k_sp_pack<true><<<pb, 256, 0, st>>>(A);
     else k_sp_pack<false><<<pb, 256, 0, st>>>(A);
