@@ -235,6 +235,10 @@ __device__ __forceinline__ float rq_next(const SolveArgs& S, const float2* rq, u
     return fmaf(-a, qv, v.x);
 }
 
+// PREC 0: diagonal scaling; PREC 1: the learned S' (particle columns), its
+// product fused into the residual update with each neighbour's r - alpha q
+// formed from the (r, q) pairs, the new residual into the other pair buffer;
+// both keep two grid-wide reductions per iteration.
 template <bool EX, int PREC, bool SW>
 __global__ void __launch_bounds__(PPE_THREADS) k_ppe_solve(SolveArgs S) {
     // Rows are the ordered list of non-Dirichlet rows; slices of 8 of them

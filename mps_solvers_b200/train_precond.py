@@ -43,7 +43,7 @@ def training_scene(k: int) -> scene.Scene:
 
 def evaluate(w: np.ndarray, k: int = HELD_OUT, warm: int = 50, steps: int = 20) -> dict:
     """PCG iterations and PPE solve milliseconds per step, diagonal scaling
-    against the learned factor, on scene k after `warm` steps."""
+    against the learned preconditioner, on scene k after `warm` steps."""
     out = {}
     with tempfile.TemporaryDirectory() as d:
         scene.write_case(d, training_scene(k))
