@@ -116,11 +116,12 @@ typedef struct {
                             in shared memory across CG iterations (0: 8;
                             -1: none; at most 8 in the compact layout, 6 in
                             the 8-byte layout with stored weights)           */
-    int precond_every;   /* learned preconditioner on the compact layout: steps
-                            between two evaluations of the network; between
-                            them the symmetric form of the factor is kept by
-                            particle (GEO index) and re-packed for the current
-                            rows every step (0: 40; 1: every step)           */
+    int precond_every;   /* learned preconditioner (every layout, batches
+                            too): steps between two evaluations of the
+                            network; between them the symmetric form of the
+                            factor is kept by particle (GEO index) and
+                            re-packed for the current rows every step
+                            (0: 40; 1: every step)                           */
 } mps_options;
 
 /* The 16 values of input.dat as the reference holds them after
